@@ -1,0 +1,184 @@
+/*
+ * p3m_b200 -- C ABI of the B200 (sm_100a) P3M force step and integrator.
+ *
+ * A drop-in for the hot path of xgdhar/MD-force-routines: the Python modules
+ * yukawa_pp, yukawa_pm_ord6, yukawa_gf_opt, yukawa_p3m_ord6,
+ * velocity_verlet_p3m_ord6 and thermostat_p3m_ord6 of this package call these
+ * entry points through ctypes. Each entry point names the reference routine it
+ * replaces (file:line in the reference tree).
+ *
+ * Conventions
+ *  - Every function returns an int status: P3M_OK (0) or a negative P3M_E*
+ *    code; none aborts. p3m_last_error() gives a message for the last failure
+ *    on a context (or of a context-free call when ctx is NULL).
+ *  - Host arrays are C-contiguous float64 in the reference's layouts: particle
+ *    arrays (N,3) row-major, meshes (Mz,My,Mx) with x fastest.
+ *  - One context per host thread; calls on a context run in order on its own
+ *    CUDA stream. Calls that take host pointers copy in, compute and copy out
+ *    before they return ("compat" calls). p3m_run() works on device-resident
+ *    state and returns without waiting unless asked to.
+ *  - A context holds R replicas (independent systems) with their own N, box,
+ *    kappa, alpha, r_c and mesh; every stage advances all of them in one
+ *    launch.
+ */
+#ifndef P3M_B200_H
+#define P3M_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define P3M_OK 0
+#define P3M_EARG (-1)          /* invalid argument or unsupported size        */
+#define P3M_ECUDA (-2)         /* CUDA runtime error                          */
+#define P3M_ENODEV (-3)        /* no usable sm_100 device                     */
+#define P3M_EBOX (-4)          /* particle outside [-L, 2L) or non-finite     */
+#define P3M_ENONFINITE (-5)    /* NaN/Inf in forces or energies               */
+#define P3M_ESTATE (-6)        /* call out of order (e.g. no state uploaded)  */
+
+/* arithmetic of the bulk stages (PP pair loop, assignment, FFT, gather) */
+#define P3M_FP64 0             /* everything in FP64: the plain method        */
+#define P3M_FP32 1             /* FP32 bulk, FP64 reductions and positions    */
+
+/* p3m_run modes */
+#define P3M_MODE_NVE 0         /* velocity_verlet_p3m_ord6.update per step    */
+#define P3M_MODE_THERMOSTAT 1  /* thermostat_p3m_ord6.vscale per step         */
+
+typedef struct p3m_ctx p3m_ctx;
+
+/* One replica. Mirrors the constants the reference's driver passes down the
+ * call stack (yukawa_MD_p3m_ord6.py:26-79). */
+typedef struct {
+    int32_t n;          /* particles                                         */
+    int32_t mesh;       /* M = Mx = My = Mz: power of two, 32..256 (0: no PM) */
+    int32_t order;      /* charge-assignment order p: must be 6              */
+    int32_t m_alias;    /* mx_max = my_max = mz_max of gf_opt (reference: 3) */
+    double box;         /* L = Lx = Ly = Lz                                  */
+    double kappa;       /* screening parameter                               */
+    double alpha;       /* Ewald splitting parameter (G / G_ew)              */
+    double rc;          /* PP cutoff; floor(L/rc) must be >= 3               */
+    double dt;          /* time step                                         */
+    double t_desired;   /* thermostat target temperature (1/Gamma)           */
+    double af, uf, kf;  /* acceleration, energy and kinetic-energy factors    */
+} p3m_replica_desc;
+
+/* ---- context ---------------------------------------------------------- */
+int p3m_create(const p3m_replica_desc *reps, int n_reps, int precision, int device,
+               p3m_ctx **out);
+int p3m_destroy(p3m_ctx *ctx);
+const char *p3m_last_error(const p3m_ctx *ctx);
+int p3m_version(void);
+/* Kernels launched on the context's stream so far (monotone counter). */
+int64_t p3m_launch_count(const p3m_ctx *ctx);
+
+/* ---- compat calls: host pointers in and out, one replica ---------------- */
+
+/* yukawa_pp.py:6 particle_particle(kappa,G,rc,Lv,pos,acc_s_r) -> (U, acc).
+ * pos (n,3) in; acc (n,3) out; *U out. */
+int p3m_pp(p3m_ctx *ctx, int replica, const double *pos, double *acc, double *U);
+
+/* yukawa_pm_ord6.py:6 charge_assgn_6_numba(rho_r,pos,Z,N,...) -> rho_r.
+ * rho (M,M,M) out. Z may be NULL (unit charges). */
+int p3m_assign(p3m_ctx *ctx, int replica, const double *pos, const double *Z, double *rho);
+
+/* yukawa_pm_ord6.py:213 field_assgn_6_numba(acc,E_x_p,..,E_x_r,..,pos,Z,..)
+ * Ex,Ey,Ez (M,M,M) in; acc (n,3) out; Ep (3,n) out (may be NULL). */
+int p3m_gather(p3m_ctx *ctx, int replica, const double *pos, const double *Z,
+               const double *Ex, const double *Ey, const double *Ez, double *acc,
+               double *Ep);
+
+/* yukawa_gf_opt.py:5 gf_opt(kappa,Gew,p,mx_max,my_max,mz_max,Mx,..,Lz):
+ * the optimal influence function on an M^3 mesh in the reference's fftshifted
+ * layout, computed in FP64 on the device. G_k (M,M,M) out; *A_pm out.
+ * Context-free: runs on `device`. */
+int p3m_gf_opt(int device, double kappa, double alpha, int p, int m_alias, int M,
+               double box, double *G_k, double *A_pm);
+
+/* Install the influence function the PM stage uses for `replica`, given in the
+ * reference's fftshifted (M,M,M) layout (as returned by gf_opt). With
+ * G_k == NULL the context computes it on the device itself. */
+int p3m_set_green(p3m_ctx *ctx, int replica, const double *G_k);
+
+/* yukawa_pm_ord6.py:440 particle_mesh_fft_r(...) -> (U_f, acc_f).
+ * acc (n,3) out; *U out; Ep (3,n) out (may be NULL); rho (M,M,M) out (may be
+ * NULL). */
+int p3m_pm(p3m_ctx *ctx, int replica, const double *pos, const double *Z, double *acc,
+           double *U, double *Ep, double *rho);
+
+/* yukawa_p3m_ord6.py:6 force_pot(...) -> (U, acc), with acc = af*(pp+pm) and
+ * U = uf*(U_pp + U_pm + U_self). parts (3) out: U_short, U_fft, U_self (may
+ * be NULL). */
+int p3m_force(p3m_ctx *ctx, int replica, const double *pos, const double *Z, double *acc,
+              double *U, double *parts);
+
+/* velocity_verlet_p3m_ord6.py:5 update(pos,vel,acc,dt,...) -> (pos,vel,acc,U)
+ * in place on host arrays (n,3); *U out. */
+int p3m_update(p3m_ctx *ctx, int replica, double *pos, double *vel, double *acc, double *U);
+
+/* thermostat_p3m_ord6.py:5 vscale(pos,vel,acc,T_desired,PBC,it,...) in place;
+ * *U and *T (temperature before the rescale) out. */
+int p3m_vscale(p3m_ctx *ctx, int replica, int it, double *pos, double *vel, double *acc,
+               double *U, double *T);
+
+/* One row of n(q,t), yukawa_MD_p3m_ord6.py:215-219: out (nq,3) complex128 as
+ * interleaved (re,im) doubles, for the wave numbers qv (nq). */
+int p3m_nqt(p3m_ctx *ctx, int replica, const double *pos, const double *qv, int nq,
+            double *out);
+
+/* ---- device-resident ("fast") path over all replicas ----------------------- */
+
+/* Copy state in/out. Any of the pointers may be NULL. Arrays are (n,3). */
+int p3m_set_state(p3m_ctx *ctx, int replica, const double *pos, const double *vel,
+                  const double *acc);
+int p3m_get_state(p3m_ctx *ctx, int replica, double *pos, double *vel, double *acc);
+
+/* Compute acc for the uploaded positions of all replicas (the driver's
+ * initial force call, yukawa_MD_p3m_ord6.py:171). */
+int p3m_init_forces(p3m_ctx *ctx);
+
+/* Configure the per-step n(q,t) record: nq wave numbers per replica given as
+ * multiples of 2*pi/L (qmult, nq), a ring of `capacity` steps. nq == 0
+ * disables it. */
+int p3m_set_nqt(p3m_ctx *ctx, const double *qmult, int nq, int capacity);
+
+/* Advance all replicas n_steps. mode: P3M_MODE_NVE or P3M_MODE_THERMOSTAT
+ * (it0 = step index of the first step, for the thermostat's it<=1999 switch).
+ * record_nqt: accumulate n(q,t) rows each step. use_graph: capture the step
+ * in a CUDA graph on first use and replay it. sync: wait for completion. */
+int p3m_run(p3m_ctx *ctx, int n_steps, int mode, int it0, int record_nqt, int use_graph,
+            int sync);
+
+/* Per-step energies recorded by p3m_run, (steps, R, 4) doubles:
+ * U, K, T (before any rescale), and the thermostat factor applied. Returns
+ * the number of steps copied in *n_out. */
+int p3m_get_energies(p3m_ctx *ctx, double *out, int max_steps, int *n_out);
+
+/* n(q,t) rows recorded by p3m_run for `replica`: (steps, nq, 3) complex as
+ * interleaved (re,im) doubles. */
+int p3m_get_nqt(p3m_ctx *ctx, int replica, double *out, int max_steps, int *n_out);
+
+/* Device status word accumulated since the last call (P3M_OK or the first
+ * error seen by a kernel), then cleared. Synchronises the stream. */
+int p3m_check(p3m_ctx *ctx);
+
+/* Wait for all work on the context's stream. */
+int p3m_sync(p3m_ctx *ctx);
+
+/* PP work decomposition: threads per i-particle (1, 2, 4) and CTAs per cell
+ * (1..4). p3m_create picks a default from the cell count; the autotuner of the
+ * Python package times the candidates and installs the fastest. */
+int p3m_set_pp_config(p3m_ctx *ctx, int tpi, int split);
+int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, int *split);
+
+/* Stream the context launches on (a cudaStream_t), for callers that time it
+ * with their own events. */
+void *p3m_stream(p3m_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* P3M_B200_H */

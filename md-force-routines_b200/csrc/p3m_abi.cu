@@ -1,0 +1,1005 @@
+// C ABI of libp3m_b200: contexts, device buffers, the compat entry points that
+// mirror the reference's Python functions, and the device-resident stepper.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "p3m_kernels.h"
+
+using namespace p3m;
+
+struct p3m_ctx {
+    int device = 0;
+    int prec = P3M_FP32;
+    int nrep = 0;
+    std::vector<p3m_replica_desc> desc;
+    std::vector<RepDev> rh;
+    std::vector<char> green_ready;
+    DevState s;
+    cudaStream_t st = nullptr;
+    int *counters = nullptr;      // [0] run step, [1] ring position, [2] it0
+    double *ring = nullptr;       // energies [cap][nrep][4]
+    int ring_cap = 0;
+    int ring_rows = 0;            // rows written (host-side tally)
+    double *qmult = nullptr;      // [nq]
+    int nq = 0, nqt_cap = 0;
+    double *nqt_part = nullptr;   // [nblk][nq*6]
+    double *nqt_ring = nullptr;   // [cap][nrep][nq*6]
+    int nqt_rows = 0;
+    double *scratch = nullptr;    // FP64 staging: max(3 M^3, gf partials)
+    double *ep = nullptr;         // FP64 field at particles (ntot,3)
+    double *tmp_nq = nullptr;     // one n(q) row for the compat call [nrep][nq*6]
+    int tmp_nq_cap = 0;
+    double *hbuf = nullptr;       // pinned host staging
+    size_t hbuf_bytes = 0;
+    bool state_set = false;
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    long long launches = 0;
+    std::string err;
+};
+
+static thread_local std::string g_err;
+
+#define P3M_VERSION 100
+
+#define CK(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) return fail(ctx, P3M_ECUDA, #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+static int fail(p3m_ctx *ctx, int code, const char *what, const char *why)
+{
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s: %s", what, why ? why : "");
+    if (ctx) ctx->err = buf; else g_err = buf;
+    return code;
+}
+
+static bool is_pow2(int m) { return m > 0 && (m & (m - 1)) == 0; }
+
+static int ilog2(int m)
+{
+    int l = 0;
+    while ((1 << l) < m) ++l;
+    return l;
+}
+
+template <typename X> static cudaError_t dalloc(X **p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(X));
+    if (e == cudaSuccess) e = cudaMemset(*p, 0, count * sizeof(X));
+    return e;
+}
+
+static cudaError_t valloc(void **p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
+    return e;
+}
+
+static int check_device(p3m_ctx *ctx, int device)
+{
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return fail(ctx, P3M_ENODEV, "no CUDA device", e != cudaSuccess ? cudaGetErrorString(e) : "");
+    if (device < 0 || device >= n) return fail(ctx, P3M_ENODEV, "device index out of range", "");
+    cudaDeviceProp pr;
+    CK(cudaGetDeviceProperties(&pr, device));
+    if (pr.major != 10)
+        return fail(ctx, P3M_ENODEV, "library is built for sm_100a (B200)", pr.name);
+    CK(cudaSetDevice(device));
+    return P3M_OK;
+}
+
+template <typename T> static size_t tsize() { return sizeof(T); }
+
+static int pp_default_split(int ncell, int ntot, int *tpi)
+{
+    const int target = 148 * 8;
+    const int navg = ntot / (ncell > 0 ? ncell : 1);
+    if (ncell >= target) {
+        *tpi = 1;
+        return navg > 128 ? 2 : 1;
+    }
+    *tpi = 4;
+    int chunks = (navg + 31) / 32;
+    int want = (target + ncell - 1) / ncell;
+    int split = chunks < want ? chunks : want;
+    return split < 1 ? 1 : split;
+}
+
+extern "C" int p3m_version(void) { return P3M_VERSION; }
+
+extern "C" const char *p3m_last_error(const p3m_ctx *ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+
+extern "C" int64_t p3m_launch_count(const p3m_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" void *p3m_stream(p3m_ctx *ctx) { return ctx ? (void *)ctx->st : nullptr; }
+
+extern "C" int p3m_destroy(p3m_ctx *ctx)
+{
+    if (!ctx) return P3M_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    for (auto &row : ctx->graph)
+        for (auto &g : row)
+            if (g) cudaGraphExecDestroy(g);
+    DevState &s = ctx->s;
+    void *ptrs[] = {s.reps, s.pos, s.vel, s.acc, s.charge, s.prep, s.cell_key, s.cell_count,
+                    s.cell_start, s.cell_cursor, s.cell_tmp, s.cell_perm, s.cell_slot, s.xs_cell,
+                    s.acc_pp, s.brick_key, s.brick_count, s.brick_start, s.brick_cursor,
+                    s.brick_perm, s.brick_slot, s.tiles, s.spec, s.ek, s.green, s.efield,
+                    s.acc_pm, s.twiddle, s.u_pp_part, s.u_pm_part, s.kin_part, s.rep_out,
+                    s.status, ctx->counters, ctx->ring, ctx->qmult, ctx->nqt_part,
+                    ctx->nqt_ring, ctx->scratch, ctx->ep, ctx->tmp_nq};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (ctx->hbuf) cudaFreeHost(ctx->hbuf);
+    if (ctx->st) cudaStreamDestroy(ctx->st);
+    delete ctx;
+    return P3M_OK;
+}
+
+template <typename T> static int alloc_bulk(p3m_ctx *ctx)
+{
+    using T4 = typename V4<T>::t;
+    using C = typename C2<T>::t;
+    DevState &s = ctx->s;
+    CK(valloc(&s.xs_cell, (size_t)s.ntot * sizeof(T4)));
+    CK(valloc(&s.acc_pp, (size_t)s.ntot * sizeof(T4)));
+    if (s.has_mesh) {
+        CK(valloc(&s.acc_pm, (size_t)s.ntot * sizeof(T4)));
+        CK(valloc(&s.spec, (size_t)s.nspec * sizeof(C)));
+        CK(valloc(&s.ek, (size_t)3 * s.nspec * sizeof(C)));
+        CK(valloc(&s.green, (size_t)s.nspec * sizeof(T)));
+        CK(valloc(&s.efield, (size_t)3 * s.nmesh * sizeof(T)));
+        // twiddles exp(-2 pi i k/256), k < 128, from long double
+        std::vector<C> tw(128);
+        for (int k = 0; k < 128; ++k) {
+            long double a = -2.0L * 3.141592653589793238462643383279502884L * k / 256.0L;
+            tw[k].x = (T)cosl(a);
+            tw[k].y = (T)sinl(a);
+        }
+        CK(valloc(&s.twiddle, 128 * sizeof(C)));
+        CK(cudaMemcpy(s.twiddle, tw.data(), 128 * sizeof(C), cudaMemcpyHostToDevice));
+        configure_mesh_kernels<T>();
+    }
+    configure_pp_kernels<T>();
+    configure_integrate_kernels<T>(64);
+    return P3M_OK;
+}
+
+extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precision, int device,
+                          p3m_ctx **out)
+{
+    if (!out) return fail(nullptr, P3M_EARG, "p3m_create", "out is NULL");
+    *out = nullptr;
+    if (!reps || n_reps <= 0) return fail(nullptr, P3M_EARG, "p3m_create", "no replicas");
+    if (precision != P3M_FP32 && precision != P3M_FP64)
+        return fail(nullptr, P3M_EARG, "p3m_create", "precision must be P3M_FP32 or P3M_FP64");
+    int with_mesh = reps[0].mesh > 0;
+    for (int r = 0; r < n_reps; ++r) {
+        const p3m_replica_desc &d = reps[r];
+        char why[256];
+        why[0] = 0;
+        if (d.n <= 0) snprintf(why, sizeof why, "replica %d: n must be > 0", r);
+        else if (!(d.box > 0) || !(d.rc > 0) || !(d.alpha > 0) || !(d.kappa >= 0))
+            snprintf(why, sizeof why, "replica %d: box, rc, alpha must be > 0, kappa >= 0", r);
+        else if ((int)floor(d.box / d.rc) < 3)
+            snprintf(why, sizeof why,
+                     "replica %d: floor(L/rc) = %d < 3 (the 27-cell stencil would count pairs twice)",
+                     r, (int)floor(d.box / d.rc));
+        else if ((d.mesh > 0) != with_mesh)
+            snprintf(why, sizeof why, "replica %d: all replicas need a mesh, or none", r);
+        else if (d.mesh > 0 && (!is_pow2(d.mesh) || d.mesh < 32 || d.mesh > 256))
+            snprintf(why, sizeof why, "replica %d: mesh must be a power of two in [32, 256]", r);
+        else if (d.mesh > 0 && d.order != 6)
+            snprintf(why, sizeof why, "replica %d: only charge-assignment order 6 is supported", r);
+        else if (d.m_alias < 0 || d.m_alias > 7)
+            snprintf(why, sizeof why, "replica %d: m_alias must be in [0, 7]", r);
+        if (why[0]) return fail(nullptr, P3M_EARG, "p3m_create", why);
+    }
+    p3m_ctx *ctx = new p3m_ctx();
+    int rc = check_device(ctx, device);
+    if (rc != P3M_OK) {
+        g_err = ctx->err;
+        delete ctx;
+        return rc;
+    }
+    ctx->device = device;
+    ctx->prec = precision;
+    ctx->nrep = n_reps;
+    ctx->desc.assign(reps, reps + n_reps);
+    ctx->green_ready.assign(n_reps, 0);
+    DevState &s = ctx->s;
+    s.nrep = n_reps;
+    s.has_mesh = with_mesh;
+    ctx->rh.resize(n_reps);
+    long long mesh = 0, spec = 0, tile = 0;
+    int p = 0, cell = 0, brick = 0, wa = 0, wb = 0, wc = 0, blk = 0, maxm = 0;
+    for (int r = 0; r < n_reps; ++r) {
+        const p3m_replica_desc &d = reps[r];
+        RepDev &R = ctx->rh[r];
+        memset(&R, 0, sizeof R);
+        R.n = d.n;
+        R.p_off = p;
+        R.L = d.box;
+        R.kappa = d.kappa;
+        R.alpha = d.alpha;
+        R.rc = d.rc;
+        R.nc = (int)floor(d.box / d.rc);
+        R.cellw = d.box / R.nc;
+        R.cell_off = cell;
+        R.dt = d.dt;
+        R.t_desired = d.t_desired;
+        R.af = d.af;
+        R.uf = d.uf;
+        R.kf = d.kf;
+        R.inv_cellw = 1.0 / R.cellw;
+        R.inv_L = 1.0 / d.box;
+        R.inv_V = 1.0 / (d.box * d.box * d.box);
+        R.blk_off = blk;
+        R.M = d.mesh;
+        if (d.mesh > 0) {
+            const int M = d.mesh;
+            R.logM = ilog2(M);
+            R.h = d.box / M;
+            R.inv_h = 1.0 / R.h;
+            R.nb = M / BRICK;
+            R.brick_off = brick;
+            R.mesh_off = mesh;
+            R.spec_off = spec;
+            R.tile_off = tile;
+            R.wa_off = wa;
+            R.wb_off = wb;
+            R.wc_off = wc;
+            brick += R.nb * R.nb * R.nb;
+            mesh += (long long)M * M * M;
+            spec += (long long)(M / 2 + 1) * M * M;
+            tile += (long long)R.nb * R.nb * R.nb * TILE3;
+            wa += M * (M / (2 * PENCIL));
+            wb += (M / 2 + 1) * (M / PENCIL);
+            wc += (M / 2 + 1) * (M / PENCIL);
+            if (M > maxm) maxm = M;
+        } else {
+            R.brick_off = brick;
+            R.wa_off = wa;
+            R.wb_off = wb;
+            R.wc_off = wc;
+        }
+        p += d.n;
+        cell += R.nc * R.nc * R.nc;
+        blk += (d.n + PBLK - 1) / PBLK;
+    }
+    s.ntot = p;
+    s.ncell = cell;
+    s.nbrick = brick;
+    s.nmesh = mesh;
+    s.nspec = spec;
+    s.ntile = tile;
+    s.wa = wa;
+    s.wb = wb;
+    s.wc = wc;
+    s.nblk = blk;
+    s.max_mesh = maxm;
+    s.pp_split = pp_default_split(cell, p, &s.pp_tpi);
+
+    auto cleanup = [&](int code) {
+        std::string e = ctx->err;
+        p3m_destroy(ctx);
+        g_err = e;
+        return code;
+    };
+#define CKC(call)                                                            \
+    do {                                                                     \
+        cudaError_t e_ = (call);                                             \
+        if (e_ != cudaSuccess) {                                             \
+            fail(ctx, P3M_ECUDA, #call, cudaGetErrorString(e_));             \
+            return cleanup(P3M_ECUDA);                                       \
+        }                                                                    \
+    } while (0)
+    CKC(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+    CKC(dalloc(&s.reps, n_reps));
+    CKC(cudaMemcpy(s.reps, ctx->rh.data(), sizeof(RepDev) * n_reps, cudaMemcpyHostToDevice));
+    CKC(dalloc(&s.pos, (size_t)3 * p));
+    CKC(dalloc(&s.vel, (size_t)3 * p));
+    CKC(dalloc(&s.acc, (size_t)3 * p));
+    CKC(dalloc(&s.charge, (size_t)p));
+    {
+        std::vector<double> ones(p, 1.0);
+        CKC(cudaMemcpy(s.charge, ones.data(), sizeof(double) * p, cudaMemcpyHostToDevice));
+        std::vector<int> pr(p);
+        for (int r = 0; r < n_reps; ++r)
+            for (int i = 0; i < reps[r].n; ++i) pr[ctx->rh[r].p_off + i] = r;
+        CKC(dalloc(&s.prep, (size_t)p));
+        CKC(cudaMemcpy(s.prep, pr.data(), sizeof(int) * p, cudaMemcpyHostToDevice));
+    }
+    CKC(dalloc(&s.cell_key, (size_t)p));
+    CKC(dalloc(&s.cell_count, (size_t)cell));
+    CKC(dalloc(&s.cell_start, (size_t)cell + 1));
+    CKC(dalloc(&s.cell_cursor, (size_t)cell));
+    CKC(dalloc(&s.cell_tmp, (size_t)p));
+    CKC(dalloc(&s.cell_perm, (size_t)p));
+    CKC(dalloc(&s.cell_slot, (size_t)p));
+    CKC(dalloc(&s.brick_key, (size_t)p));
+    CKC(dalloc(&s.brick_count, (size_t)brick));
+    CKC(dalloc(&s.brick_start, (size_t)brick + 1));
+    CKC(dalloc(&s.brick_cursor, (size_t)brick));
+    CKC(dalloc(&s.brick_perm, (size_t)p));
+    CKC(dalloc(&s.brick_slot, (size_t)p));
+    if (with_mesh) CKC(dalloc(&s.tiles, (size_t)tile));
+    CKC(dalloc(&s.u_pp_part, (size_t)cell * 4));
+    CKC(dalloc(&s.u_pm_part, (size_t)wc));
+    CKC(dalloc(&s.kin_part, (size_t)blk));
+    CKC(dalloc(&s.rep_out, (size_t)8 * n_reps));
+    CKC(dalloc(&s.status, 1));
+    CKC(dalloc(&ctx->counters, 4));
+    ctx->ring_cap = 8192;
+    CKC(dalloc(&ctx->ring, (size_t)ctx->ring_cap * n_reps * 4));
+    {
+        size_t sc = (size_t)3 * maxm * maxm * maxm;
+        size_t gfb = (size_t)gf_opt_blocks(maxm > 0 ? maxm : 1);
+        CKC(dalloc(&ctx->scratch, (sc > gfb ? sc : gfb) + gfb + 16));
+    }
+    CKC(dalloc(&ctx->ep, (size_t)3 * p));
+    int arc = (precision == P3M_FP32) ? alloc_bulk<float>(ctx) : alloc_bulk<double>(ctx);
+    if (arc != P3M_OK) return cleanup(arc);
+    CKC(cudaGetLastError());
+    CKC(cudaDeviceSynchronize());
+#undef CKC
+    *out = ctx;
+    return P3M_OK;
+}
+
+// ---------------------------------------------------------------------------
+// internal sequences (enqueue only)
+// ---------------------------------------------------------------------------
+
+template <typename T> static void seq_sort(p3m_ctx *ctx, bool keys)
+{
+    DevState &s = ctx->s;
+    if (keys) {
+        launch_keys<T>(s, ctx->st);
+        ctx->launches++;
+    }
+    launch_scan(s, ctx->st);
+    launch_scatter(s, ctx->st);
+    launch_fix_cells<T>(s, ctx->st);
+    ctx->launches += 3;
+}
+
+template <typename T> static void seq_pp(p3m_ctx *ctx)
+{
+    launch_pp<T>(ctx->s, ctx->st);
+    launch_reduce_pp(ctx->s, ctx->st);
+    ctx->launches += 2;
+}
+
+template <typename T> static void seq_pm(p3m_ctx *ctx)
+{
+    DevState &s = ctx->s;
+    launch_assign<T>(s, ctx->st);
+    launch_fft_forward<T>(s, ctx->st);
+    launch_reduce_pm(s, ctx->st);
+    launch_fft_inverse<T>(s, ctx->st);
+    launch_gather<T>(s, ctx->st);
+    ctx->launches += 8;
+}
+
+// Compute the influence function of every replica that has none yet.
+template <typename T> static int ensure_green(p3m_ctx *ctx)
+{
+    for (int r = 0; r < ctx->nrep; ++r) {
+        if (ctx->green_ready[r] || ctx->rh[r].M == 0) continue;
+        const p3m_replica_desc &d = ctx->desc[r];
+        launch_gf_opt(d.kappa, d.alpha, d.order, d.m_alias, d.mesh, d.box, ctx->scratch,
+                      ctx->scratch + (size_t)3 * ctx->s.max_mesh * ctx->s.max_mesh * ctx->s.max_mesh,
+                      ctx->st);
+        launch_green_from_host_layout<T>(ctx->s, r, ctx->scratch, ctx->st);
+        ctx->launches += 2;
+        ctx->green_ready[r] = 1;
+    }
+    CK(cudaGetLastError());
+    return P3M_OK;
+}
+
+// One full force evaluation of the current device positions: sort (with or
+// without the key pass), PP, PM. Leaves acc_pp / acc_pm and U parts.
+template <typename T> static int seq_force(p3m_ctx *ctx, bool keys)
+{
+    if (ctx->s.has_mesh) {
+        int rc = ensure_green<T>(ctx);
+        if (rc != P3M_OK) return rc;
+    }
+    seq_sort<T>(ctx, keys);
+    seq_pp<T>(ctx);
+    if (ctx->s.has_mesh) seq_pm<T>(ctx);
+    return P3M_OK;
+}
+
+// One integrator step of every replica (mode 0 NVE, 1 thermostat).
+template <typename T> static void seq_step(p3m_ctx *ctx, int mode, int record_nqt)
+{
+    DevState &s = ctx->s;
+    launch_kick_drift(s, ctx->st);
+    ctx->launches++;
+    seq_sort<T>(ctx, false);
+    seq_pp<T>(ctx);
+    if (s.has_mesh) seq_pm<T>(ctx);
+    launch_kick_finish<T>(s, 1, nullptr, ctx->st);
+    launch_step_reduce(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, ctx->st);
+    ctx->launches += 2;
+    if (mode == P3M_MODE_THERMOSTAT) {
+        launch_scale_vel(s, ctx->st);
+        ctx->launches++;
+    }
+    if (record_nqt && ctx->nq > 0) {
+        launch_nqt<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nqt_part, ctx->nqt_ring, ctx->counters,
+                      ctx->nqt_cap, ctx->st);
+        ctx->launches += 2;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host staging helpers
+// ---------------------------------------------------------------------------
+
+// Host <-> device copies on the context's stream (callers synchronise in
+// finish()).
+static int h2d(p3m_ctx *ctx, void *dst, const void *src, size_t bytes)
+{
+    if (!bytes) return P3M_OK;
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->st));
+    return P3M_OK;
+}
+
+static int d2h(p3m_ctx *ctx, void *dst, const void *src, size_t bytes)
+{
+    if (!bytes) return P3M_OK;
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->st));
+    return P3M_OK;
+}
+
+static int finish(p3m_ctx *ctx)
+{
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+    int st = 0;
+    CK(cudaMemcpy(&st, ctx->s.status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st) {
+        CK(cudaMemset(ctx->s.status, 0, sizeof(int)));
+        if (st & ST_BOX) return fail(ctx, P3M_EBOX, "particle outside [-L, 2L) or non-finite position", "");
+        if (st & ST_NONFINITE) return fail(ctx, P3M_ENONFINITE, "non-finite force or energy", "");
+    }
+    return P3M_OK;
+}
+
+static int compat_check(p3m_ctx *ctx, int replica)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (ctx->nrep != 1 || replica != 0)
+        return fail(ctx, P3M_EARG, "compat call", "needs a single-replica context and replica 0");
+    CK(cudaSetDevice(ctx->device));
+    return P3M_OK;
+}
+
+static int upload_charge(p3m_ctx *ctx, const double *Z)
+{
+    const int n = ctx->s.ntot;
+    if (Z) return h2d(ctx, ctx->s.charge, Z, sizeof(double) * n);
+    return P3M_OK;
+}
+
+#define DISPATCH(fn, ...) (ctx->prec == P3M_FP32 ? fn<float>(__VA_ARGS__) : fn<double>(__VA_ARGS__))
+#define RET(x) do { int rc_ = (x); if (rc_ != P3M_OK) return rc_; } while (0)
+
+// ---------------------------------------------------------------------------
+// compat entry points
+// ---------------------------------------------------------------------------
+
+template <typename T> static int do_pp(p3m_ctx *ctx, const double *pos, double *acc, double *U)
+{
+    DevState &s = ctx->s;
+    RET(h2d(ctx, s.pos, pos, sizeof(double) * 3 * s.ntot));
+    seq_sort<T>(ctx, true);
+    seq_pp<T>(ctx);
+    launch_combine<T>(s, 1, 0, 0, s.acc, nullptr, ctx->st);
+    ctx->launches++;
+    RET(d2h(ctx, acc, s.acc, sizeof(double) * 3 * s.ntot));
+    double ro[8];
+    RET(d2h(ctx, ro, s.rep_out, sizeof ro));
+    RET(finish(ctx));
+    *U = ro[RO_UPP];
+    return P3M_OK;
+}
+
+extern "C" int p3m_pp(p3m_ctx *ctx, int replica, const double *pos, double *acc, double *U)
+{
+    RET(compat_check(ctx, replica));
+    if (!pos || !acc || !U) return fail(ctx, P3M_EARG, "p3m_pp", "NULL argument");
+    return DISPATCH(do_pp, ctx, pos, acc, U);
+}
+
+static int need_mesh(p3m_ctx *ctx, const char *who)
+{
+    if (!ctx->s.has_mesh) return fail(ctx, P3M_EARG, who, "context has no mesh");
+    return P3M_OK;
+}
+
+template <typename T> static int do_assign(p3m_ctx *ctx, const double *pos, const double *Z, double *rho)
+{
+    DevState &s = ctx->s;
+    const int M = ctx->rh[0].M;
+    RET(h2d(ctx, s.pos, pos, sizeof(double) * 3 * s.ntot));
+    RET(upload_charge(ctx, Z));
+    seq_sort<T>(ctx, true);
+    launch_assign<T>(s, ctx->st);
+    launch_tiles_to_mesh<T>(s, 0, ctx->scratch, ctx->st);
+    ctx->launches += 2;
+    RET(d2h(ctx, rho, ctx->scratch, sizeof(double) * M * M * M));
+    return finish(ctx);
+}
+
+extern "C" int p3m_assign(p3m_ctx *ctx, int replica, const double *pos, const double *Z, double *rho)
+{
+    RET(compat_check(ctx, replica));
+    RET(need_mesh(ctx, "p3m_assign"));
+    if (!pos || !rho) return fail(ctx, P3M_EARG, "p3m_assign", "NULL argument");
+    return DISPATCH(do_assign, ctx, pos, Z, rho);
+}
+
+template <typename T>
+static int do_gather(p3m_ctx *ctx, const double *pos, const double *Z, const double *Ex,
+                     const double *Ey, const double *Ez, double *acc, double *Ep)
+{
+    DevState &s = ctx->s;
+    const size_t M3 = (size_t)ctx->rh[0].M * ctx->rh[0].M * ctx->rh[0].M;
+    RET(h2d(ctx, s.pos, pos, sizeof(double) * 3 * s.ntot));
+    RET(upload_charge(ctx, Z));
+    RET(h2d(ctx, ctx->scratch, Ex, sizeof(double) * M3));
+    RET(h2d(ctx, ctx->scratch + M3, Ey, sizeof(double) * M3));
+    RET(h2d(ctx, ctx->scratch + 2 * M3, Ez, sizeof(double) * M3));
+    launch_efield_from_mesh<T>(s, 0, ctx->scratch, ctx->scratch + M3, ctx->scratch + 2 * M3, ctx->st);
+    ctx->launches++;
+    seq_sort<T>(ctx, true);
+    launch_gather<T>(s, ctx->st);
+    launch_combine<T>(s, 0, 1, 0, s.acc, ctx->ep, ctx->st);
+    ctx->launches += 2;
+    RET(d2h(ctx, acc, s.acc, sizeof(double) * 3 * s.ntot));
+    RET(finish(ctx));
+    if (Ep) {
+        std::vector<double> e(3 * (size_t)s.ntot);
+        CK(cudaMemcpy(e.data(), ctx->ep, sizeof(double) * e.size(), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < s.ntot; ++i)
+            for (int d = 0; d < 3; ++d) Ep[(size_t)d * s.ntot + i] = e[3 * (size_t)i + d];
+    }
+    return P3M_OK;
+}
+
+extern "C" int p3m_gather(p3m_ctx *ctx, int replica, const double *pos, const double *Z,
+                          const double *Ex, const double *Ey, const double *Ez, double *acc,
+                          double *Ep)
+{
+    RET(compat_check(ctx, replica));
+    RET(need_mesh(ctx, "p3m_gather"));
+    if (!pos || !Ex || !Ey || !Ez || !acc) return fail(ctx, P3M_EARG, "p3m_gather", "NULL argument");
+    return DISPATCH(do_gather, ctx, pos, Z, Ex, Ey, Ez, acc, Ep);
+}
+
+extern "C" int p3m_gf_opt(int device, double kappa, double alpha, int p, int m_alias, int M,
+                          double box, double *G_k, double *A_pm)
+{
+    p3m_ctx *ctx = nullptr;
+    if (!G_k || !A_pm) return fail(nullptr, P3M_EARG, "p3m_gf_opt", "NULL argument");
+    if (M < 2 || M > 1024 || !(box > 0) || !(alpha > 0) || p < 1 || m_alias < 0 || m_alias > 7)
+        return fail(nullptr, P3M_EARG, "p3m_gf_opt", "bad size or parameter");
+    int rc = check_device(nullptr, device);
+    if (rc != P3M_OK) return rc;
+    const size_t n = (size_t)M * M * M;
+    const int nb = gf_opt_blocks(M);
+    double *d_g = nullptr, *d_a = nullptr;
+    CK(cudaMalloc(&d_g, n * sizeof(double)));
+    cudaError_t e = cudaMalloc(&d_a, nb * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaFree(d_g);
+        return fail(nullptr, P3M_ECUDA, "cudaMalloc", cudaGetErrorString(e));
+    }
+    launch_gf_opt(kappa, alpha, p, m_alias, M, box, d_g, d_a, 0);
+    std::vector<double> a(nb);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(G_k, d_g, n * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(a.data(), d_a, nb * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d_g);
+    cudaFree(d_a);
+    if (e != cudaSuccess) return fail(nullptr, P3M_ECUDA, "p3m_gf_opt", cudaGetErrorString(e));
+    double s = 0.0;
+    for (int k = 0; k < nb; ++k) s += a[k];
+    *A_pm = s;
+    return P3M_OK;
+}
+
+template <typename T> static int do_set_green(p3m_ctx *ctx, int replica, const double *G_k)
+{
+    const RepDev &R = ctx->rh[replica];
+    if (!G_k) {
+        ctx->green_ready[replica] = 0;
+        return ensure_green<T>(ctx);
+    }
+    const size_t M3 = (size_t)R.M * R.M * R.M;
+    RET(h2d(ctx, ctx->scratch, G_k, sizeof(double) * M3));
+    launch_green_from_host_layout<T>(ctx->s, replica, ctx->scratch, ctx->st);
+    ctx->launches++;
+    ctx->green_ready[replica] = 1;
+    return finish(ctx);
+}
+
+extern "C" int p3m_set_green(p3m_ctx *ctx, int replica, const double *G_k)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (replica < 0 || replica >= ctx->nrep) return fail(ctx, P3M_EARG, "p3m_set_green", "replica");
+    RET(need_mesh(ctx, "p3m_set_green"));
+    CK(cudaSetDevice(ctx->device));
+    return DISPATCH(do_set_green, ctx, replica, G_k);
+}
+
+template <typename T>
+static int do_pm(p3m_ctx *ctx, const double *pos, const double *Z, double *acc, double *U,
+                 double *Ep, double *rho)
+{
+    DevState &s = ctx->s;
+    const int M = ctx->rh[0].M;
+    RET(ensure_green<T>(ctx));
+    RET(h2d(ctx, s.pos, pos, sizeof(double) * 3 * s.ntot));
+    RET(upload_charge(ctx, Z));
+    seq_sort<T>(ctx, true);
+    seq_pm<T>(ctx);
+    launch_combine<T>(s, 0, 1, 0, s.acc, ctx->ep, ctx->st);
+    ctx->launches++;
+    if (rho) {
+        launch_tiles_to_mesh<T>(s, 0, ctx->scratch, ctx->st);
+        ctx->launches++;
+        RET(d2h(ctx, rho, ctx->scratch, sizeof(double) * M * M * M));
+    }
+    RET(d2h(ctx, acc, s.acc, sizeof(double) * 3 * s.ntot));
+    double ro[8];
+    RET(d2h(ctx, ro, s.rep_out, sizeof ro));
+    RET(finish(ctx));
+    *U = ro[RO_UPM];
+    if (Ep) {
+        std::vector<double> e(3 * (size_t)s.ntot);
+        CK(cudaMemcpy(e.data(), ctx->ep, sizeof(double) * e.size(), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < s.ntot; ++i)
+            for (int d = 0; d < 3; ++d) Ep[(size_t)d * s.ntot + i] = e[3 * (size_t)i + d];
+    }
+    return P3M_OK;
+}
+
+extern "C" int p3m_pm(p3m_ctx *ctx, int replica, const double *pos, const double *Z, double *acc,
+                      double *U, double *Ep, double *rho)
+{
+    RET(compat_check(ctx, replica));
+    RET(need_mesh(ctx, "p3m_pm"));
+    if (!pos || !acc || !U) return fail(ctx, P3M_EARG, "p3m_pm", "NULL argument");
+    return DISPATCH(do_pm, ctx, pos, Z, acc, U, Ep, rho);
+}
+
+template <typename T>
+static int do_force(p3m_ctx *ctx, const double *pos, const double *Z, double *acc, double *U,
+                    double *parts)
+{
+    DevState &s = ctx->s;
+    RET(h2d(ctx, s.pos, pos, sizeof(double) * 3 * s.ntot));
+    RET(upload_charge(ctx, Z));
+    RET(seq_force<T>(ctx, true));
+    launch_kick_finish<T>(s, 0, nullptr, ctx->st);
+    launch_step_reduce(s, 2, ctx->counters, nullptr, 0, ctx->st);
+    ctx->launches += 2;
+    RET(d2h(ctx, acc, s.acc, sizeof(double) * 3 * s.ntot));
+    double ro[8];
+    RET(d2h(ctx, ro, s.rep_out, sizeof ro));
+    RET(finish(ctx));
+    *U = ro[RO_U];
+    if (parts) {
+        parts[0] = ro[RO_UPP];
+        parts[1] = ro[RO_UPM];
+        parts[2] = ro[RO_USELF];
+    }
+    return P3M_OK;
+}
+
+extern "C" int p3m_force(p3m_ctx *ctx, int replica, const double *pos, const double *Z,
+                         double *acc, double *U, double *parts)
+{
+    RET(compat_check(ctx, replica));
+    if (!pos || !acc || !U) return fail(ctx, P3M_EARG, "p3m_force", "NULL argument");
+    return DISPATCH(do_force, ctx, pos, Z, acc, U, parts);
+}
+
+template <typename T>
+static int do_update(p3m_ctx *ctx, int mode, int it, double *pos, double *vel, double *acc,
+                     double *U, double *Tout)
+{
+    DevState &s = ctx->s;
+    const size_t b = sizeof(double) * 3 * s.ntot;
+    RET(h2d(ctx, s.pos, pos, b));
+    RET(h2d(ctx, s.vel, vel, b));
+    RET(h2d(ctx, s.acc, acc, b));
+    if (s.has_mesh) RET(ensure_green<T>(ctx));
+    launch_set_counters(ctx->counters, 0, -1, it, ctx->st);
+    ctx->launches++;
+    seq_step<T>(ctx, mode, 0);
+    RET(d2h(ctx, pos, s.pos, b));
+    RET(d2h(ctx, vel, s.vel, b));
+    RET(d2h(ctx, acc, s.acc, b));
+    double ro[8];
+    RET(d2h(ctx, ro, s.rep_out, sizeof ro));
+    RET(finish(ctx));
+    *U = ro[RO_U];
+    if (Tout) *Tout = ro[RO_T];
+    return P3M_OK;
+}
+
+extern "C" int p3m_update(p3m_ctx *ctx, int replica, double *pos, double *vel, double *acc, double *U)
+{
+    RET(compat_check(ctx, replica));
+    if (!pos || !vel || !acc || !U) return fail(ctx, P3M_EARG, "p3m_update", "NULL argument");
+    return DISPATCH(do_update, ctx, P3M_MODE_NVE, 0, pos, vel, acc, U, nullptr);
+}
+
+extern "C" int p3m_vscale(p3m_ctx *ctx, int replica, int it, double *pos, double *vel, double *acc,
+                          double *U, double *T)
+{
+    RET(compat_check(ctx, replica));
+    if (!pos || !vel || !acc || !U) return fail(ctx, P3M_EARG, "p3m_vscale", "NULL argument");
+    return DISPATCH(do_update, ctx, P3M_MODE_THERMOSTAT, it, pos, vel, acc, U, T);
+}
+
+template <typename T>
+static int do_nqt(p3m_ctx *ctx, int replica, const double *pos, const double *qv, int nq, double *out)
+{
+    DevState &s = ctx->s;
+    const RepDev &R = ctx->rh[replica];
+    if (nq > 64) return fail(ctx, P3M_EARG, "p3m_nqt", "nq must be <= 64");
+    if (ctx->tmp_nq_cap < nq) {
+        if (ctx->tmp_nq) cudaFree(ctx->tmp_nq);
+        ctx->tmp_nq = nullptr;
+        CK(dalloc(&ctx->tmp_nq, (size_t)ctx->nrep * 64 * 6 + (size_t)s.nblk * 64 * 6 + 64));
+        ctx->tmp_nq_cap = 64;
+    }
+    double *qm = ctx->tmp_nq;
+    double *part = qm + 64;
+    double *o = part + (size_t)s.nblk * 64 * 6;
+    std::vector<double> qmult(nq);
+    for (int k = 0; k < nq; ++k) qmult[k] = qv[k] * R.L / (2.0 * 3.141592653589793238);
+    RET(h2d(ctx, s.pos + 3 * (size_t)R.p_off, pos, sizeof(double) * 3 * R.n));
+    CK(cudaMemcpyAsync(qm, qmult.data(), sizeof(double) * nq, cudaMemcpyHostToDevice, ctx->st));
+    launch_nqt<T>(s, s.pos, qm, nq, part, o, nullptr, 0, ctx->st);
+    ctx->launches += 2;
+    RET(d2h(ctx, out, o + (size_t)replica * nq * 6, sizeof(double) * nq * 6));
+    RET(finish(ctx));
+    // (nq, 3) complex: reorder [iq][axis][re,im] is already the layout
+    return P3M_OK;
+}
+
+extern "C" int p3m_nqt(p3m_ctx *ctx, int replica, const double *pos, const double *qv, int nq,
+                       double *out)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (replica < 0 || replica >= ctx->nrep || !pos || !qv || !out || nq <= 0)
+        return fail(ctx, P3M_EARG, "p3m_nqt", "bad argument");
+    CK(cudaSetDevice(ctx->device));
+    return DISPATCH(do_nqt, ctx, replica, pos, qv, nq, out);
+}
+
+// ---------------------------------------------------------------------------
+// device-resident path
+// ---------------------------------------------------------------------------
+
+extern "C" int p3m_set_state(p3m_ctx *ctx, int replica, const double *pos, const double *vel,
+                             const double *acc)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (replica < 0 || replica >= ctx->nrep) return fail(ctx, P3M_EARG, "p3m_set_state", "replica");
+    CK(cudaSetDevice(ctx->device));
+    const RepDev &R = ctx->rh[replica];
+    const size_t o = 3 * (size_t)R.p_off, b = sizeof(double) * 3 * R.n;
+    if (pos) RET(h2d(ctx, ctx->s.pos + o, pos, b));
+    if (vel) RET(h2d(ctx, ctx->s.vel + o, vel, b));
+    if (acc) RET(h2d(ctx, ctx->s.acc + o, acc, b));
+    ctx->state_set = true;
+    return finish(ctx);
+}
+
+extern "C" int p3m_get_state(p3m_ctx *ctx, int replica, double *pos, double *vel, double *acc)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (replica < 0 || replica >= ctx->nrep) return fail(ctx, P3M_EARG, "p3m_get_state", "replica");
+    CK(cudaSetDevice(ctx->device));
+    const RepDev &R = ctx->rh[replica];
+    const size_t o = 3 * (size_t)R.p_off, b = sizeof(double) * 3 * R.n;
+    if (pos) RET(d2h(ctx, pos, ctx->s.pos + o, b));
+    if (vel) RET(d2h(ctx, vel, ctx->s.vel + o, b));
+    if (acc) RET(d2h(ctx, acc, ctx->s.acc + o, b));
+    return finish(ctx);
+}
+
+template <typename T> static int do_init_forces(p3m_ctx *ctx)
+{
+    RET(seq_force<T>(ctx, true));
+    launch_kick_finish<T>(ctx->s, 0, nullptr, ctx->st);
+    launch_step_reduce(ctx->s, 2, ctx->counters, nullptr, 0, ctx->st);
+    ctx->launches += 2;
+    return finish(ctx);
+}
+
+extern "C" int p3m_init_forces(p3m_ctx *ctx)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    CK(cudaSetDevice(ctx->device));
+    return DISPATCH(do_init_forces, ctx);
+}
+
+extern "C" int p3m_set_nqt(p3m_ctx *ctx, const double *qmult, int nq, int capacity)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (nq < 0 || nq > 64 || (nq > 0 && (!qmult || capacity <= 0)))
+        return fail(ctx, P3M_EARG, "p3m_set_nqt", "need 0 <= nq <= 64 and capacity > 0");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (ctx->qmult) cudaFree(ctx->qmult);
+    if (ctx->nqt_part) cudaFree(ctx->nqt_part);
+    if (ctx->nqt_ring) cudaFree(ctx->nqt_ring);
+    ctx->qmult = ctx->nqt_part = ctx->nqt_ring = nullptr;
+    for (auto &row : ctx->graph)
+        if (row[1]) { cudaGraphExecDestroy(row[1]); row[1] = nullptr; }
+    ctx->nq = nq;
+    ctx->nqt_cap = capacity;
+    ctx->nqt_rows = 0;
+    if (nq == 0) return P3M_OK;
+    CK(dalloc(&ctx->qmult, (size_t)nq));
+    CK(cudaMemcpy(ctx->qmult, qmult, sizeof(double) * nq, cudaMemcpyHostToDevice));
+    CK(dalloc(&ctx->nqt_part, (size_t)ctx->s.nblk * nq * 6));
+    CK(dalloc(&ctx->nqt_ring, (size_t)capacity * ctx->nrep * nq * 6));
+    // ring positions restart at 0
+    launch_set_counters(ctx->counters, -1, 0, 0, ctx->st);
+    ctx->ring_rows = 0;
+    return finish(ctx);
+}
+
+template <typename T> static int do_run(p3m_ctx *ctx, int n_steps, int mode, int it0, int rec,
+                                        int use_graph, int sync)
+{
+    DevState &s = ctx->s;
+    if (s.has_mesh) RET(ensure_green<T>(ctx));
+    launch_set_counters(ctx->counters, 0, -1, it0, ctx->st);
+    ctx->launches++;
+    const int gi = (mode == P3M_MODE_THERMOSTAT) ? 1 : 0, gr = rec ? 1 : 0;
+    if (use_graph && !ctx->graph[gi][gr]) {
+        cudaGraph_t g;
+        const long long before = ctx->launches;
+        CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+        seq_step<T>(ctx, mode, rec);
+        cudaError_t e = cudaStreamEndCapture(ctx->st, &g);
+        ctx->launches = before;
+        if (e != cudaSuccess) return fail(ctx, P3M_ECUDA, "cudaStreamEndCapture", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&ctx->graph[gi][gr], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(ctx, P3M_ECUDA, "cudaGraphInstantiate", cudaGetErrorString(e));
+    }
+    for (int k = 0; k < n_steps; ++k) {
+        if (use_graph) {
+            const long long before = ctx->launches;
+            CK(cudaGraphLaunch(ctx->graph[gi][gr], ctx->st));
+            // count the kernels the graph holds (same sequence as seq_step)
+            ctx->launches = before + (long long)(8 + (s.has_mesh ? 8 : 0) + (gi ? 1 : 0) +
+                                                 ((gr && ctx->nq > 0) ? 2 : 0));
+        } else {
+            seq_step<T>(ctx, mode, rec);
+        }
+    }
+    ctx->ring_rows += n_steps;
+    if (rec) ctx->nqt_rows += n_steps;
+    CK(cudaGetLastError());
+    if (sync) return finish(ctx);
+    return P3M_OK;
+}
+
+extern "C" int p3m_run(p3m_ctx *ctx, int n_steps, int mode, int it0, int record_nqt, int use_graph,
+                       int sync)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (n_steps < 0 || (mode != P3M_MODE_NVE && mode != P3M_MODE_THERMOSTAT))
+        return fail(ctx, P3M_EARG, "p3m_run", "bad n_steps or mode");
+    if (record_nqt && ctx->nq == 0) return fail(ctx, P3M_EARG, "p3m_run", "n(q,t) not configured");
+    CK(cudaSetDevice(ctx->device));
+    return DISPATCH(do_run, ctx, n_steps, mode, it0, record_nqt, use_graph, sync);
+}
+
+extern "C" int p3m_get_energies(p3m_ctx *ctx, double *out, int max_steps, int *n_out)
+{
+    if (!ctx || !out || !n_out) return fail(ctx, P3M_EARG, "p3m_get_energies", "NULL argument");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    int pos[4];
+    CK(cudaMemcpy(pos, ctx->counters, sizeof pos, cudaMemcpyDeviceToHost));
+    const int total = pos[1];
+    int n = total < ctx->ring_cap ? total : ctx->ring_cap;
+    if (n > max_steps) n = max_steps;
+    const size_t row = (size_t)ctx->nrep * 4;
+    for (int k = 0; k < n; ++k) {
+        const int step = total - n + k;
+        CK(cudaMemcpy(out + (size_t)k * row, ctx->ring + (size_t)(step % ctx->ring_cap) * row,
+                      sizeof(double) * row, cudaMemcpyDeviceToHost));
+    }
+    *n_out = n;
+    return P3M_OK;
+}
+
+extern "C" int p3m_get_nqt(p3m_ctx *ctx, int replica, double *out, int max_steps, int *n_out)
+{
+    if (!ctx || !out || !n_out) return fail(ctx, P3M_EARG, "p3m_get_nqt", "NULL argument");
+    if (replica < 0 || replica >= ctx->nrep || ctx->nq == 0)
+        return fail(ctx, P3M_EARG, "p3m_get_nqt", "bad replica or n(q,t) not configured");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    int pos[4];
+    CK(cudaMemcpy(pos, ctx->counters, sizeof pos, cudaMemcpyDeviceToHost));
+    const int total = ctx->nqt_rows < pos[1] ? ctx->nqt_rows : pos[1];
+    int n = total < ctx->nqt_cap ? total : ctx->nqt_cap;
+    if (n > max_steps) n = max_steps;
+    const size_t rowlen = (size_t)ctx->nq * 6;
+    for (int k = 0; k < n; ++k) {
+        const int step = pos[1] - n + k;
+        const double *src = ctx->nqt_ring + ((size_t)(step % ctx->nqt_cap) * ctx->nrep + replica) * rowlen;
+        CK(cudaMemcpy(out + (size_t)k * rowlen, src, sizeof(double) * rowlen, cudaMemcpyDeviceToHost));
+    }
+    *n_out = n;
+    return P3M_OK;
+}
+
+extern "C" int p3m_check(p3m_ctx *ctx)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    CK(cudaSetDevice(ctx->device));
+    return finish(ctx);
+}
+
+extern "C" int p3m_sync(p3m_ctx *ctx)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    return P3M_OK;
+}
+
+extern "C" int p3m_set_pp_config(p3m_ctx *ctx, int tpi, int split)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (!(tpi == 1 || tpi == 2 || tpi == 4) || split < 1 || split > 4)
+        return fail(ctx, P3M_EARG, "p3m_set_pp_config", "tpi in {1,2,4}, split in [1,4]");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->s.pp_tpi = tpi;
+    ctx->s.pp_split = split;
+    for (auto &row : ctx->graph)
+        for (auto &g : row)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    return P3M_OK;
+}
+
+extern "C" int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, int *split)
+{
+    if (!ctx || !tpi || !split) return fail(ctx, P3M_EARG, "p3m_get_pp_config", "NULL argument");
+    *tpi = ctx->s.pp_tpi;
+    *split = ctx->s.pp_split;
+    return P3M_OK;
+}

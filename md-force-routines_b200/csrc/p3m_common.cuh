@@ -1,0 +1,155 @@
+// Shared device-side definitions of the p3m_b200 kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "p3m_b200.h"
+
+namespace p3m {
+
+// Mesh bricks of the deterministic charge assignment: a brick is BRICK^3 base
+// cells; the order-6 stencil of a particle with base index i reaches nodes
+// i..i+5 (yukawa_pm_ord6.py:52-93), so a brick's tile spans BRICK+5 nodes.
+constexpr int BRICK = 16;
+constexpr int HALO = 5;
+constexpr int TILE = BRICK + HALO;
+constexpr int TILE3 = TILE * TILE * TILE;
+
+// Lines per pencil tile in the FFT passes (consecutive y rows or z lines).
+constexpr int PENCIL = 16;
+constexpr int MAX_LOGM = 8;  // M <= 256
+constexpr int PBLK = 256;    // particles per block in replica-aligned particle kernels
+
+// Device status bits (first error wins in the host's reading order).
+enum : int {
+    ST_BOX = 1,        // particle outside [-L, 2L) or position not finite
+    ST_NONFINITE = 2,  // NaN/Inf in forces or energies
+};
+
+// Per-replica constants. Offsets index the concatenated device arrays.
+struct RepDev {
+    int n, p_off;          // particles, offset into particle arrays
+    int M, logM;           // mesh side and log2
+    int nc, cell_off;      // PP cells per side, offset into cell arrays
+    int nb, brick_off;     // bricks per side, offset into brick arrays
+    long long mesh_off;    // offset into real meshes (M^3 per replica)
+    long long spec_off;    // offset into half spectra ((M/2+1) M^2)
+    long long tile_off;    // offset into assignment tiles (nb^3 TILE^3)
+    // work-item offsets of the mesh passes (prefix sums over replicas)
+    int wa_off;            // x-R2C / x-C2R items: M * M/(2 PENCIL)
+    int wb_off;            // y-line items: (M/2+1) * M/PENCIL
+    int wc_off;            // z-line items: (M/2+1) * M/PENCIL
+    int blk_off;           // offset of this replica's particle blocks (PBLK each)
+    double L, kappa, alpha, rc, cellw, h, dt, t_desired, af, uf, kf;
+    double inv_cellw, inv_h, inv_L, inv_V;
+};
+
+template <typename T> struct V4;
+template <> struct V4<float> { using t = float4; };
+template <> struct V4<double> { using t = double4; };
+template <typename T> struct C2;
+template <> struct C2<float> { using t = float2; };
+template <> struct C2<double> { using t = double2; };
+
+template <typename T>
+__device__ __forceinline__ typename C2<T>::t make_c(T x, T y)
+{
+    typename C2<T>::t r;
+    r.x = x;
+    r.y = y;
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ typename C2<T>::t cmul(typename C2<T>::t a, typename C2<T>::t b)
+{
+    typename C2<T>::t r;
+    r.x = a.x * b.x - a.y * b.y;
+    r.y = a.x * b.y + a.y * b.x;
+    return r;
+}
+
+// Replica owning a global index: largest r with off(r) <= idx.
+template <typename F>
+__device__ __forceinline__ int find_rep(int idx, int nrep, F off)
+{
+    int lo = 0, hi = nrep - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (off(mid) <= idx) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block sum (fixed tree). All threads must call it; the result
+// is valid in thread 0. `scratch` holds >= 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double *scratch)
+{
+    v = warp_sum(v);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) scratch[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x < 32) {
+        int nw = (blockDim.x + 31) >> 5;
+        t = (lane < nw) ? scratch[lane] : 0.0;
+        t = warp_sum(t);
+    }
+    return t;
+}
+
+__device__ __forceinline__ void raise_status(int *status, int bit)
+{
+    atomicOr(status, bit);
+}
+
+// One periodic fold by a box length (positions are kept in [-L, 2L)).
+__device__ __forceinline__ double fold_box(double x, double L)
+{
+    if (x < 0.0) return x + L;
+    if (x >= L) return x - L;
+    return x;
+}
+
+__device__ __forceinline__ int fold_index(int i, int M)
+{
+    if (i < 0) return i + M;
+    if (i >= M) return i - M;
+    return i;
+}
+
+// PP cell and mesh brick of a particle (see p3m_sort.cu). Raises ST_BOX and
+// files the particle under cell 0 when it is outside [-L, 2L) or not finite.
+__device__ __forceinline__ void particle_keys(const RepDev &R, double x, double y, double z,
+                                              int has_mesh, int *cell, int *brick, int *status)
+{
+    const double L = R.L;
+    const bool ok = (x >= -L && x < 2.0 * L) && (y >= -L && y < 2.0 * L) && (z >= -L && z < 2.0 * L);
+    if (!ok) {
+        raise_status(status, ST_BOX);
+        x = y = z = 0.0;
+    }
+    const double xw = fold_box(x, L), yw = fold_box(y, L), zw = fold_box(z, L);
+    const int cx = min((int)floor(xw / R.cellw), R.nc - 1);
+    const int cy = min((int)floor(yw / R.cellw), R.nc - 1);
+    const int cz = min((int)floor(zw / R.cellw), R.nc - 1);
+    *cell = R.cell_off + cx + R.nc * (cy + R.nc * cz);
+    *brick = -1;
+    if (has_mesh && R.M > 0) {
+        const int ix = fold_index((int)floor(x / R.h), R.M);
+        const int iy = fold_index((int)floor(y / R.h), R.M);
+        const int iz = fold_index((int)floor(z / R.h), R.M);
+        *brick = R.brick_off + ix / BRICK + R.nb * (iy / BRICK + R.nb * (iz / BRICK));
+    }
+}
+
+}  // namespace p3m

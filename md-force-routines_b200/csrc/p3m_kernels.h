@@ -1,0 +1,98 @@
+// Host-side launchers of the p3m_b200 kernels (internal to the library).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "p3m_common.cuh"
+
+namespace p3m {
+
+// Device arrays of one context, shared by all launchers. Particle arrays are
+// concatenated over replicas in replica order; cell, brick and mesh arrays
+// likewise. `T` selects the precision of the bulk buffers (void* here).
+struct DevState {
+    int nrep = 0, ntot = 0, ncell = 0, nbrick = 0;
+    long long nmesh = 0, nspec = 0, ntile = 0;
+    int wa = 0, wb = 0, wc = 0;  // total work items of the mesh passes
+    int pp_split = 1;            // CTAs per PP cell (autotuned)
+    int pp_tpi = 1;              // threads per i-particle in the PP loop
+    int has_mesh = 0;
+    int max_mesh = 0;            // largest M over replicas
+    int nblk = 0;                // replica-aligned particle blocks (PBLK each)
+    RepDev *reps = nullptr;      // [nrep]
+    // particle state, FP64 (ntot,3) row-major in original order
+    double *pos = nullptr, *vel = nullptr, *acc = nullptr, *charge = nullptr;
+    int *prep = nullptr;         // particle -> replica
+    // cell sort
+    int *cell_key = nullptr, *cell_count = nullptr, *cell_start = nullptr;
+    int *cell_cursor = nullptr, *cell_tmp = nullptr, *cell_perm = nullptr, *cell_slot = nullptr;
+    void *xs_cell = nullptr;     // V4<T> sorted positions relative to the cell origin
+    void *acc_pp = nullptr;      // V4<T> PP acceleration, cell-sorted order
+    // brick sort
+    int *brick_key = nullptr, *brick_count = nullptr, *brick_start = nullptr;
+    int *brick_cursor = nullptr, *brick_perm = nullptr, *brick_slot = nullptr;
+    // mesh
+    unsigned long long *tiles = nullptr;  // fixed-point assignment tiles (int64)
+    void *spec = nullptr;        // C2<T> half spectrum rho_k / phi_k, [kx][z][y]
+    void *ek = nullptr;          // C2<T> 3 field spectra, [3][kx][z][y]
+    void *green = nullptr;       // T influence function / V, [kx][z][y]
+    void *efield = nullptr;      // T 3 real field meshes [3][z][y][x]
+    void *acc_pm = nullptr;      // V4<T> PM acceleration, brick-sorted order
+    void *twiddle = nullptr;     // C2<T> exp(-2 pi i k / 256), k < 128
+    // reductions
+    double *u_pp_part = nullptr;  // [ncell * pp_split]
+    double *u_pm_part = nullptr;  // [wc]
+    double *kin_part = nullptr;   // per particle block
+    double *rep_out = nullptr;    // [nrep * 8] per-replica scalars of the last step
+    int *status = nullptr;
+};
+
+enum RepOut { RO_UPP = 0, RO_UPM = 1, RO_USELF = 2, RO_U = 3, RO_K = 4, RO_T = 5, RO_FACT = 6 };
+
+// fixed-point scale of the deterministic charge assignment
+constexpr double ASSIGN_SCALE = 1099511627776.0;  // 2^40
+
+template <typename T> void configure_pp_kernels();
+template <typename T> void configure_mesh_kernels();
+template <typename T> void launch_keys(const DevState &s, cudaStream_t st);
+void launch_scan(const DevState &s, cudaStream_t st);
+void launch_scatter(const DevState &s, cudaStream_t st);
+template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st);
+template <typename T> void launch_pp(const DevState &s, cudaStream_t st);
+void launch_reduce_pp(const DevState &s, cudaStream_t st);
+
+template <typename T> void launch_assign(const DevState &s, cudaStream_t st);
+template <typename T> void launch_fft_forward(const DevState &s, cudaStream_t st);
+template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st);
+template <typename T> void launch_gather(const DevState &s, cudaStream_t st);
+void launch_reduce_pm(const DevState &s, cudaStream_t st);
+
+template <typename T> void launch_green_from_host_layout(const DevState &s, int rep,
+                                                         const double *gk_dev,
+                                                         cudaStream_t st);
+template <typename T> void launch_tiles_to_mesh(const DevState &s, int rep, double *rho,
+                                                cudaStream_t st);
+template <typename T> void launch_efield_from_mesh(const DevState &s, int rep,
+                                                   const double *ex, const double *ey,
+                                                   const double *ez, cudaStream_t st);
+void launch_gf_opt(double kappa, double alpha, int p, int m_alias, int M, double L,
+                   double *G_k, double *a_part, cudaStream_t st);
+
+void launch_kick_drift(const DevState &s, cudaStream_t st);
+template <typename T> void launch_kick_finish(const DevState &s, int do_kick, double *ep_out,
+                                              cudaStream_t st);
+void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring, int ring_cap,
+                        cudaStream_t st);
+void launch_set_counters(int *counters, int run_step, int ring_pos, int it0, cudaStream_t st);
+void launch_scale_vel(const DevState &s, cudaStream_t st);
+template <typename T> void launch_combine(const DevState &s, int use_pp, int use_pm, int scale_af,
+                                          double *out, double *ep_out, cudaStream_t st);
+template <typename T> void launch_nqt(const DevState &s, const double *pos, const double *qmult,
+                                      int nq, double *part, double *out, const int *counters,
+                                      int ring_cap, cudaStream_t st);
+template <typename T> void configure_integrate_kernels(int max_nq);
+int gf_opt_blocks(int M);
+
+
+}  // namespace p3m

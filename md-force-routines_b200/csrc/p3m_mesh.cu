@@ -1,0 +1,626 @@
+// Particle-mesh (PM) stages: order-6 charge assignment, 3-D FFT of the
+// charge mesh, the influence-function multiply with ik differentiation, three
+// inverse FFTs of the field components and the order-6 force gather.
+//
+// This computes what yukawa_pm_ord6.py:440-484 computes:
+//   rho   = charge_assgn_6(pos)                       (:445, :6-95)
+//   rho_k = fftshift(fftn(rho)); phi_k = G_k rho_k     (:447-451)
+//   U_f   = 1/2 sum |rho_k|^2 G_k / V                  (:453-457)
+//   E     = (M^3/V) real(ifftn(ifftshift(-i k phi_k))) (:459-480)
+//   acc   = Z field_assgn_6(E, pos)                    (:482, :213-312)
+// on half spectra (R2C / C2R). Two facts make that equal to the reference's
+// full complex transforms: the real part of ifftn equals the C2R transform of
+// the Hermitian part of the spectrum, and the -i k_a multiplier of field
+// component a is anti-Hermitian on a's own Nyquist plane, where the
+// reference's real() therefore cancels it -- so it is zeroed there. U_f sums
+// the half spectrum with weight 2 off the kx = 0 and kx = M/2 planes.
+//
+// Layouts (per replica, concatenated over replicas):
+//   tiles   int64 [brick][TILE^3]   fixed-point partial charge of each brick
+//   spec    C2<T> [kx][z][y]        kx in [0, M/2], y fastest
+//   ek      C2<T> [3][kx][z][y]     field spectra
+//   green   T     [kx][z][y]        G_k / V in the same layout
+//   efield  T     [3][z][y][x]      real field meshes, x fastest
+//
+// Assignment is deterministic: each CTA owns one brick of BRICK^3 base
+// cells and accumulates its particles' 216-node stencils into a shared-memory
+// tile of TILE^3 nodes in 64-bit fixed point (scale 2^40), so the sum does
+// not depend on the order in which threads add. Overlapping tile halos are
+// summed (again as integers) when the first FFT pass reads the mesh.
+//
+// The FFT is an in-place radix-2 decimation-in-time transform of 16 lines
+// at a time held in shared memory ([element][line], line stride padded to
+// 17), the input permuted to bit-reversed order as it is loaded. Twiddles
+// exp(-2 pi i k/256) come from an FP64-accurate table.
+#include "p3m_kernels.h"
+
+namespace p3m {
+
+constexpr int FFT_THREADS = 256;
+constexpr int LS = PENCIL + 1;  // padded line stride of the shared tiles
+
+template <typename T> using cplx = typename C2<T>::t;
+
+__device__ __forceinline__ int brev(int n, int logM) { return (int)(__brev((unsigned)n) >> (32 - logM)); }
+
+// signed frequency of index n on an M-point axis
+__device__ __forceinline__ int freq(int n, int M) { return n < (M >> 1) ? n : n - M; }
+
+template <typename T>
+__device__ __forceinline__ void load_twiddles(cplx<T> *tw, const cplx<T> *g)
+{
+    for (int k = threadIdx.x; k < 128; k += blockDim.x) tw[k] = g[k];
+}
+
+// In-place DIT FFT of PENCIL lines of length 2^logM: element n of line l at
+// buf[n * LS + l], input in bit-reversed order, output in natural order.
+// Unnormalised; inverse uses conjugate twiddles. Ends with a barrier.
+template <typename T>
+__device__ void fft_pencil(cplx<T> *buf, int logM, const cplx<T> *tw, bool inverse)
+{
+    const int M = 1 << logM;
+    const int nb = PENCIL * (M >> 1);
+    for (int s = 0; s < logM; ++s) {
+        const int half = 1 << s;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            const int l = b & (PENCIL - 1), j = b >> 4;
+            const int k = j & (half - 1);
+            const int i0 = ((j >> s) << (s + 1)) + k, i1 = i0 + half;
+            cplx<T> w = tw[k << (7 - s)];
+            if (inverse) w.y = -w.y;
+            cplx<T> a = buf[i0 * LS + l], c = buf[i1 * LS + l];
+            cplx<T> t = cmul<T>(w, c);
+            buf[i0 * LS + l] = make_c<T>(a.x + t.x, a.y + t.y);
+            buf[i1 * LS + l] = make_c<T>(a.x - t.x, a.y - t.y);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Charge assignment
+// ---------------------------------------------------------------------------
+
+// Order-6 weights at node offset x (yukawa_pm_ord6.py:29-34).
+template <typename T>
+__device__ __forceinline__ void weights6(T x, T *w)
+{
+    T x2 = x * x, x3 = x2 * x, x4 = x3 * x, x5 = x4 * x;
+    w[0] = ((T)1 - (T)10 * x + (T)40 * x2 - (T)80 * x3 + (T)80 * x4 - (T)32 * x5) / (T)3840;
+    w[1] = ((T)237 - (T)750 * x + (T)840 * x2 - (T)240 * x3 - (T)240 * x4 + (T)160 * x5) / (T)3840;
+    w[2] = ((T)841 - (T)770 * x - (T)440 * x2 + (T)560 * x3 + (T)80 * x4 - (T)160 * x5) / (T)1920;
+    w[3] = ((T)841 + (T)770 * x - (T)440 * x2 - (T)560 * x3 + (T)80 * x4 + (T)160 * x5) / (T)1920;
+    w[4] = ((T)237 + (T)750 * x + (T)840 * x2 + (T)240 * x3 - (T)240 * x4 - (T)160 * x5) / (T)3840;
+    w[5] = ((T)1 + (T)10 * x + (T)40 * x2 + (T)80 * x3 + (T)80 * x4 + (T)32 * x5) / (T)3840;
+}
+
+// Base index (unwrapped) and offset along one axis (yukawa_pm_ord6.py:17-27).
+__device__ __forceinline__ int base_offset(double p, double h, double &off)
+{
+    int ix = (int)floor(p / h);
+    off = (p - (ix + 0.5) * h) / h;
+    return ix;
+}
+
+__device__ __forceinline__ int wrapM(int i, int M)
+{
+    i %= M;
+    return i < 0 ? i + M : i;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_assign(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_start,
+         const int *__restrict__ brick_perm, const double *__restrict__ pos,
+         const double *__restrict__ charge, unsigned long long *__restrict__ tiles, int nbrick)
+{
+    extern __shared__ __align__(16) unsigned long long tile[];
+    for (int b = blockIdx.x; b < nbrick; b += gridDim.x) {
+        const int r = find_rep(b, nrep, [&](int k) { return reps[k].brick_off; });
+        const RepDev &R = reps[r];
+        const int nb = R.nb, M = R.M, local = b - R.brick_off;
+        const int bx = (local % nb) * BRICK, by = ((local / nb) % nb) * BRICK,
+                  bz = (local / (nb * nb)) * BRICK;
+        __syncthreads();
+        for (int k = threadIdx.x; k < TILE3; k += blockDim.x) tile[k] = 0ull;
+        __syncthreads();
+        const int p0 = brick_start[b], p1 = brick_start[b + 1];
+        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+            const int i = brick_perm[p];
+            double ox, oy, oz;
+            int ix = base_offset(pos[3 * i + 0], R.h, ox);
+            int iy = base_offset(pos[3 * i + 1], R.h, oy);
+            int iz = base_offset(pos[3 * i + 2], R.h, oz);
+            const int lx = wrapM(ix, M) - bx, ly = wrapM(iy, M) - by, lz = wrapM(iz, M) - bz;
+            // a particle outside [-L, 2L) was filed under brick 0 by the key
+            // pass (and flagged there); it must not reach outside this tile
+            if ((unsigned)lx >= (unsigned)BRICK || (unsigned)ly >= (unsigned)BRICK ||
+                (unsigned)lz >= (unsigned)BRICK)
+                continue;
+            T wx[6], wy[6], wz[6];
+            weights6<T>((T)ox, wx);
+            weights6<T>((T)oy, wy);
+            weights6<T>((T)oz, wz);
+            const T q = (T)charge[i];
+#pragma unroll
+            for (int g = 0; g < 6; ++g) {
+#pragma unroll
+                for (int a = 0; a < 6; ++a) {
+                    const T qzy = q * wz[g] * wy[a];
+                    unsigned long long *row = &tile[((lz + g) * TILE + (ly + a)) * TILE + lx];
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) {
+                        double v = (double)(qzy * wx[c]) * ASSIGN_SCALE;
+                        atomicAdd(row + c, (unsigned long long)__double2ll_rn(v));
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        unsigned long long *dst = tiles + R.tile_off + (long long)local * TILE3;
+        for (int k = threadIdx.x; k < TILE3; k += blockDim.x) dst[k] = tile[k];
+    }
+}
+
+// Charge on node (x,y,z) of replica R: the integer sum of the (up to 8)
+// brick tiles that cover it, converted from fixed point.
+__device__ __forceinline__ long long rho_fixed(const RepDev &R,
+                                               const unsigned long long *__restrict__ tiles,
+                                               int x, int y, int z)
+{
+    const int nb = R.nb;
+    const int bx = x / BRICK, by = y / BRICK, bz = z / BRICK;
+    const int ox = x - bx * BRICK, oy = y - by * BRICK, oz = z - bz * BRICK;
+    unsigned long long s = 0;
+    const int ndx = ox < HALO ? 2 : 1, ndy = oy < HALO ? 2 : 1, ndz = oz < HALO ? 2 : 1;
+    for (int dz = 0; dz < ndz; ++dz) {
+        const int tz = oz + dz * BRICK, cz = (bz - dz + nb) % nb;
+        for (int dy = 0; dy < ndy; ++dy) {
+            const int ty = oy + dy * BRICK, cy = (by - dy + nb) % nb;
+            for (int dx = 0; dx < ndx; ++dx) {
+                const int tx = ox + dx * BRICK, cx = (bx - dx + nb) % nb;
+                const long long brick = cx + nb * (cy + (long long)nb * cz);
+                s += tiles[R.tile_off + brick * TILE3 + (tz * TILE + ty) * TILE + tx];
+            }
+        }
+    }
+    return (long long)s;
+}
+
+// ---------------------------------------------------------------------------
+// FFT passes
+// ---------------------------------------------------------------------------
+
+// Pass A: rows of the charge mesh (reduced from the tiles) -> R2C along x,
+// written transposed into spec[kx][z][y]. Item = (replica, z, 32-row tile);
+// two real rows share one complex line.
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS)
+k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const unsigned long long *__restrict__ tiles,
+            cplx<T> *__restrict__ spec, const cplx<T> *__restrict__ twg, int nitems)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *tw = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *buf = tw + 128;
+    load_twiddles<T>(tw, twg);
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int r = find_rep(item, nrep, [&](int k) { return reps[k].wa_off; });
+        const RepDev &R = reps[r];
+        const int M = R.M, logM = R.logM, w = item - R.wa_off;
+        const int nyt = M / (2 * PENCIL);
+        const int z = w / nyt, y0 = (w % nyt) * (2 * PENCIL);
+        __syncthreads();
+        for (int e = threadIdx.x; e < 2 * PENCIL * M; e += blockDim.x) {
+            const int x = e % M, j = e / M;
+            const long long f = rho_fixed(R, tiles, x, y0 + j, z);
+            const T v = (T)((double)f * (1.0 / ASSIGN_SCALE));
+            T *dst = reinterpret_cast<T *>(&buf[brev(x, logM) * LS + (j >> 1)]);
+            dst[j & 1] = v;
+        }
+        __syncthreads();
+        fft_pencil<T>(buf, logM, tw, false);
+        // split the two real rows: Xa = (Z[k] + conj Z[M-k])/2, Xb = (Z[k] - conj Z[M-k])/2i
+        const int nk = (M >> 1) + 1;
+        cplx<T> *out = spec + R.spec_off;
+        for (int e = threadIdx.x; e < 2 * PENCIL * nk; e += blockDim.x) {
+            const int j = e & (2 * PENCIL - 1), k = e >> 5;
+            const int l = j >> 1;
+            const cplx<T> Z = buf[k * LS + l];
+            const cplx<T> Zm = buf[((M - k) & (M - 1)) * LS + l];
+            cplx<T> X;
+            if ((j & 1) == 0) {
+                X.x = (T)0.5 * (Z.x + Zm.x);
+                X.y = (T)0.5 * (Z.y - Zm.y);
+            } else {
+                X.x = (T)0.5 * (Z.y + Zm.y);
+                X.y = (T)0.5 * (Zm.x - Z.x);
+            }
+            out[((long long)k * M + z) * M + y0 + j] = X;
+        }
+    }
+}
+
+// Passes B / D: FFT along y of contiguous lines spec[kx][z][:]. Item =
+// (replica, [component,] kx, 16-line z tile). `ncomp` arrays of `stride`
+// elements are processed (1 forward, 3 inverse).
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS)
+k_fft_y(const RepDev *__restrict__ reps, int nrep, cplx<T> *__restrict__ data, long long stride,
+        int ncomp, const cplx<T> *__restrict__ twg, int nitems_per_comp, bool inverse)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *tw = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *buf = tw + 128;
+    load_twiddles<T>(tw, twg);
+    for (int item = blockIdx.x; item < nitems_per_comp * ncomp; item += gridDim.x) {
+        const int comp = item / nitems_per_comp, it = item % nitems_per_comp;
+        const int r = find_rep(it, nrep, [&](int k) { return reps[k].wb_off; });
+        const RepDev &R = reps[r];
+        const int M = R.M, logM = R.logM, w = it - R.wb_off;
+        const int nzt = M / PENCIL;
+        const int kx = w / nzt, z0 = (w % nzt) * PENCIL;
+        cplx<T> *base = data + comp * stride + R.spec_off + ((long long)kx * M + z0) * M;
+        __syncthreads();
+        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
+            const int y = e % M, l = e / M;
+            buf[brev(y, logM) * LS + l] = base[(long long)l * M + y];
+        }
+        __syncthreads();
+        fft_pencil<T>(buf, logM, tw, inverse);
+        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
+            const int y = e % M, l = e / M;
+            base[(long long)l * M + y] = buf[y * LS + l];
+        }
+    }
+}
+
+// Pass C: forward FFT along z, U_f partial, phi = (G/V) rho_k, then the three
+// field spectra with their inverse z transforms. E_z = IFFT_z(-i kz phi);
+// E_x and E_y use psi = IFFT_z(phi) since their multipliers are constant
+// along z: E_x = -i kx psi, E_y = -i ky psi. Item = (replica, kx, 16-wide y
+// tile).
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS)
+k_fft_z_green(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict__ spec,
+              const T *__restrict__ green, cplx<T> *__restrict__ ek, long long nspec,
+              double *__restrict__ u_part, const cplx<T> *__restrict__ twg, int nitems)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *tw = reinterpret_cast<cplx<T> *>(smem_raw);
+    __shared__ double red[32];
+    load_twiddles<T>(tw, twg);
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int r = find_rep(item, nrep, [&](int k) { return reps[k].wc_off; });
+        const RepDev &R = reps[r];
+        const int M = R.M, logM = R.logM, w = item - R.wc_off;
+        cplx<T> *buf = tw + 128;
+        cplx<T> *buf2 = buf + M * LS;
+        const int nyt = M / PENCIL;
+        const int kx = w / nyt, y0 = (w % nyt) * PENCIL;
+        const long long lbase = R.spec_off + (long long)kx * M * M + y0;  // + z*M + l
+        __syncthreads();
+        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
+            const int l = e & (PENCIL - 1), z = e >> 4;
+            buf[brev(z, logM) * LS + l] = spec[lbase + (long long)z * M + l];
+        }
+        __syncthreads();
+        fft_pencil<T>(buf, logM, tw, false);
+        const double wkx = (kx == 0 || kx == (M >> 1)) ? 1.0 : 2.0;
+        double u = 0.0;
+        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
+            const int l = e & (PENCIL - 1), n = e >> 4;
+            const cplx<T> rk = buf[n * LS + l];
+            const T g = green[lbase + (long long)n * M + l];
+            u += wkx * (double)g * ((double)rk.x * rk.x + (double)rk.y * rk.y);
+            buf2[brev(n, logM) * LS + l] = make_c<T>(g * rk.x, g * rk.y);
+        }
+        __syncthreads();
+        const T twopi_L = (T)(6.283185307179586477 * R.inv_L);
+        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
+            const int l = e & (PENCIL - 1), n = e >> 4;
+            const int br = brev(n, logM);
+            const cplx<T> ph = buf2[br * LS + l];
+            const T kz = (n == (M >> 1)) ? (T)0 : twopi_L * (T)freq(n, M);
+            // -i kz phi = (kz phi.y, -kz phi.x)
+            buf[br * LS + l] = make_c<T>(kz * ph.y, -kz * ph.x);
+        }
+        __syncthreads();
+        fft_pencil<T>(buf, logM, tw, true);   // E_z
+        fft_pencil<T>(buf2, logM, tw, true);  // psi
+        const T kxv = (kx == (M >> 1)) ? (T)0 : twopi_L * (T)kx;
+        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
+            const int l = e & (PENCIL - 1), z = e >> 4;
+            const int yy = y0 + l;
+            const T kyv = (yy == (M >> 1)) ? (T)0 : twopi_L * (T)freq(yy, M);
+            const cplx<T> ps = buf2[z * LS + l];
+            const long long o = lbase + (long long)z * M + l;
+            ek[o] = make_c<T>(kxv * ps.y, -kxv * ps.x);
+            ek[nspec + o] = make_c<T>(kyv * ps.y, -kyv * ps.x);
+            ek[2 * nspec + o] = buf[z * LS + l];
+        }
+        const double ut = block_sum(u, red);
+        if (threadIdx.x == 0) u_part[item] = ut;
+    }
+}
+
+// Pass E: C2R along x of the three field spectra, written as real meshes
+// efield[c][z][y][x]. Item = (replica, component, z, 32-row tile); rows
+// 2l and 2l+1 share complex line l: Z[k] = Xa[k] + i Xb[k] over the
+// Hermitian extension, with the imaginary parts at k = 0 and M/2 dropped.
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS)
+k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict__ ek,
+            long long nspec, T *__restrict__ efield, long long nmesh,
+            const cplx<T> *__restrict__ twg, int nitems_per_comp)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *tw = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *buf = tw + 128;
+    load_twiddles<T>(tw, twg);
+    for (int item = blockIdx.x; item < nitems_per_comp * 3; item += gridDim.x) {
+        const int comp = item / nitems_per_comp, it = item % nitems_per_comp;
+        const int r = find_rep(it, nrep, [&](int k) { return reps[k].wa_off; });
+        const RepDev &R = reps[r];
+        const int M = R.M, logM = R.logM, w = it - R.wa_off;
+        const int nyt = M / (2 * PENCIL);
+        const int z = w / nyt, y0 = (w % nyt) * (2 * PENCIL);
+        const cplx<T> *src = ek + comp * nspec + R.spec_off;
+        const int nk = (M >> 1) + 1;
+        __syncthreads();
+        for (int e = threadIdx.x; e < PENCIL * nk; e += blockDim.x) {
+            const int l = e & (PENCIL - 1), k = e >> 4;
+            const long long o = ((long long)k * M + z) * M + y0 + 2 * l;
+            const cplx<T> a = src[o], b = src[o + 1];
+            if (k == 0 || k == (M >> 1)) {
+                buf[brev(k, logM) * LS + l] = make_c<T>(a.x, b.x);
+            } else {
+                buf[brev(k, logM) * LS + l] = make_c<T>(a.x - b.y, a.y + b.x);
+                buf[brev(M - k, logM) * LS + l] = make_c<T>(a.x + b.y, b.x - a.y);
+            }
+        }
+        __syncthreads();
+        fft_pencil<T>(buf, logM, tw, true);
+        T *dst = efield + comp * nmesh + R.mesh_off + ((long long)z * M + y0) * M;
+        for (int e = threadIdx.x; e < 2 * PENCIL * M; e += blockDim.x) {
+            const int x = e % M, j = e / M;
+            const cplx<T> v = buf[x * LS + (j >> 1)];
+            dst[(long long)j * M + x] = (j & 1) ? v.y : v.x;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Gather
+// ---------------------------------------------------------------------------
+
+// Field at each particle (brick-sorted order): E = sum over the 216 stencil
+// nodes of E[node] wz wy wx (yukawa_pm_ord6.py:298-300). Written as
+// (Ex, Ey, Ez, Z) so the caller forms acc = Z E (:308-310).
+template <typename T>
+__global__ void __launch_bounds__(128)
+k_gather(const RepDev *__restrict__ reps, const int *__restrict__ prep,
+         const int *__restrict__ brick_perm, const double *__restrict__ pos,
+         const double *__restrict__ charge, const T *__restrict__ efield, long long nmesh,
+         typename V4<T>::t *__restrict__ acc_pm, int ntot)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ntot; p += gridDim.x * blockDim.x) {
+        const int i = brick_perm[p];
+        const RepDev &R = reps[prep[i]];
+        if (R.M == 0) continue;
+        const int M = R.M;
+        double ox, oy, oz;
+        const int ix = base_offset(pos[3 * i + 0], R.h, ox);
+        const int iy = base_offset(pos[3 * i + 1], R.h, oy);
+        const int iz = base_offset(pos[3 * i + 2], R.h, oz);
+        T wx[6], wy[6], wz[6];
+        weights6<T>((T)ox, wx);
+        weights6<T>((T)oy, wy);
+        weights6<T>((T)oz, wz);
+        int xs[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) xs[c] = wrapM(ix + c, M);
+        const T *Ex = efield + R.mesh_off;
+        const T *Ey = Ex + nmesh;
+        const T *Ez = Ey + nmesh;
+        T ex = 0, ey = 0, ez = 0;
+#pragma unroll 1
+        for (int g = 0; g < 6; ++g) {
+            const long long zo = (long long)wrapM(iz + g, M) * M;
+#pragma unroll
+            for (int a = 0; a < 6; ++a) {
+                const long long ro = (zo + wrapM(iy + a, M)) * M;
+                const T wzy = wz[g] * wy[a];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    const long long o = ro + xs[c];
+                    const T wgt = wzy * wx[c];
+                    ex += __ldg(Ex + o) * wgt;
+                    ey += __ldg(Ey + o) * wgt;
+                    ez += __ldg(Ez + o) * wgt;
+                }
+            }
+        }
+        typename V4<T>::t out;
+        out.x = ex;
+        out.y = ey;
+        out.z = ez;
+        out.w = (T)charge[i];
+        acc_pm[p] = out;
+    }
+}
+
+// Per-replica U_f = 1/2 sum over the replica's pass-C partials.
+__global__ void k_reduce_pm(const RepDev *__restrict__ reps, int nrep,
+                            const double *__restrict__ u_part, int wc_total,
+                            double *__restrict__ rep_out)
+{
+    const int lane = threadIdx.x & 31;
+    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nrep;
+         r += gridDim.x * (blockDim.x >> 5)) {
+        if (reps[r].M == 0) {
+            if (lane == 0) rep_out[8 * r + RO_UPM] = 0.0;
+            continue;
+        }
+        const int b = reps[r].wc_off, e = (r + 1 < nrep) ? reps[r + 1].wc_off : wc_total;
+        double t = 0.0;
+        for (int k = b + lane; k < e; k += 32) t += u_part[k];
+        t = warp_sum(t);
+        if (lane == 0) rep_out[8 * r + RO_UPM] = 0.5 * t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Conversions used by the compat entry points
+// ---------------------------------------------------------------------------
+
+// Influence function from the reference's fftshifted (M,M,M) FP64 layout
+// (index n <-> k = 2 pi (n - M/2)/L) into green[kx][z][y] / V.
+template <typename T>
+__global__ void k_green_from_shifted(const RepDev *__restrict__ reps, int rep,
+                                     const double *__restrict__ gk, T *__restrict__ green)
+{
+    const RepDev &R = reps[rep];
+    const int M = R.M, h = M >> 1, nk = h + 1;
+    const long long n = (long long)nk * M * M;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(e % M), z = (int)((e / M) % M), kx = (int)(e / ((long long)M * M));
+        const int sx = (kx + h) & (M - 1), sy = (y + h) & (M - 1), sz = (z + h) & (M - 1);
+        green[R.spec_off + e] = (T)(gk[((long long)sz * M + sy) * M + sx] * R.inv_V);
+    }
+}
+
+template <typename T>
+__global__ void k_tiles_to_mesh(const RepDev *__restrict__ reps, int rep,
+                                const unsigned long long *__restrict__ tiles,
+                                double *__restrict__ rho)
+{
+    const RepDev &R = reps[rep];
+    const int M = R.M;
+    const long long n = (long long)M * M * M;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(e % M), y = (int)((e / M) % M), z = (int)(e / ((long long)M * M));
+        const long long f = rho_fixed(R, tiles, x, y, z);
+        rho[e] = (double)f * (1.0 / ASSIGN_SCALE);
+    }
+}
+
+template <typename T>
+__global__ void k_efield_from_mesh(const RepDev *__restrict__ reps, int rep,
+                                   const double *__restrict__ ex, const double *__restrict__ ey,
+                                   const double *__restrict__ ez, T *__restrict__ efield,
+                                   long long nmesh)
+{
+    const RepDev &R = reps[rep];
+    const long long n = (long long)R.M * R.M * R.M;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        efield[R.mesh_off + e] = (T)ex[e];
+        efield[nmesh + R.mesh_off + e] = (T)ey[e];
+        efield[2 * nmesh + R.mesh_off + e] = (T)ez[e];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+template <typename T> static size_t fft_smem(int maxM, int nbuf)
+{
+    return (128 + (size_t)nbuf * maxM * LS) * sizeof(cplx<T>);
+}
+
+template <typename K> static void set_smem(K kernel, size_t bytes)
+{
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+static int grid_items(int n, int cap = 148 * 8) { return n < cap ? (n > 0 ? n : 1) : cap; }
+
+template <typename T> void configure_mesh_kernels()
+{
+    set_smem(k_assign<T>, TILE3 * sizeof(unsigned long long));
+    set_smem(k_fft_x_r2c<T>, fft_smem<T>(256, 1));
+    set_smem(k_fft_y<T>, fft_smem<T>(256, 1));
+    set_smem(k_fft_z_green<T>, fft_smem<T>(256, 2));
+    set_smem(k_fft_x_c2r<T>, fft_smem<T>(256, 1));
+}
+
+template <typename T> void launch_assign(const DevState &s, cudaStream_t st)
+{
+    const size_t smem = TILE3 * sizeof(unsigned long long);
+    k_assign<T><<<grid_items(s.nbrick, 148 * 16), 256, smem, st>>>(
+        s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, s.tiles, s.nbrick);
+}
+
+template <typename T> void launch_fft_forward(const DevState &s, cudaStream_t st)
+{
+    using C = cplx<T>;
+    const int maxM = s.max_mesh;
+    const size_t sm1 = fft_smem<T>(maxM, 1), sm2 = fft_smem<T>(maxM, 2);
+    k_fft_x_r2c<T><<<grid_items(s.wa), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, s.tiles, (C *)s.spec,
+                                                                (const C *)s.twiddle, s.wa);
+    k_fft_y<T><<<grid_items(s.wb), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, (C *)s.spec, s.nspec, 1,
+                                                            (const C *)s.twiddle, s.wb, false);
+    k_fft_z_green<T><<<grid_items(s.wc), FFT_THREADS, sm2, st>>>(
+        s.reps, s.nrep, (const C *)s.spec, (const T *)s.green, (C *)s.ek, s.nspec, s.u_pm_part,
+        (const C *)s.twiddle, s.wc);
+}
+
+template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st)
+{
+    using C = cplx<T>;
+    const size_t sm1 = fft_smem<T>(s.max_mesh, 1);
+    k_fft_y<T><<<grid_items(3 * s.wb), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, (C *)s.ek, s.nspec, 3,
+                                                                (const C *)s.twiddle, s.wb, true);
+    k_fft_x_c2r<T><<<grid_items(3 * s.wa), FFT_THREADS, sm1, st>>>(
+        s.reps, s.nrep, (const C *)s.ek, s.nspec, (T *)s.efield, s.nmesh, (const C *)s.twiddle,
+        s.wa);
+}
+
+template <typename T> void launch_gather(const DevState &s, cudaStream_t st)
+{
+    k_gather<T><<<grid_items((s.ntot + 127) / 128, 148 * 16), 128, 0, st>>>(
+        s.reps, s.prep, s.brick_perm, s.pos, s.charge, (const T *)s.efield, s.nmesh,
+        (typename V4<T>::t *)s.acc_pm, s.ntot);
+}
+
+void launch_reduce_pm(const DevState &s, cudaStream_t st)
+{
+    k_reduce_pm<<<(s.nrep + 3) / 4, 128, 0, st>>>(s.reps, s.nrep, s.u_pm_part, s.wc, s.rep_out);
+}
+
+template <typename T>
+void launch_green_from_host_layout(const DevState &s, int rep, const double *gk_dev, cudaStream_t st)
+{
+    k_green_from_shifted<T><<<592, 256, 0, st>>>(s.reps, rep, gk_dev, (T *)s.green);
+}
+
+template <typename T> void launch_tiles_to_mesh(const DevState &s, int rep, double *rho, cudaStream_t st)
+{
+    k_tiles_to_mesh<T><<<592, 256, 0, st>>>(s.reps, rep, s.tiles, rho);
+}
+
+template <typename T>
+void launch_efield_from_mesh(const DevState &s, int rep, const double *ex, const double *ey,
+                             const double *ez, cudaStream_t st)
+{
+    k_efield_from_mesh<T><<<592, 256, 0, st>>>(s.reps, rep, ex, ey, ez, (T *)s.efield, s.nmesh);
+}
+
+#define P3M_INST(T)                                                                        \
+    template void configure_mesh_kernels<T>();                                              \
+    template void launch_assign<T>(const DevState &, cudaStream_t);                         \
+    template void launch_fft_forward<T>(const DevState &, cudaStream_t);                    \
+    template void launch_fft_inverse<T>(const DevState &, cudaStream_t);                    \
+    template void launch_gather<T>(const DevState &, cudaStream_t);                         \
+    template void launch_green_from_host_layout<T>(const DevState &, int, const double *,   \
+                                                   cudaStream_t);                          \
+    template void launch_tiles_to_mesh<T>(const DevState &, int, double *, cudaStream_t);   \
+    template void launch_efield_from_mesh<T>(const DevState &, int, const double *,         \
+                                             const double *, const double *, cudaStream_t);
+P3M_INST(float)
+P3M_INST(double)
+
+}  // namespace p3m

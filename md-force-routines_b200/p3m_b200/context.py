@@ -1,0 +1,291 @@
+"""Python wrapper of a p3m_b200 context (one or more replicas on one GPU)."""
+from __future__ import annotations
+
+import ctypes
+import os
+from collections import OrderedDict
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import FP32, FP64, MODE_NVE, MODE_THERMOSTAT, P3MError, ReplicaDesc, check, dptr, lib
+
+
+@dataclass
+class Replica:
+    """One independent system: the constants of yukawa_MD_p3m_ord6.py:26-79."""
+
+    N: int
+    L: float
+    kappa: float
+    alpha: float
+    rc: float
+    M: int = 0
+    dt: float = 0.1
+    T_desired: float = 0.01
+    af: float = 1.0 / 3.0
+    uf: float = 1.0
+    kf: float = 1.5
+    p: int = 6
+    m_alias: int = 3
+    seed: int = field(default=0, compare=False)
+
+    def desc(self) -> ReplicaDesc:
+        return ReplicaDesc(int(self.N), int(self.M), int(self.p), int(self.m_alias),
+                           float(self.L), float(self.kappa), float(self.alpha), float(self.rc),
+                           float(self.dt), float(self.T_desired), float(self.af),
+                           float(self.uf), float(self.kf))
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None and a.shape != shape:
+        a = a.reshape(shape)
+    return a
+
+
+class Context:
+    """Device buffers, stream and CUDA graphs for a batch of replicas."""
+
+    def __init__(self, replicas, precision=FP32, device=0):
+        if isinstance(replicas, Replica):
+            replicas = [replicas]
+        self.replicas = list(replicas)
+        self.precision = precision
+        self.device = device
+        R = len(self.replicas)
+        arr = (ReplicaDesc * R)(*[r.desc() for r in self.replicas])
+        h = ctypes.c_void_p()
+        rc = lib().p3m_create(arr, R, int(precision), int(device), ctypes.byref(h))
+        check(rc, None)
+        self._h = h
+        self._green_key = [None] * R
+
+    # -- lifetime -------------------------------------------------------------
+    @property
+    def handle(self):
+        if self._h is None:
+            raise P3MError(-6, "context is closed")
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib().p3m_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _ck(self, rc):
+        return check(rc, self.handle)
+
+    # -- compat calls (single replica) -----------------------------------------
+    def pp(self, pos):
+        """yukawa_pp.particle_particle -> (U, acc)."""
+        pos = _f64(pos)
+        acc = np.empty_like(pos)
+        U = np.zeros(1)
+        self._ck(lib().p3m_pp(self.handle, 0, dptr(pos), dptr(acc), dptr(U)))
+        return float(U[0]), acc
+
+    def assign(self, pos, Z=None):
+        """charge_assgn_6_numba -> rho (M,M,M)."""
+        M = self.replicas[0].M
+        pos = _f64(pos)
+        rho = np.empty((M, M, M))
+        self._ck(lib().p3m_assign(self.handle, 0, dptr(pos), dptr(None if Z is None else _f64(Z)),
+                                  dptr(rho)))
+        return rho
+
+    def gather(self, pos, Z, Ex, Ey, Ez):
+        """field_assgn_6_numba -> (acc (N,3), E_p (3,N))."""
+        pos = _f64(pos)
+        n = pos.shape[0]
+        acc = np.empty((n, 3))
+        Ep = np.empty((3, n))
+        self._ck(lib().p3m_gather(self.handle, 0, dptr(pos), dptr(None if Z is None else _f64(Z)),
+                                  dptr(_f64(Ex)), dptr(_f64(Ey)), dptr(_f64(Ez)), dptr(acc),
+                                  dptr(Ep)))
+        return acc, Ep
+
+    def set_green(self, G_k=None, replica=0):
+        """Install an influence function (fftshifted (M,M,M) FP64), or compute
+        it on the device when G_k is None."""
+        self._ck(lib().p3m_set_green(self.handle, replica,
+                                     dptr(None if G_k is None else _f64(G_k))))
+
+    def set_green_cached(self, G_k, replica=0):
+        """set_green, skipped when the same array (same buffer and sampled
+        contents) was installed last."""
+        G = _f64(G_k)
+        flat = G.reshape(-1)
+        idx = np.linspace(0, flat.size - 1, 61).astype(np.int64)
+        key = (G.ctypes.data, G.shape, flat[idx].tobytes())
+        if self._green_key[replica] != key:
+            self.set_green(G, replica)
+            self._green_key[replica] = key
+
+    def pm(self, pos, Z=None, want_rho=False):
+        """particle_mesh_fft_r -> (U_f, acc (N,3), E_p (3,N), rho or None)."""
+        M = self.replicas[0].M
+        pos = _f64(pos)
+        n = pos.shape[0]
+        acc = np.empty((n, 3))
+        Ep = np.empty((3, n))
+        U = np.zeros(1)
+        rho = np.empty((M, M, M)) if want_rho else None
+        self._ck(lib().p3m_pm(self.handle, 0, dptr(pos), dptr(None if Z is None else _f64(Z)),
+                              dptr(acc), dptr(U), dptr(Ep), dptr(rho)))
+        return float(U[0]), acc, Ep, rho
+
+    def force(self, pos, Z=None):
+        """force_pot -> (U, acc, (U_short, U_fft, U_self))."""
+        pos = _f64(pos)
+        acc = np.empty_like(pos)
+        U = np.zeros(1)
+        parts = np.zeros(3)
+        self._ck(lib().p3m_force(self.handle, 0, dptr(pos), dptr(None if Z is None else _f64(Z)),
+                                 dptr(acc), dptr(U), dptr(parts)))
+        return float(U[0]), acc, tuple(float(x) for x in parts)
+
+    def update(self, pos, vel, acc):
+        """velocity_verlet update, in place on the given float64 arrays -> U."""
+        U = np.zeros(1)
+        self._ck(lib().p3m_update(self.handle, 0, dptr(pos), dptr(vel), dptr(acc), dptr(U)))
+        return float(U[0])
+
+    def vscale(self, it, pos, vel, acc):
+        """thermostat vscale, in place -> (U, T before rescale)."""
+        U = np.zeros(1)
+        T = np.zeros(1)
+        self._ck(lib().p3m_vscale(self.handle, 0, int(it), dptr(pos), dptr(vel), dptr(acc),
+                                  dptr(U), dptr(T)))
+        return float(U[0]), float(T[0])
+
+    def nqt(self, pos, qv, replica=0):
+        """One n(q,t) row: complex128 (nq, 3)."""
+        pos = _f64(pos)
+        qv = _f64(qv)
+        out = np.empty((len(qv), 3, 2))
+        self._ck(lib().p3m_nqt(self.handle, replica, dptr(pos), dptr(qv), len(qv), dptr(out)))
+        return out[..., 0] + 1j * out[..., 1]
+
+    # -- device-resident path ------------------------------------------------------
+    def set_state(self, replica, pos=None, vel=None, acc=None):
+        self._ck(lib().p3m_set_state(self.handle, replica,
+                                     dptr(None if pos is None else _f64(pos)),
+                                     dptr(None if vel is None else _f64(vel)),
+                                     dptr(None if acc is None else _f64(acc))))
+
+    def get_state(self, replica):
+        n = self.replicas[replica].N
+        pos, vel, acc = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
+        self._ck(lib().p3m_get_state(self.handle, replica, dptr(pos), dptr(vel), dptr(acc)))
+        return pos, vel, acc
+
+    def init_forces(self):
+        self._ck(lib().p3m_init_forces(self.handle))
+
+    def set_nqt(self, qmult, capacity):
+        qm = None if qmult is None or len(qmult) == 0 else _f64(qmult)
+        self._ck(lib().p3m_set_nqt(self.handle, dptr(qm), 0 if qm is None else len(qm),
+                                   int(capacity)))
+
+    def run(self, n_steps, mode=MODE_NVE, it0=0, record_nqt=False, graph=True, sync=True):
+        self._ck(lib().p3m_run(self.handle, int(n_steps), int(mode), int(it0), int(bool(record_nqt)),
+                               int(bool(graph)), int(bool(sync))))
+
+    def thermostat(self, n_steps, it0=0, **kw):
+        self.run(n_steps, MODE_THERMOSTAT, it0=it0, **kw)
+
+    def energies(self, max_steps=1 << 20):
+        """Per-step (U, K, T, factor) of every replica: (steps, R, 4)."""
+        R = len(self.replicas)
+        cap = min(max_steps, 8192)
+        out = np.empty((cap, R, 4))
+        n = ctypes.c_int()
+        self._ck(lib().p3m_get_energies(self.handle, dptr(out), cap, ctypes.byref(n)))
+        return out[: n.value]
+
+    def get_nqt(self, replica, nq, max_steps=1 << 16):
+        out = np.empty((max_steps, nq, 3, 2))
+        n = ctypes.c_int()
+        self._ck(lib().p3m_get_nqt(self.handle, replica, dptr(out), max_steps, ctypes.byref(n)))
+        o = out[: n.value]
+        return o[..., 0] + 1j * o[..., 1]
+
+    def check(self):
+        self._ck(lib().p3m_check(self.handle))
+
+    def sync(self):
+        self._ck(lib().p3m_sync(self.handle))
+
+    def launch_count(self):
+        return int(lib().p3m_launch_count(self.handle))
+
+    def stream(self):
+        return lib().p3m_stream(self.handle)
+
+    def set_pp_config(self, tpi, split):
+        self._ck(lib().p3m_set_pp_config(self.handle, int(tpi), int(split)))
+
+    def pp_config(self):
+        t, s = ctypes.c_int(), ctypes.c_int()
+        self._ck(lib().p3m_get_pp_config(self.handle, ctypes.byref(t), ctypes.byref(s)))
+        return t.value, s.value
+
+
+def gf_opt_device(kappa, alpha, p, m_alias, M, L, device=0):
+    """yukawa_gf_opt on the GPU in FP64 -> (G_k (M,M,M) fftshifted, A_pm)."""
+    G = np.empty((M, M, M))
+    A = np.zeros(1)
+    check(lib().p3m_gf_opt(int(device), float(kappa), float(alpha), int(p), int(m_alias), int(M),
+                           float(L), dptr(G), dptr(A)), None)
+    return G, float(A[0])
+
+
+# -- contexts of the compat (reference-signature) functions --------------------------
+
+_PRECISIONS = {"fp64": FP64, "fp32": FP32}
+_compat_precision = _PRECISIONS[os.environ.get("P3M_B200_PRECISION", "fp64").lower()]
+_compat_cache: "OrderedDict[tuple, Context]" = OrderedDict()
+_COMPAT_MAX = 8
+
+
+def set_compat_precision(name: str):
+    """Arithmetic of the reference-signature functions: 'fp64' (default, the
+    plain method) or 'fp32' (FP32 bulk stages, FP64 reductions)."""
+    global _compat_precision
+    _compat_precision = _PRECISIONS[name.lower()]
+
+
+def compat_precision():
+    return _compat_precision
+
+
+def compat_context(N, L, kappa, alpha, rc, M=0, dt=0.1, T_desired=0.01, af=1.0 / 3.0, uf=1.0,
+                   kf=1.5, p=6, m_alias=3):
+    key = (int(N), float(L), float(kappa), float(alpha), float(rc), int(M), float(dt),
+           float(T_desired), float(af), float(uf), float(kf), int(p), int(m_alias),
+           _compat_precision)
+    ctx = _compat_cache.get(key)
+    if ctx is None:
+        ctx = Context(Replica(N=N, L=L, kappa=kappa, alpha=alpha, rc=rc, M=M, dt=dt,
+                              T_desired=T_desired, af=af, uf=uf, kf=kf, p=p, m_alias=m_alias),
+                      precision=_compat_precision)
+        _compat_cache[key] = ctx
+        while len(_compat_cache) > _COMPAT_MAX:
+            _, old = _compat_cache.popitem(last=False)
+            old.close()
+    else:
+        _compat_cache.move_to_end(key)
+    return ctx

@@ -1,0 +1,290 @@
+"""CPU oracle for the P3M force step and integrator -- TEST INFRASTRUCTURE ONLY.
+
+This module is the checker, never the product: only ``tests/``, the smoke check
+in ``__graft_entry__.py`` and the CPU-baseline leg of ``bench.py`` import it.
+The product path (``md-force-routines_b200``) never imports anything under
+``oracle/`` and fails loudly when its CUDA library is missing.
+
+It restates, in Python 3 + numpy over the plain-C kernels of ``oracle.c``, the
+FP64 algorithm of the reference (xgdhar/MD-force-routines):
+
+* ``pp``           yukawa_pp.py:6-139            (C: oracle_pp)
+* ``assign6``      yukawa_pm_ord6.py:6-95         (C: oracle_assign6)
+* ``gather6``      yukawa_pm_ord6.py:213-312      (C: oracle_gather6)
+* ``pm``           yukawa_pm_ord6.py:440-484      (numpy FFT chain)
+* ``gf_opt``       yukawa_gf_opt.py:5-98          (C: oracle_gf_opt)
+* ``force_pot``    yukawa_p3m_ord6.py:6-29
+* ``update``       velocity_verlet_p3m_ord6.py:5-26
+* ``vscale``       thermostat_p3m_ord6.py:5-25
+* ``nqt``          yukawa_MD_p3m_ord6.py:121-137, 214-219
+* ``sqw``          s_of_q_w.py:3-20 and s_of_q_w_avg.py:5-20
+
+Pinning: ``tests/golden/*.npz`` hold the reference's own numba outputs on the
+same inputs (generated by ``tests/golden/make_golden.py``); the tests check
+this restatement against them. The reference's FFT goes through pyFFTW (FFTW
+>= 3.3, no pinned version); neither is installed here, so the FFT step here and
+in the golden vectors is numpy.fft (pocketfft) -- that library boundary is
+the one place where parity is unpinned.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    """Compile oracle.c into liboracle.so (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
+    return _LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        lib = ctypes.CDLL(_LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.oracle_pp.argtypes = [ctypes.c_int, dp, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, dp, dp]
+        lib.oracle_pp.restype = ctypes.c_int
+        lib.oracle_assign6.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, dp]
+        lib.oracle_assign6.restype = ctypes.c_int
+        lib.oracle_gather6.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, dp, dp, dp, dp, dp]
+        lib.oracle_gather6.restype = ctypes.c_int
+        lib.oracle_gf_opt.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      dp, dp]
+        lib.oracle_gf_opt.restype = None
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _c64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def pp(kappa, G, rc, Lv, pos):
+    """yukawa_pp.py:6-139 -> (U_s_r, acc_s_r)."""
+    pos = _c64(pos)
+    n = pos.shape[0]
+    acc = np.zeros((n, 3))
+    U = np.zeros(1)
+    st = _load().oracle_pp(n, _p(pos), float(Lv[0]), float(Lv[1]), float(Lv[2]),
+                           float(kappa), float(G), float(rc), _p(acc), _p(U))
+    if st != 0:
+        raise ValueError("oracle_pp: particle outside the cell grid")
+    return float(U[0]), acc
+
+
+def assign6(pos, Z, Mx, My, Mz, hx, hy, hz):
+    """yukawa_pm_ord6.py:6-95 -> rho_r (Mz,My,Mx)."""
+    pos, Z = _c64(pos), _c64(Z)
+    rho = np.zeros((Mz, My, Mx))
+    st = _load().oracle_assign6(pos.shape[0], _p(pos), _p(Z), Mx, My, Mz, hx, hy, hz, _p(rho))
+    if st != 0:
+        raise ValueError("oracle_assign6: particle outside [-L, 2L)")
+    return rho
+
+
+def gather6(pos, Z, Mx, My, Mz, hx, hy, hz, Ex, Ey, Ez):
+    """yukawa_pm_ord6.py:213-312 -> (acc (N,3), E_p (3,N))."""
+    pos, Z = _c64(pos), _c64(Z)
+    Ex, Ey, Ez = _c64(Ex), _c64(Ey), _c64(Ez)
+    n = pos.shape[0]
+    acc = np.zeros((n, 3))
+    Ep = np.zeros((3, n))
+    st = _load().oracle_gather6(n, _p(pos), _p(Z), Mx, My, Mz, hx, hy, hz,
+                                _p(Ex), _p(Ey), _p(Ez), _p(acc), _p(Ep))
+    if st != 0:
+        raise ValueError("oracle_gather6: particle outside [-L, 2L)")
+    return acc, Ep
+
+
+def gf_opt(kappa, Gew, p, mx_max, my_max, mz_max, Mx, My, Mz, hx, hy, hz, Lx, Ly, Lz):
+    """yukawa_gf_opt.py:5-98 -> (G_k, kx_v, ky_v, kz_v, A_pm)."""
+    G_k = np.zeros((Mz, My, Mx))
+    A = np.zeros(1)
+    _load().oracle_gf_opt(kappa, Gew, p, mx_max, my_max, mz_max, Mx, My, Mz,
+                          hx, hy, hz, Lx, Ly, Lz, _p(G_k), _p(A))
+    nx_mid = Mx // 2 if Mx % 2 == 0 else (Mx - 1) // 2
+    ny_mid = My // 2 if My % 2 == 0 else (My - 1) // 2
+    nz_mid = Mz // 2 if Mz % 2 == 0 else (Mz - 1) // 2
+    kx_v = 2 * np.pi * (np.arange(Mx).reshape((1, Mx)) - nx_mid) / Lx
+    ky_v = 2 * np.pi * (np.arange(My).reshape((My, 1)) - ny_mid) / Ly
+    kz_v = 2 * np.pi * (np.arange(Mz).reshape((Mz, 1, 1)) - nz_mid) / Lz
+    return G_k, kx_v, ky_v, kz_v, float(A[0])
+
+
+def pm_fields(pos, Z, G_k, kx_v, ky_v, kz_v, Mx, My, Mz, hx, hy, hz, Lx, Ly, Lz):
+    """The mesh part of yukawa_pm_ord6.py:440-480: returns (U_f, rho, E_x, E_y, E_z).
+
+    assign (:445) -> fftn + fftshift (:447-449) -> phi = G_k rho_k (:451) ->
+    U_f = 1/2 sum |rho_k|^2 G_k / V (:453-457) -> E_k = -i k phi (:459-461) ->
+    ifftshift + ifftn (:463-472) -> scale M^3/V and real part (:474-480).
+    """
+    V = Lx * Ly * Lz
+    M_V = Mx * My * Mz
+    rho = assign6(pos, Z, Mx, My, Mz, hx, hy, hz)
+    rho_k = np.fft.fftshift(np.fft.fftn(rho))
+    phi_k = G_k * rho_k
+    rho_k_sq = np.real(rho_k) * np.real(rho_k) + np.imag(rho_k) * np.imag(rho_k)
+    U_f = 0.5 * np.sum(rho_k_sq * G_k) / V
+    E = []
+    for kv in (kx_v, ky_v, kz_v):
+        E_k = -1j * kv * phi_k
+        E_r = np.fft.ifftn(np.fft.ifftshift(E_k))
+        E.append(np.real(M_V * E_r / V))
+    return float(U_f), rho, E[0], E[1], E[2]
+
+
+def pm(pos, Z, G_k, kx_v, ky_v, kz_v, Mx, My, Mz, hx, hy, hz, Lx, Ly, Lz):
+    """yukawa_pm_ord6.py:440-484 (particle_mesh_fft_r) -> (U_f, acc_f, E_p)."""
+    U_f, _, Ex, Ey, Ez = pm_fields(pos, Z, G_k, kx_v, ky_v, kz_v, Mx, My, Mz,
+                                   hx, hy, hz, Lx, Ly, Lz)
+    acc, Ep = gather6(pos, Z, Mx, My, Mz, hx, hy, hz, Ex, Ey, Ez)
+    return U_f, acc, Ep
+
+
+class Params:
+    """The run constants the reference's driver passes down the call stack
+    (yukawa_MD_p3m_ord6.py:26-79)."""
+
+    def __init__(self, N, kappa, G, rc, M, L=None, Gamma=1.0, dt=0.1, p=6, m_max=3,
+                 af=1.0 / 3.0, uf=1.0, kf=1.5):
+        self.N = int(N)
+        self.L = float(L) if L is not None else (4.0 * np.pi * N / 3.0) ** (1.0 / 3.0)
+        self.Lv = np.array([self.L] * 3)
+        self.kappa, self.G, self.rc = float(kappa), float(G), float(rc)
+        self.M = int(M)
+        self.h = self.L / self.M
+        self.Gamma = float(Gamma)
+        self.T_desired = 1.0 / self.Gamma
+        self.dt = float(dt)
+        self.p, self.m_max = int(p), int(m_max)
+        self.af, self.uf, self.kf = af, uf, kf
+        self.Z = np.ones(self.N)
+        self._gk = None
+
+    def green(self):
+        if self._gk is None:
+            M, h, L = self.M, self.h, self.L
+            self._gk = gf_opt(self.kappa, self.G, self.p, self.m_max, self.m_max,
+                              self.m_max, M, M, M, h, h, h, L, L, L)
+        return self._gk
+
+
+def force_pot(P: Params, pos):
+    """yukawa_p3m_ord6.py:6-29 -> (U, acc, (U_short, U_fft, U_self)).
+
+    acc = af*(acc_pp + acc_pm) (:21), U = uf*(U_short+U_fft+U_self) with
+    U_self = -N G / sqrt(pi) (:23-24).
+    """
+    G_k, kx_v, ky_v, kz_v, _ = P.green()
+    U_short, acc_s_r = pp(P.kappa, P.G, P.rc, P.Lv, pos)
+    M, h, L = P.M, P.h, P.L
+    U_fft, acc_fft, _ = pm(pos, P.Z, G_k, kx_v, ky_v, kz_v, M, M, M, h, h, h, L, L, L)
+    acc = P.af * (acc_s_r + acc_fft)
+    U_self = -P.N * P.G / np.sqrt(np.pi)
+    U = P.uf * (U_short + U_fft + U_self)
+    return U, acc, (U_short, U_fft, U_self)
+
+
+def wrap(P: Params, pos):
+    """Single periodic wrap of velocity_verlet_p3m_ord6.py:12-19 (vectorised;
+    the same comparisons in the same order per element)."""
+    pos = pos.copy()
+    L = P.Lv
+    hi = pos > L[None, :]
+    pos[hi] = (pos - L[None, :])[hi]
+    lo = pos < 0.0
+    pos[lo] = (pos + L[None, :])[lo]
+    return pos
+
+
+def update(P: Params, pos, vel, acc):
+    """velocity_verlet_p3m_ord6.py:5-26 -> (pos, vel, acc, U)."""
+    vel = vel + 0.5 * acc * P.dt
+    pos = pos + vel * P.dt
+    pos = wrap(P, pos)
+    U, acc, _ = force_pot(P, pos)
+    vel = vel + 0.5 * acc * P.dt
+    return pos, vel, acc, U
+
+
+def vscale(P: Params, pos, vel, acc, it):
+    """thermostat_p3m_ord6.py:5-25 -> (pos, vel, acc, U, T).
+
+    T = kf*sum(v^2)/kf/N; for it <= 1999 v *= sqrt(T_d/T), otherwise
+    v *= sqrt((20 T_d/T - 1)/20).
+    """
+    pos, vel, acc, U = update(P, pos, vel, acc)
+    K = P.kf * np.sum(vel ** 2)
+    T = K / P.kf / float(P.N)
+    if it <= 1999:
+        fact = np.sqrt(P.T_desired / T)
+    else:
+        fact = np.sqrt((20.0 * P.T_desired / T - 1.0) / 20.0)
+    vel = vel * fact
+    return pos, vel, acc, U, T
+
+
+def q_vectors_reference(L):
+    """The q list of yukawa_MD_p3m_ord6.py:122-137: (iq+1) dq {1, sqrt2, sqrt3}."""
+    dq = 2.0 * np.pi / L
+    Nq = 3 * int(2.5 / dq)
+    qv = np.zeros(Nq)
+    for iqv in range(0, Nq, 3):
+        iq = iqv / 3.0
+        qv[iqv] = (iq + 1.0) * dq
+        qv[iqv + 1] = (iq + 1.0) * np.sqrt(2.0) * dq
+        qv[iqv + 2] = (iq + 1.0) * np.sqrt(3.0) * dq
+    return qv
+
+
+def nqt(pos, qv):
+    """One row of n(q,t), yukawa_MD_p3m_ord6.py:215-219: n[iq, ax] =
+    sum_i exp(-i q x_{i,ax}) -> complex128 (Nq, 3)."""
+    out = np.zeros((len(qv), 3), dtype=np.complex128)
+    for iq, q in enumerate(qv):
+        for ax in range(3):
+            out[iq, ax] = np.sum(np.exp(-1j * q * pos[:, ax]))
+    return out
+
+
+def sqw(n_q_t, N, dt, T):
+    """s_of_q_w.py:3-20: S(q,w) = |dt FFT_t n(q,t)|^2/(N T) per axis -> (Nt, 3)."""
+    out = np.zeros((n_q_t.shape[0], 3))
+    for ax in range(3):
+        out[:, ax] = np.absolute(np.fft.fft(n_q_t[:, ax]) * dt) ** 2 / (N * T)
+    return out
+
+
+def sqw_avg(n_q_t_array, Nq, N, dt, T, stride=3):
+    """s_of_q_w_avg.py:5-20 plus the replica mean of s_of_q_w_script.py:37:
+    mean over axes of sqw() on every ``stride``-th q column, then over runs."""
+    R = n_q_t_array.shape[0]
+    out = np.zeros((R, Nq, n_q_t_array.shape[1]))
+    for j in range(R):
+        for i in range(Nq):
+            out[j, i, :] = np.mean(sqw(n_q_t_array[j][:, i * stride, :], N, dt, T), axis=1)
+    return out.mean(axis=0)

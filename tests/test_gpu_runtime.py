@@ -1,0 +1,214 @@
+"""Device-resident stepping, batching, graphs, determinism and robustness."""
+import numpy as np
+import pytest
+
+from gpu_util import oracle_params, rel_rms, replica_from_golden
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _init_state(r, seed):
+    import initialize_pos_vel
+
+    pos, vel = np.zeros((r.N, 3)), np.zeros((r.N, 3))
+    initialize_pos_vel.initial(seed, r.N, [r.L] * 3, pos, vel, r.T_desired)
+    return pos, vel
+
+
+def test_run_matches_compat_steps(golden):
+    """p3m_run (graph) == the compat vscale/update loop, bit for bit."""
+    from p3m_b200 import FP64, MODE_NVE, MODE_THERMOSTAT, Context
+
+    g = golden
+    r = replica_from_golden(g)
+    S = int(g["trace_steps"])
+    with Context(r, precision=FP64) as c:
+        c.set_green(g["G_k"])
+        c.set_state(0, g["pos0"], g["vel0"])
+        c.init_forces()
+        c.run(S, MODE_THERMOSTAT, it0=0, graph=True)
+        c.run(S, MODE_NVE, graph=True)
+        pos, vel, acc = c.get_state(0)
+        E = c.energies()
+    with Context(r, precision=FP64) as c:
+        c.set_green(g["G_k"])
+        _, a, _ = c.force(g["pos0"])
+        p, v = g["pos0"].copy(), g["vel0"].copy()
+        for it in range(S):
+            c.vscale(it, p, v, a)
+        for _ in range(S):
+            c.update(p, v, a)
+    assert np.array_equal(pos, p) and np.array_equal(vel, v) and np.array_equal(acc, a)
+    assert E.shape == (2 * S, 1, 4)
+    np.testing.assert_allclose(E[:, 0, 0], g["trace"][:, 0], rtol=1e-9)
+
+
+@pytest.mark.parametrize("prec_name", ["fp32", "fp64"])
+def test_graph_equals_eager_and_deterministic(prec_name):
+    from p3m_b200 import FP32, FP64, MODE_NVE, Context, Replica
+
+    prec = {"fp32": FP32, "fp64": FP64}[prec_name]
+    N = 3000
+    L = (4 * np.pi * N / 3) ** (1 / 3)
+    r = Replica(N=N, L=L, kappa=2.0, alpha=0.6, rc=L / 3.2, M=32, dt=0.1, T_desired=0.01)
+    pos, vel = _init_state(r, 5)
+    outs = []
+    for graph in (True, False, True):
+        with Context(r, precision=prec) as c:
+            c.set_state(0, pos, vel)
+            c.init_forces()
+            c.run(10, MODE_NVE, graph=graph)
+            outs.append(c.get_state(0))
+    for o in outs[1:]:
+        for a, b in zip(outs[0], o):
+            assert np.array_equal(a, b)
+
+
+def test_batch_replica_equals_alone():
+    """A replica inside an uneven batch is bit-identical to the same replica
+    run alone (FP32 path)."""
+    from p3m_b200 import FP32, MODE_NVE, MODE_THERMOSTAT, Context, Replica
+
+    reps = []
+    for N, kappa, M in [(2000, 1.0, 32), (5000, 2.0, 64), (3000, 0.5, 32)]:
+        L = (4 * np.pi * N / 3) ** (1 / 3)
+        reps.append(Replica(N=N, L=L, kappa=kappa, alpha=0.7, rc=min(5.0, L / 3.01), M=M, dt=0.1,
+                            T_desired=0.02))
+    states = [_init_state(r, 11 + i) for i, r in enumerate(reps)]
+    with Context(reps, precision=FP32) as c:
+        for i, (p, v) in enumerate(states):
+            c.set_state(i, p, v)
+        c.init_forces()
+        c.run(5, MODE_THERMOSTAT)
+        c.run(5, MODE_NVE)
+        batch = [c.get_state(i) for i in range(len(reps))]
+        E = c.energies()
+    for i, r in enumerate(reps):
+        with Context(r, precision=FP32) as c:
+            c.set_state(0, *states[i])
+            c.init_forces()
+            c.run(5, MODE_THERMOSTAT)
+            c.run(5, MODE_NVE)
+            alone = c.get_state(0)
+            Ea = c.energies()
+        for a, b in zip(batch[i], alone):
+            assert np.array_equal(a, b)
+        assert np.array_equal(E[:, i, :], Ea[:, 0, :])
+
+
+def test_fp32_force_error_cfg1_size():
+    """FP32 total-force error against the FP64 oracle at the N=1e4, 64^3,
+    kappa=2, alpha=0.6, rc=6 configuration (RMS <= 1e-5)."""
+    from p3m_b200 import FP32, FP64, Context, Replica
+
+    N = 10000
+    L = (4 * np.pi * N / 3) ** (1 / 3)
+    r = Replica(N=N, L=L, kappa=2.0, alpha=0.6, rc=6.0, M=64, T_desired=0.01)
+    pos, _ = _init_state(r, 1)
+    with Context(r, precision=FP64) as c:
+        U64, a64, parts64 = c.force(pos)
+        G, A = None, None
+    with Context(r, precision=FP32) as c:
+        U32, a32, _ = c.force(pos)
+    # the FP64 device result against the oracle (PP in C, PM in numpy, G from
+    # the device gf_opt which is pinned to the reference at 16^3 and 32^3)
+    from p3m_b200 import gf_opt_device
+
+    P = O.Params(N, 2.0, 0.6, 6.0, 64, Gamma=100.0)
+    Gk, _ = gf_opt_device(2.0, 0.6, 6, 3, 64, L)
+    mid = 32
+    kv = 2 * np.pi * (np.arange(64) - mid) / L
+    P._gk = (Gk, kv.reshape(1, 64), kv.reshape(64, 1), kv.reshape(64, 1, 1), 0.0)
+    Uo, ao, _ = O.force_pot(P, pos)
+    assert U64 == pytest.approx(Uo, rel=1e-10)
+    assert rel_rms(a64, ao) < 1e-9
+    assert rel_rms(a32, ao) <= 1e-5
+    assert U32 == pytest.approx(Uo, rel=1e-6)
+
+
+def test_edge_particle_at_box_edge():
+    """x = L exactly is the periodic image of x = 0 for the mesh (as the
+    reference's single wrap makes it) and for the PP cells."""
+    from p3m_b200 import FP64, Context, Replica
+
+    N = 2000
+    L = (4 * np.pi * N / 3) ** (1 / 3)
+    r = Replica(N=N, L=L, kappa=1.0, alpha=0.7, rc=L / 3.0, M=32)
+    pos, _ = _init_state(r, 3)
+    pos_edge = pos.copy()
+    pos_edge[7] = [L, 0.5 * L, L]
+    pos_zero = pos_edge.copy()
+    pos_zero[7] = [0.0, 0.5 * L, 0.0]
+    with Context(r, precision=FP64) as c:
+        U1, a1, _ = c.force(pos_edge)
+        U2, a2, _ = c.force(pos_zero)
+        rho_e = c.assign(pos_edge)
+    assert U1 == pytest.approx(U2, rel=1e-12)
+    assert rel_rms(a1, a2) < 1e-12
+    h = L / 32
+    rho_o = O.assign6(pos_edge, np.ones(N), 32, 32, 32, h, h, h)
+    assert np.max(np.abs(rho_e - rho_o)) < 1e-11
+
+
+def test_out_of_box_raises():
+    from p3m_b200 import FP64, Context, P3MError, Replica
+
+    N = 2000
+    L = (4 * np.pi * N / 3) ** (1 / 3)
+    r = Replica(N=N, L=L, kappa=1.0, alpha=0.7, rc=L / 3.0, M=32)
+    pos, _ = _init_state(r, 3)
+    pos[5, 1] = 2.5 * L
+    with Context(r, precision=FP64) as c:
+        with pytest.raises(P3MError) as e:
+            c.force(pos)
+        assert e.value.code == -4
+        pos[5, 1] = 0.5 * L
+        c.force(pos)  # the context stays usable
+
+
+def test_bad_descriptors_rejected():
+    from p3m_b200 import FP32, Context, P3MError, Replica
+
+    L = 10.0
+    with pytest.raises(P3MError):
+        Context(Replica(N=100, L=L, kappa=1, alpha=1, rc=4.0, M=32), precision=FP32)  # 2 cells
+    with pytest.raises(P3MError):
+        Context(Replica(N=100, L=L, kappa=1, alpha=1, rc=3.0, M=48), precision=FP32)  # not 2^k
+    with pytest.raises(P3MError):
+        Context(Replica(N=0, L=L, kappa=1, alpha=1, rc=3.0, M=32), precision=FP32)
+
+
+def test_nqt_ring_matches_oracle():
+    from p3m_b200 import FP64, MODE_NVE, Context, Replica
+
+    N = 2000
+    L = (4 * np.pi * N / 3) ** (1 / 3)
+    r = Replica(N=N, L=L, kappa=1.0, alpha=0.7, rc=L / 3.0, M=32)
+    pos, vel = _init_state(r, 9)
+    qmult = np.arange(1, 9, dtype=np.float64)
+    with Context(r, precision=FP64) as c:
+        c.set_state(0, pos, vel)
+        c.init_forces()
+        c.set_nqt(qmult, 16)
+        c.run(4, MODE_NVE, record_nqt=True)
+        nqt = c.get_nqt(0, len(qmult))
+        p, _, _ = c.get_state(0)
+    assert nqt.shape == (4, 8, 3)
+    ref = O.nqt(p, qmult * 2 * np.pi / L)
+    np.testing.assert_allclose(nqt[-1], ref, rtol=0, atol=1e-9)
+
+
+def test_launch_count_grows():
+    from p3m_b200 import FP32, MODE_NVE, Context, Replica
+
+    N = 2000
+    L = (4 * np.pi * N / 3) ** (1 / 3)
+    r = Replica(N=N, L=L, kappa=1.0, alpha=0.7, rc=L / 3.0, M=32)
+    pos, vel = _init_state(r, 2)
+    with Context(r, precision=FP32) as c:
+        c.set_state(0, pos, vel)
+        c.init_forces()
+        n0 = c.launch_count()
+        c.run(3, MODE_NVE)
+        assert c.launch_count() - n0 >= 3 * 16
