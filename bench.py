@@ -1,0 +1,458 @@
+#!/usr/bin/env python
+"""Throughput of the P3M MD step on B200, in particle-steps/s.
+
+Workload (default): the batched ensemble of 20 Yukawa OCP replicas, each
+N = 10^4, Gamma = 100, kappa = 2, 64^3 mesh, p = 6, alpha = 0.6, r_c = 6,
+dt = 0.1, seeds 1..20, advanced together (FP32 bulk arithmetic, FP64
+reductions and positions) by CUDA-graph-captured NVE steps that also record
+n(q,t) on 32 wave numbers x 3 axes. A "step" is one velocity-Verlet step of
+every replica.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Ours: one process per GPU (torchrun for N > 1), each with its own 20-replica
+ensemble (replicas only: no data-path collective; weak scaling). The timed
+region is K graph launches between CUDA events on the context's stream,
+after a barrier and device synchronisation; the max over ranks is taken.
+The line also carries the plain FP64 single-replica path on the same
+ensemble, the FP32-vs-FP64 force error, the end-to-end number through the
+C ABI with host buffers, the PP kernel's roofline and the CPU baseline (the
+oracle port on one host core).
+
+--impl reference: the reference's CPU path for the same workload, run as the
+oracle port (the reference's own code is Python/numba that does not travel
+to the GPU box) over all host cores, one replica per process.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "md-force-routines_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-steps/s on 1 B200: batched FP32 vs plain FP64 P3M at force err<=1e-5"
+UNIT = "particle-steps/s"
+WORKLOAD = ("cfg3 ensemble: 20 replicas x N=1e4, Gamma=100, kappa=2, 64^3 mesh, p=6, "
+            "alpha=0.6, rc=6, dt=0.1, NVE steps with n(q,t) (32 q x 3 axes)")
+FLOP_PER_PAIR = 48  # fixed convention for the PP roofline (unique pairs)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--replicas", type=int, default=20)
+    ap.add_argument("--equil", type=int, default=300,
+                    help="untimed thermostat steps before the NVE warm-up")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the FP64, e2e, roofline and CPU-baseline legs")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": float(np.median(loaded)) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None,
+                "samples": len(rows), "reasons": reasons}
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def initial_states(reps):
+    import initialize_pos_vel
+
+    out = []
+    for r in reps:
+        pos, vel = np.zeros((r.N, 3)), np.zeros((r.N, 3))
+        initialize_pos_vel.initial(r.seed, r.N, [r.L] * 3, pos, vel, r.T_desired)
+        out.append((pos, vel))
+    return out
+
+
+def pp_flop(reps):
+    """Algorithmic PP work of one step: N rc^3/2 unique in-cutoff pairs per
+    replica (number density 3/(4 pi)) x 48 FLOP."""
+    return float(sum(r.N * r.rc ** 3 / 2.0 * FLOP_PER_PAIR for r in reps))
+
+
+def working_set_mb(reps):
+    b = 0
+    for r in reps:
+        M = r.M
+        spec = (M // 2 + 1) * M * M
+        nb = (M // 16) ** 3
+        b += r.N * (3 * 3 * 8 + 32 + 16 + 16 + 40)        # state, staged, acc_pp/pm, keys
+        b += spec * 8 * 4 + spec * 4 + 3 * M ** 3 * 4      # spectra, green, fields
+        b += nb * 21 ** 3 * 8                              # assignment tiles
+    return b / 1e6
+
+
+def dist_setup(backend):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the oracle port on the host cores
+# ---------------------------------------------------------------------------
+_REF_STATE = {}
+
+
+def _ref_worker(args):
+    """Advance one replica n steps with the oracle port; returns seconds."""
+    idx, params, G, n_steps = args
+    from oracle import oracle as O
+
+    if idx not in _REF_STATE:
+        N, L, kappa, alpha, rc, M, dt, Gamma, seed = params
+        P = O.Params(N, kappa, alpha, rc, M, L=L, Gamma=Gamma, dt=dt)
+        mid = M // 2
+        kv = 2 * np.pi * (np.arange(M) - mid) / L
+        P._gk = (G, kv.reshape(1, M), kv.reshape(M, 1), kv.reshape(M, 1, 1), 0.0)
+        import initialize_pos_vel
+
+        pos, vel = np.zeros((N, 3)), np.zeros((N, 3))
+        initialize_pos_vel.initial(seed, N, [L] * 3, pos, vel, 1.0 / Gamma)
+        _, acc, _ = O.force_pot(P, pos)
+        _REF_STATE[idx] = [P, pos, vel, acc]
+    st = _REF_STATE[idx]
+    t0 = time.perf_counter()
+    for _ in range(n_steps):
+        st[1], st[2], st[3], _ = O.update(st[0], st[1], st[2], st[3])
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup("gloo")
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+    from p3m_b200.configs import cfg3
+
+    O.build()
+    reps = cfg3(args.replicas)
+    r0 = reps[0]
+    h = r0.L / r0.M
+    G, _, _, _, _ = O.gf_opt(r0.kappa, r0.alpha, 6, 3, 3, 3, r0.M, r0.M, r0.M, h, h, h,
+                             r0.L, r0.L, r0.L)
+    cores = os.cpu_count() or 1
+    nproc = min(len(reps), cores)
+    params = [(r.N, r.L, r.kappa, r.alpha, r.rc, r.M, r.dt, 1.0 / r.T_desired, r.seed) for r in reps]
+    # bounded sample: each step of this arm is one NVE step of every replica;
+    # cap the steps so the arm ends within a few minutes
+    steps = max(1, min(args.steps, 10))
+    warm = max(1, min(args.warmup, 2))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(nproc) as pool:
+        # pin replicas to workers: one task per replica per phase
+        pool.map(_ref_worker, [(i, params[i], G, warm) for i in range(len(reps))], chunksize=1)
+        t0 = time.perf_counter()
+        pool.map(_ref_worker, [(i, params[i], G, steps) for i in range(len(reps))], chunksize=1)
+        wall = time.perf_counter() - t0
+    total = sum(r.N for r in reps) * steps
+    value = total / wall
+    sample = (f"{len(reps)} replicas x N=1e4 (64^3) advanced {steps} NVE steps each by the oracle "
+              f"port (C PP + numpy FFT/PM) in {nproc} spawned processes; wall {wall:.2f} s")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * wall / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded initialize_pos_vel states)",
+            "config": {"workload": WORKLOAD, "replicas": len(reps), "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def cpu_baseline_port(rep, G, n_steps=4):
+    """The oracle port on one core for replica `rep` (bounded sample)."""
+    from oracle import oracle as O
+
+    M = rep.M
+    P = O.Params(rep.N, rep.kappa, rep.alpha, rep.rc, M, L=rep.L, Gamma=1.0 / rep.T_desired,
+                 dt=rep.dt)
+    kv = 2 * np.pi * (np.arange(M) - M // 2) / rep.L
+    P._gk = (G, kv.reshape(1, M), kv.reshape(M, 1), kv.reshape(M, 1, 1), 0.0)
+    (pos, vel), = initial_states([rep])
+    _, acc, _ = O.force_pot(P, pos)
+    times = []
+    for _ in range(n_steps):
+        t0 = time.perf_counter()
+        pos, vel, acc, _ = O.update(P, pos, vel, acc)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    return {"value": rep.N / t, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"1 replica (N={rep.N}, {M}^3) x {n_steps} NVE steps, median step "
+                      f"{t * 1e3:.1f} ms, oracle port (C PP + numpy FFT/PM), 1 thread"}
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_setup("nccl")
+    torch.cuda.set_device(local)
+    from p3m_b200 import FP32, MODE_NVE, MODE_THERMOSTAT, Context
+    from p3m_b200.configs import CFG3_QMULT, cfg3
+
+    reps = cfg3(args.replicas, first_seed=1 + rank * args.replicas)
+    states = initial_states(reps)
+    ctx = Context(reps, precision=FP32, device=local)
+    for i, (p, v) in enumerate(states):
+        ctx.set_state(i, p, v)
+    ctx.init_forces()
+    ctx.set_nqt(CFG3_QMULT, 4096)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+
+    # equilibration with the reference's thermostat (thermostat_p3m_ord6.vscale)
+    # from the random initial state, then NVE warm-up (also builds the graph)
+    ctx.run(args.equil, MODE_THERMOSTAT, it0=0, graph=True)
+    ctx.run(max(args.warmup, 3), MODE_NVE, record_nqt=True, graph=True)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    ctx.sync()
+    n0 = ctx.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.run(args.steps, MODE_NVE, record_nqt=True, graph=True, sync=False)
+    e1.record(stream)
+    e1.synchronize()
+    ctx.sync()
+    ms = e0.elapsed_time(e1)
+    launches = ctx.launch_count() - n0
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ctx.check()
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    n_part = sum(r.N for r in reps)
+    value = n_part * args.steps * world / (ms * 1e-3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded initialize_pos_vel: uniform positions, Maxwell-Boltzmann "
+                    "velocities)",
+            "config": {"workload": WORKLOAD, "replicas": len(reps), "N_per_replica": reps[0].N,
+                       "mesh": reps[0].M, "parallelism": f"replicas x{world}" if world > 1 else "replicas",
+                       "l2": f"inputs larger than L2 (working set {working_set_mb(reps):.0f} MB > 126 MB)",
+                       "pp_config": list(ctx.pp_config())},
+            "gpu_launches": launches, "clocks": clocks}
+
+    if not args.no_extras and rank == 0:
+        eq_states = [ctx.get_state(i)[:2] for i in range(len(reps))]
+        extras(args, line, ctx, reps, eq_states, local)
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def extras(args, line, ctx, reps, states, device):
+    import torch
+
+    from p3m_b200 import FP32, FP64, MODE_NVE, Context, fp32_peak_tflops, gf_opt_device, lib
+
+    # -- per-stage device times and the PP roofline (FP32 pipe) ------------------
+    try:
+        stages = ctx.profile_stages(iters=20)
+    except Exception as e:  # measurement only: report and carry on
+        print(f"profile_stages: {e}", file=sys.stderr)
+        stages = {}
+    flagged = [k for k, v in stages.items() if v < 0]
+    if flagged:
+        print(f"profile_stages: status raised in {flagged}: "
+              f"{lib().p3m_last_error(ctx.handle).decode()}", file=sys.stderr)
+        stages = {k: abs(v) for k, v in stages.items()}
+    peak = fp32_peak_tflops(device)
+    pp_ms = stages.get("pp", 0.0)
+    flop = pp_flop(reps)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "pp_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("cfg3_bytes_per_launch")
+        except Exception:
+            traffic = None
+    achieved = flop / (pp_ms * 1e-3) / 1e12 if pp_ms > 0 else None
+    line["roofline"] = {"kernel": "k_pp (PP pair loop, FP32)", "bound": "fp32",
+                        "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                        "peak_source": "measured FP32 FMA probe (p3m_fp32_peak) on this GPU; "
+                                       "MEASURED_PEAKS.json has no FP32 figure",
+                        "work": f"{flop:.3e} FLOP per launch = sum N rc^3/2 pairs x {FLOP_PER_PAIR}"}
+    if "fft_both" in stages and "fft_forward" in stages:
+        stages["fft_inverse"] = stages["fft_both"] - stages["fft_forward"]
+    line["stages_ms"] = {k: round(v, 5) for k, v in stages.items()}
+
+    # -- FP32 force error against the FP64 path on replica 0's initial state -----
+    r0 = reps[0]
+    with Context(r0, precision=FP64, device=device) as c64, \
+            Context(r0, precision=FP32, device=device) as c32:
+        _, a64, _ = c64.force(states[0][0])
+        _, a32, _ = c32.force(states[0][0])
+    ref_rms = np.sqrt(np.mean(np.sum(a64 ** 2, axis=1)))
+    line["force_err"] = {
+        "rms_rel": float(np.sqrt(np.sum((a32 - a64) ** 2) / np.sum(a64 ** 2))),
+        "max_rel": float(np.max(np.sqrt(np.sum((a32 - a64) ** 2, axis=1))) / ref_rms),
+        "vs": "FP64 device path (pinned to the FP64 oracle by the parity tests)"}
+
+    # -- the plain FP64 single-replica path on the same ensemble -------------------
+    t_tot, ps = 0.0, 0
+    nrun = min(args.steps, 20)
+    for r, (p, v) in zip(reps, states):
+        with Context(r, precision=FP64, device=device) as c:
+            c.set_state(0, p, v)
+            c.init_forces()
+            c.run(3, MODE_NVE, graph=True)
+            s = torch.cuda.ExternalStream(c.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            c.run(nrun, MODE_NVE, graph=True, sync=False)
+            e1.record(s)
+            e1.synchronize()
+            t_tot += e0.elapsed_time(e1) * 1e-3
+            ps += r.N * nrun
+    fp64 = ps / t_tot
+    line["fp64_plain"] = {"value": fp64, "unit": UNIT,
+                          "how": f"each replica alone, FP64 bulk, graph-captured NVE steps "
+                                 f"({nrun} per replica, device-timed)",
+                          "batched_fp32_over_fp64": line["value"] / line["n_gpus"] / fp64}
+
+    # -- end to end through the C ABI with host buffers ----------------------------
+    # per step: H2D of every replica's (pos, vel, acc) from pinned host memory,
+    # one batched step, D2H of the state and of the step's energies
+    host = []
+    for i, r in enumerate(reps):
+        bufs = [torch.empty((r.N, 3), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+        bufs[0][:] = states[i][0]
+        bufs[1][:] = states[i][1]
+        bufs[2][:] = 0.0
+        host.append(bufs)
+    with Context(reps, precision=FP32, device=device) as c:
+        for i, b in enumerate(host):
+            c.set_state(i, b[0], b[1])
+        c.init_forces()
+        for i, b in enumerate(host):
+            b[0][:], b[1][:], b[2][:] = c.get_state(i)
+        c.run(2, MODE_NVE, graph=True)
+        n_e2e = min(args.steps, 50)
+        s = torch.cuda.ExternalStream(c.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(n_e2e):
+            for i, b in enumerate(host):
+                c.set_state(i, b[0], b[1], b[2])
+            c.run(1, MODE_NVE, graph=True)
+            for i, b in enumerate(host):
+                b[0][:], b[1][:], b[2][:] = c.get_state(i)
+            c.energies(max_steps=1)
+        e1.record(s)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3
+    nb = sum(r.N for r in reps) * 3 * 8
+    line["e2e"] = {"value": sum(r.N for r in reps) * n_e2e / t, "unit": UNIT,
+                   "h2d_bytes_per_step": 3 * nb, "d2h_bytes_per_step": 3 * nb + 4 * 8 * len(reps),
+                   "how": "p3m_set_state x R (pinned host -> device), p3m_run(1), p3m_get_state x R "
+                          "and p3m_get_energies per step"}
+
+    # -- CPU baseline: the oracle port on one host core ------------------------------
+    G, _ = gf_opt_device(r0.kappa, r0.alpha, 6, 3, r0.M, r0.L, device=device)
+    line["cpu_baseline"] = cpu_baseline_port(r0, G)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -173,6 +173,18 @@ int p3m_sync(p3m_ctx *ctx);
 int p3m_set_pp_config(p3m_ctx *ctx, int tpi, int split);
 int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, int *split);
 
+/* Measurement: average device time (ms) of each step stage over `iters`
+ * back-to-back launches, timed with CUDA events on the context's stream.
+ * Stage i is named by p3m_stage_name(i); *n_out stages are written. The
+ * drift stage moves the particles: call it after the run being measured. */
+int p3m_profile_stages(p3m_ctx *ctx, int iters, double *ms, int max_stages, int *n_out);
+const char *p3m_stage_name(int i);
+
+/* Measurement: FP32 FMA throughput of `device` in TFLOP/s (8 independent FMA
+ * chains per thread, 8 CTAs of 256 threads per SM) -- the denominator of the
+ * FP32-pipe-bound PP kernel's roofline. */
+int p3m_fp32_peak(int device, double *tflops);
+
 /* Stream the context launches on (a cudaStream_t), for callers that time it
  * with their own events. */
 void *p3m_stream(p3m_ctx *ctx);

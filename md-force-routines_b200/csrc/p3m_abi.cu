@@ -154,7 +154,7 @@ template <typename T> static int alloc_bulk(p3m_ctx *ctx)
     using T4 = typename V4<T>::t;
     using C = typename C2<T>::t;
     DevState &s = ctx->s;
-    CK(valloc(&s.xs_cell, (size_t)s.ntot * sizeof(T4)));
+    CK(valloc(&s.xs_cell, (size_t)s.ntot * sizeof(double4)));
     CK(valloc(&s.acc_pp, (size_t)s.ntot * sizeof(T4)));
     if (s.has_mesh) {
         CK(valloc(&s.acc_pm, (size_t)s.ntot * sizeof(T4)));
@@ -1001,5 +1001,146 @@ extern "C" int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, int *split)
     if (!ctx || !tpi || !split) return fail(ctx, P3M_EARG, "p3m_get_pp_config", "NULL argument");
     *tpi = ctx->s.pp_tpi;
     *split = ctx->s.pp_split;
+    return P3M_OK;
+}
+
+// ---------------------------------------------------------------------------
+// measurement
+// ---------------------------------------------------------------------------
+
+// Each stage is idempotent when repeated (the inverse FFT works in place on
+// the field spectra, so it is timed together with the forward pass that
+// rebuilds them: fft_inverse = fft_both - fft_forward).
+static const char *kStageNames[] = {"drift_sort", "keys_sort", "pp", "assign", "fft_forward",
+                                    "fft_both", "gather", "finish", "nqt", "step"};
+static const int kNumStages = 10;
+
+extern "C" const char *p3m_stage_name(int i)
+{
+    return (i >= 0 && i < kNumStages) ? kStageNames[i] : "";
+}
+
+template <typename T> static void enqueue_stage(p3m_ctx *ctx, int k)
+{
+    DevState &s = ctx->s;
+    switch (k) {
+    case 0:
+        launch_kick_drift(s, ctx->st);
+        seq_sort<T>(ctx, false);
+        break;
+    case 1: seq_sort<T>(ctx, true); break;
+    case 2: seq_pp<T>(ctx); break;
+    case 3: launch_assign<T>(s, ctx->st); ctx->launches++; break;
+    case 4: launch_fft_forward<T>(s, ctx->st); ctx->launches += 3; break;
+    case 5:
+        launch_fft_forward<T>(s, ctx->st);
+        launch_fft_inverse<T>(s, ctx->st);
+        ctx->launches += 5;
+        break;
+    case 6: launch_gather<T>(s, ctx->st); ctx->launches++; break;
+    case 7:
+        launch_kick_finish<T>(s, 0, nullptr, ctx->st);
+        launch_step_reduce(s, 2, ctx->counters, nullptr, 0, ctx->st);
+        ctx->launches += 2;
+        break;
+    case 8:
+        if (ctx->nq > 0) {
+            launch_nqt<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nqt_part, ctx->tmp_nq ? ctx->tmp_nq : ctx->nqt_part,
+                          nullptr, 0, ctx->st);
+            ctx->launches += 2;
+        }
+        break;
+    default: break;
+    }
+}
+
+// Average device time of each stage over `iters` back-to-back launches
+// (CUDA events on the context's stream). The drift stage moves the
+// particles, so this perturbs the state; call it after the run it measures.
+template <typename T> static int do_profile(p3m_ctx *ctx, int iters, double *ms, int max_stages,
+                                            int *n_out)
+{
+    DevState &s = ctx->s;
+    if (s.has_mesh) RET(ensure_green<T>(ctx));
+    if (ctx->nq > 0 && ctx->tmp_nq_cap == 0) {
+        CK(dalloc(&ctx->tmp_nq, (size_t)ctx->nrep * 64 * 6 + (size_t)s.nblk * 64 * 6 + 64));
+        ctx->tmp_nq_cap = 64;
+    }
+    // the drift stage kicks with stale forces on every repeat: keep a copy of
+    // the state and put it back afterwards
+    const size_t sb = sizeof(double) * 3 * (size_t)s.ntot;
+    double *backup = nullptr;
+    CK(cudaMalloc(&backup, 3 * sb));
+    CK(cudaMemcpyAsync(backup, s.pos, sb, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(backup + 3 * (size_t)s.ntot, s.vel, sb, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(backup + 6 * (size_t)s.ntot, s.acc, sb, cudaMemcpyDeviceToDevice, ctx->st));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int n = 0;
+    for (int k = 0; k < kNumStages && n < max_stages; ++k, ++n) {
+        ms[n] = 0.0;
+        if (!s.has_mesh && k >= 3 && k <= 6) continue;
+        if (k == 8 && ctx->nq == 0) continue;
+        // one untimed launch, then the timed loop
+        if (k == 9) {
+            if (!ctx->graph[0][0]) { RET(do_run<T>(ctx, 1, P3M_MODE_NVE, 0, 0, 1, 1)); }
+            CK(cudaEventRecord(e0, ctx->st));
+            for (int i = 0; i < iters; ++i) CK(cudaGraphLaunch(ctx->graph[0][0], ctx->st));
+            CK(cudaEventRecord(e1, ctx->st));
+        } else {
+            enqueue_stage<T>(ctx, k);
+            CK(cudaEventRecord(e0, ctx->st));
+            for (int i = 0; i < iters; ++i) enqueue_stage<T>(ctx, k);
+            CK(cudaEventRecord(e1, ctx->st));
+        }
+        CK(cudaEventSynchronize(e1));
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, e0, e1));
+        ms[n] = (double)t / iters;
+        {
+            int stv = 0;
+            CK(cudaMemcpy(&stv, s.status, sizeof(int), cudaMemcpyDeviceToHost));
+            if (stv && k != 0) {
+                char b[128];
+                snprintf(b, sizeof b, "status %d raised while profiling stage %s", stv, kStageNames[k]);
+                ctx->err = b;
+                ms[n] = -ms[n];  // flagged
+                CK(cudaMemset(s.status, 0, sizeof(int)));
+            }
+        }
+        if (k == 0) {
+            // restore the state, clear what the stale drifts may have flagged,
+            // and re-sort for the stages that follow
+            CK(cudaMemcpyAsync(s.pos, backup, sb, cudaMemcpyDeviceToDevice, ctx->st));
+            CK(cudaMemcpyAsync(s.vel, backup + 3 * (size_t)s.ntot, sb, cudaMemcpyDeviceToDevice, ctx->st));
+            CK(cudaMemcpyAsync(s.acc, backup + 6 * (size_t)s.ntot, sb, cudaMemcpyDeviceToDevice, ctx->st));
+            CK(cudaMemsetAsync(s.status, 0, sizeof(int), ctx->st));
+            seq_sort<T>(ctx, true);
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaStreamSynchronize(ctx->st));
+    cudaFree(backup);
+    *n_out = n;
+    return finish(ctx);
+}
+
+extern "C" int p3m_profile_stages(p3m_ctx *ctx, int iters, double *ms, int max_stages, int *n_out)
+{
+    if (!ctx || !ms || !n_out || iters <= 0) return fail(ctx, P3M_EARG, "p3m_profile_stages", "bad argument");
+    CK(cudaSetDevice(ctx->device));
+    return DISPATCH(do_profile, ctx, iters, ms, max_stages, n_out);
+}
+
+extern "C" int p3m_fp32_peak(int device, double *tflops)
+{
+    if (!tflops) return fail(nullptr, P3M_EARG, "p3m_fp32_peak", "NULL argument");
+    int rc = check_device(nullptr, device);
+    if (rc != P3M_OK) return rc;
+    const double t = fp32_fma_tflops(device);
+    if (t <= 0) return fail(nullptr, P3M_ECUDA, "p3m_fp32_peak", "probe kernel failed");
+    *tflops = t;
     return P3M_OK;
 }

@@ -27,7 +27,7 @@ struct DevState {
     // cell sort
     int *cell_key = nullptr, *cell_count = nullptr, *cell_start = nullptr;
     int *cell_cursor = nullptr, *cell_tmp = nullptr, *cell_perm = nullptr, *cell_slot = nullptr;
-    void *xs_cell = nullptr;     // V4<T> sorted positions relative to the cell origin
+    void *xs_cell = nullptr;     // double4 sorted positions relative to the cell origin
     void *acc_pp = nullptr;      // V4<T> PP acceleration, cell-sorted order
     // brick sort
     int *brick_key = nullptr, *brick_count = nullptr, *brick_start = nullptr;
@@ -93,6 +93,7 @@ template <typename T> void launch_nqt(const DevState &s, const double *pos, cons
                                       int ring_cap, cudaStream_t st);
 template <typename T> void configure_integrate_kernels(int max_nq);
 int gf_opt_blocks(int M);
+double fp32_fma_tflops(int device);
 
 
 }  // namespace p3m

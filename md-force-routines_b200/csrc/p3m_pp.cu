@@ -55,26 +55,42 @@ __device__ __forceinline__ void yukawa_ewald_pair(T r2, const PairCoef<T> &c, T 
 }
 
 template <typename T> struct PPCfg;
-template <> struct PPCfg<float> { static constexpr int SCAP = 2048, LCAP = 96; };
-template <> struct PPCfg<double> { static constexpr int SCAP = 1024, LCAP = 96; };
+template <> struct PPCfg<float> { static constexpr int SCAP = 1536, LCAP = 96; };
+template <> struct PPCfg<double> { static constexpr int SCAP = 1536, LCAP = 96; };
 
 constexpr int PP_THREADS = 128;
 
+// Shared-memory bytes of the PP kernel: staged neighbours (FP64: one double4;
+// FP32: a hi and a lo float4 per particle) and the per-thread lists.
+template <typename T> constexpr size_t pp_smem_bytes()
+{
+    return (size_t)PPCfg<T>::SCAP * 32 + (size_t)PPCfg<T>::LCAP * PP_THREADS * sizeof(unsigned short);
+}
+
+// Positions come in as FP64 offsets from the cell origin (double4). The FP64
+// path stages them as they are. The FP32 path stages each coordinate as a
+// pair of floats (hi = fl(x), lo = fl(x - hi)): the cutoff filter uses hi
+// alone, and the pair terms use dx = (xi_hi - xj_hi) + (xi_lo - xj_lo), whose
+// error is a rounding of dx itself rather than of the (larger) coordinates --
+// with plain FP32 coordinates the position rounding alone gives a ~3e-6
+// relative force error.
 template <typename T, int TPI>
 __global__ void __launch_bounds__(PP_THREADS)
 k_pp(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
-     const typename V4<T>::t *__restrict__ xs, typename V4<T>::t *__restrict__ acc_out,
+     const double4 *__restrict__ xs, typename V4<T>::t *__restrict__ acc_out,
      double *__restrict__ u_part, int ncell, int split)
 {
     using T4 = typename V4<T>::t;
+    constexpr bool F32 = sizeof(T) == 4;
     constexpr int SCAP = PPCfg<T>::SCAP, LCAP = PPCfg<T>::LCAP;
     constexpr int ICH = PP_THREADS / TPI;  // i-particles per CTA pass
     extern __shared__ __align__(16) unsigned char pp_smem[];
-    T4 *stage = reinterpret_cast<T4 *>(pp_smem);
-    unsigned short *list = reinterpret_cast<unsigned short *>(pp_smem + SCAP * sizeof(T4));
+    T4 *stage = reinterpret_cast<T4 *>(pp_smem);               // FP64: double4; FP32: hi
+    float4 *stage_lo = reinterpret_cast<float4 *>(pp_smem + (size_t)SCAP * 16);  // FP32 only
+    unsigned short *list = reinterpret_cast<unsigned short *>(pp_smem + (size_t)SCAP * 32);
     __shared__ int pre[28];
     __shared__ int nstart[27];
-    __shared__ T shx[27], shy[27], shz[27];
+    __shared__ double shx[27], shy[27], shz[27];
     __shared__ double red[32];
 
     const int tid = threadIdx.x;
@@ -104,9 +120,9 @@ k_pp(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_sta
             int nb = R.cell_off + nx + nc * (ny + nc * nz);
             nstart[tid] = cell_start[nb];
             pre[tid + 1] = cell_start[nb + 1] - cell_start[nb];
-            shx[tid] = (T)(dx * R.cellw);
-            shy[tid] = (T)(dy * R.cellw);
-            shz[tid] = (T)(dz * R.cellw);
+            shx[tid] = dx * R.cellw;
+            shy[tid] = dy * R.cellw;
+            shz[tid] = dz * R.cellw;
         }
         __syncthreads();
         if (tid == 0) {
@@ -121,12 +137,23 @@ k_pp(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_sta
         for (int ch = part; ch < nchunks; ch += split) {
             const int i = ch * ICH + il;
             const bool have_i = i < nhome;
-            T4 xi;
+            T4 xi;          // FP64: position; FP32: hi part
+            float4 xl;      // FP32: lo part
             if (have_i) {
-                xi = xs[hstart + i];
+                const double4 p = xs[hstart + i];
+                if constexpr (F32) {
+                    xi.x = (float)p.x; xi.y = (float)p.y; xi.z = (float)p.z; xi.w = 0.f;
+                    xl.x = (float)(p.x - (double)xi.x);
+                    xl.y = (float)(p.y - (double)xi.y);
+                    xl.z = (float)(p.z - (double)xi.z);
+                    xl.w = 0.f;
+                } else {
+                    xi.x = p.x; xi.y = p.y; xi.z = p.z; xi.w = 0.0;
+                }
             } else {
                 xi.x = xi.y = xi.z = (T)1e18;
                 xi.w = (T)0;
+                xl.x = xl.y = xl.z = xl.w = 0.f;
             }
             T fx = 0, fy = 0, fz = 0, gx = 0, gy = 0, gz = 0;  // sums and Kahan terms
 
@@ -137,11 +164,15 @@ k_pp(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_sta
                     int g = w0 + k;
                     int cc = 0;
                     while (pre[cc + 1] <= g) ++cc;
-                    T4 p = xs[nstart[cc] + g - pre[cc]];
-                    p.x += shx[cc];
-                    p.y += shy[cc];
-                    p.z += shz[cc];
-                    stage[k] = p;
+                    const double4 p = xs[nstart[cc] + g - pre[cc]];
+                    const double x = p.x + shx[cc], y = p.y + shy[cc], z = p.z + shz[cc];
+                    T4 h;
+                    h.x = (T)x; h.y = (T)y; h.z = (T)z; h.w = (T)0;
+                    stage[k] = h;
+                    if constexpr (F32) {
+                        stage_lo[k] = make_float4((float)(x - (double)h.x), (float)(y - (double)h.y),
+                                                  (float)(z - (double)h.z), 0.f);
+                    }
                 }
                 __syncthreads();
 
@@ -152,8 +183,15 @@ k_pp(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_sta
                     T pu = 0;
                     for (int e = 0; e < mmax; ++e) {
                         if (e < cnt) {
-                            T4 q = stage[list[e * PP_THREADS + tid]];
+                            const int k = list[e * PP_THREADS + tid];
+                            const T4 q = stage[k];
                             T dx = xi.x - q.x, dy = xi.y - q.y, dz = xi.z - q.z;
+                            if constexpr (F32) {
+                                const float4 ql = stage_lo[k];
+                                dx += xl.x - ql.x;
+                                dy += xl.y - ql.y;
+                                dz += xl.z - ql.z;
+                            }
                             T r2 = dx * dx + dy * dy + dz * dz;
                             T fr, ph;
                             yukawa_ewald_pair<T>(r2, c, fr, ph);
@@ -209,22 +247,18 @@ k_pp(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_sta
 template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cudaStream_t st)
 {
     using T4 = typename V4<T>::t;
-    constexpr size_t smem =
-        PPCfg<T>::SCAP * sizeof(T4) + PPCfg<T>::LCAP * PP_THREADS * sizeof(unsigned short);
     int grid = s.ncell * s.pp_split;
-    k_pp<T, TPI><<<grid, PP_THREADS, smem, st>>>(s.reps, s.nrep, s.cell_start,
-                                                 (const T4 *)s.xs_cell, (T4 *)s.acc_pp,
-                                                 s.u_pp_part, s.ncell, s.pp_split);
+    k_pp<T, TPI><<<grid, PP_THREADS, pp_smem_bytes<T>(), st>>>(
+        s.reps, s.nrep, s.cell_start, (const double4 *)s.xs_cell, (T4 *)s.acc_pp, s.u_pp_part,
+        s.ncell, s.pp_split);
 }
 
 template <typename T> void configure_pp_kernels()
 {
-    using T4 = typename V4<T>::t;
-    constexpr size_t smem =
-        PPCfg<T>::SCAP * sizeof(T4) + PPCfg<T>::LCAP * PP_THREADS * sizeof(unsigned short);
-    cudaFuncSetAttribute(k_pp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_pp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_pp<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int smem = (int)pp_smem_bytes<T>();
+    cudaFuncSetAttribute(k_pp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_pp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_pp<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 template <typename T> void launch_pp(const DevState &s, cudaStream_t st)

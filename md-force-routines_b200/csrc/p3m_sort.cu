@@ -104,13 +104,11 @@ __global__ void k_scatter(const int *__restrict__ cell_key, const int *__restric
 }
 
 // One warp per cell: order the cell's particles by index and write their
-// positions relative to the cell origin (in T) in that order.
-template <typename T>
+// positions relative to the cell origin (FP64) in that order.
 __global__ void k_fix_cells(const RepDev *__restrict__ reps, int nrep,
                             const int *__restrict__ cell_start, const int *__restrict__ cell_tmp,
                             const double *__restrict__ pos, int *__restrict__ cell_perm,
-                            int *__restrict__ cell_slot, typename V4<T>::t *__restrict__ xs,
-                            int ncell)
+                            int *__restrict__ cell_slot, double4 *__restrict__ xs, int ncell)
 {
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
@@ -132,12 +130,7 @@ __global__ void k_fix_cells(const RepDev *__restrict__ reps, int nrep,
                 double x = fold_box(pos[3 * v + 0], R.L);
                 double y = fold_box(pos[3 * v + 1], R.L);
                 double z = fold_box(pos[3 * v + 2], R.L);
-                typename V4<T>::t q;
-                q.x = (T)(x - cx * R.cellw);
-                q.y = (T)(y - cy * R.cellw);
-                q.z = (T)(z - cz * R.cellw);
-                q.w = (T)0;
-                xs[s] = q;
+                xs[s] = make_double4(x - cx * R.cellw, y - cy * R.cellw, z - cz * R.cellw, 0.0);
             }
         }
     }
@@ -176,9 +169,9 @@ template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st)
 {
     const int wpb = 8;
     int blocks = (s.ncell + wpb - 1) / wpb;
-    k_fix_cells<T><<<blocks, wpb * 32, 0, st>>>(s.reps, s.nrep, s.cell_start, s.cell_tmp, s.pos,
-                                                s.cell_perm, s.cell_slot,
-                                                (typename V4<T>::t *)s.xs_cell, s.ncell);
+    k_fix_cells<<<blocks, wpb * 32, 0, st>>>(s.reps, s.nrep, s.cell_start, s.cell_tmp, s.pos,
+                                             s.cell_perm, s.cell_slot, (double4 *)s.xs_cell,
+                                             s.ncell);
 }
 
 template void launch_keys<float>(const DevState &, cudaStream_t);

@@ -7,7 +7,8 @@ signatures and route every stage through libp3m_b200.so.
 """
 from ._lib import FP32, FP64, MODE_NVE, MODE_THERMOSTAT, P3MError, lib  # noqa: F401
 from .context import (Context, Replica, compat_context, compat_precision,  # noqa: F401
-                      gf_opt_device, set_compat_precision)
+                      fp32_peak_tflops, gf_opt_device, set_compat_precision)
 
 __all__ = ["Context", "Replica", "P3MError", "FP32", "FP64", "MODE_NVE", "MODE_THERMOSTAT",
-           "compat_context", "set_compat_precision", "compat_precision", "gf_opt_device", "lib"]
+           "compat_context", "set_compat_precision", "compat_precision", "gf_opt_device",
+           "fp32_peak_tflops", "lib"]

@@ -91,6 +91,9 @@ SIGNATURES = {
     "p3m_stream": (_V, [_V]),
     "p3m_set_pp_config": (_I, [_V, _I, _I]),
     "p3m_get_pp_config": (_I, [_V, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "p3m_profile_stages": (_I, [_V, _I, _D, _I, ctypes.POINTER(_I)]),
+    "p3m_stage_name": (ctypes.c_char_p, [_I]),
+    "p3m_fp32_peak": (_I, [_I, _D]),
 }
 
 

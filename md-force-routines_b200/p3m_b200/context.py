@@ -235,6 +235,14 @@ class Context:
     def stream(self):
         return lib().p3m_stream(self.handle)
 
+    def profile_stages(self, iters=20):
+        """{stage name: average ms per launch} (perturbs the state: call after
+        the measured run)."""
+        ms = np.zeros(16)
+        n = ctypes.c_int()
+        self._ck(lib().p3m_profile_stages(self.handle, int(iters), dptr(ms), 16, ctypes.byref(n)))
+        return {lib().p3m_stage_name(i).decode(): float(ms[i]) for i in range(n.value)}
+
     def set_pp_config(self, tpi, split):
         self._ck(lib().p3m_set_pp_config(self.handle, int(tpi), int(split)))
 
@@ -251,6 +259,13 @@ def gf_opt_device(kappa, alpha, p, m_alias, M, L, device=0):
     check(lib().p3m_gf_opt(int(device), float(kappa), float(alpha), int(p), int(m_alias), int(M),
                            float(L), dptr(G), dptr(A)), None)
     return G, float(A[0])
+
+
+def fp32_peak_tflops(device=0):
+    """Measured FP32 FMA throughput of the device (TFLOP/s)."""
+    t = np.zeros(1)
+    check(lib().p3m_fp32_peak(int(device), dptr(t)), None)
+    return float(t[0])
 
 
 # -- contexts of the compat (reference-signature) functions --------------------------

@@ -41,7 +41,7 @@ def test_pp(golden, prec):
         assert rel_rms(acc, g["acc_pp"]) < 1e-12
     else:
         assert U == pytest.approx(float(g["U_pp"]), rel=1e-6)
-        assert rel_rms(acc, g["acc_pp"]) < 2e-6
+        assert rel_rms(acc, g["acc_pp"]) < 1e-6
 
 
 def test_assign(golden, prec):
@@ -52,7 +52,7 @@ def test_assign(golden, prec):
         rho = c.assign(g["pos0"])
     tol = 1e-11 if prec == FP64 else 1e-6
     assert np.max(np.abs(rho - g["rho"])) < tol * np.max(np.abs(g["rho"]))
-    assert abs(rho.sum() - int(g["N"])) < 1e-6
+    assert abs(rho.sum() - int(g["N"])) < (1e-9 if prec == FP64 else 1e-7) * int(g["N"])
 
 
 def test_gather(golden, prec):
@@ -147,7 +147,7 @@ def test_trace_compat(golden, prec):
     tr = np.array(tr)
     tol = 1e-9 if prec == FP64 else 1e-5
     np.testing.assert_allclose(tr, g["trace"], rtol=tol)
-    assert np.max(np.abs(p - g["pos_final"])) < (1e-10 if prec == FP64 else 1e-6)
+    assert np.max(np.abs(p - g["pos_final"])) < (1e-10 if prec == FP64 else 1e-5)
 
 
 def test_reference_modules_force_pot(golden, capsys):
@@ -204,7 +204,7 @@ def test_reference_modules_pp_pm(golden):
     assert U == pytest.approx(float(g["U_pp"]), rel=1e-12)
     rho = np.zeros((M, M, M))
     out = yukawa_pm_ord6.charge_assgn_6_numba(rho, g["pos0"], np.ones(N), N, M, M, M, h, h, h)
-    assert out is rho and np.max(np.abs(rho - g["rho"])) < 1e-12
+    assert out is rho and np.max(np.abs(rho - g["rho"])) < 1e-11 * np.max(np.abs(g["rho"]))
     kx, ky, kz = golden_kvecs(g)
     Ex, Ey, Ez = np.zeros(N), np.zeros(N), np.zeros(N)
     Uf, accf = yukawa_pm_ord6.particle_mesh_fft_r(

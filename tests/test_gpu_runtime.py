@@ -124,7 +124,8 @@ def test_fp32_force_error_cfg1_size():
     assert U64 == pytest.approx(Uo, rel=1e-10)
     assert rel_rms(a64, ao) < 1e-9
     assert rel_rms(a32, ao) <= 1e-5
-    assert U32 == pytest.approx(Uo, rel=1e-6)
+    # U = U_pp + U_pm + U_self cancels ~18x here: judge it against |U_pp|
+    assert abs(U32 - Uo) < 1e-6 * abs(parts64[0])
 
 
 def test_edge_particle_at_box_edge():
