@@ -97,6 +97,23 @@ int p3m_gather(p3m_ctx *ctx, int replica, const double *pos, const double *Z,
 int p3m_gf_opt(int device, double kappa, double alpha, int p, int m_alias, int M,
                double box, double *G_k, double *A_pm);
 
+/* gf_opt for callers that cannot allocate device memory (no counterpart in
+ * the reference). Same kernel and result as p3m_gf_opt, but the caller
+ * passes device pointers for the outputs -- G_k_dev (M*M*M doubles,
+ * fftshifted layout) and A_pm_dev (one double) -- and the stream to launch
+ * on; the call returns without waiting. The only scratch (one FP64 partial
+ * per 256-point block) lives in a fixed file-scope device array of 8192
+ * doubles (64 KiB, held on every GPU that loads the library until exit), so
+ * M is limited to 128; larger M is rejected with P3M_EARG. The call
+ * allocates nothing. The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture. All calls on a device share the array: calls that
+ * overlap on the GPU race and must be ordered by the caller. Runs on the
+ * current device. Message of the last failure: p3m_gf_opt_static_error(). */
+int p3m_gf_opt_static(double kappa, double alpha, int p, int m_alias, int M, double box,
+                      double *G_k_dev, double *A_pm_dev, void *stream);
+const char *p3m_gf_opt_static_error(void);
+
 /* Install the influence function the PM stage uses for `replica`, given in the
  * reference's fftshifted (M,M,M) layout (as returned by gf_opt). With
  * G_k == NULL the context computes it on the device itself. */

@@ -94,6 +94,9 @@ SIGNATURES = {
     "p3m_profile_stages": (_I, [_V, _I, _D, _I, ctypes.POINTER(_I)]),
     "p3m_stage_name": (ctypes.c_char_p, [_I]),
     "p3m_fp32_peak": (_I, [_I, _D]),
+    "p3m_gf_opt_static": (_I, [ctypes.c_double, ctypes.c_double, _I, _I, _I, ctypes.c_double, _V,
+                               _V, _V]),
+    "p3m_gf_opt_static_error": (ctypes.c_char_p, []),
 }
 
 
