@@ -317,8 +317,11 @@ def run_ours(args):
                     "velocities)",
             "config": {"workload": WORKLOAD, "replicas": len(reps), "N_per_replica": reps[0].N,
                        "mesh": reps[0].M, "parallelism": f"replicas x{world}" if world > 1 else "replicas",
-                       "l2": f"inputs larger than L2 (working set {working_set_mb(reps):.0f} MB > 126 MB)",
-                       "pp_config": list(ctx.pp_config())},
+                       "l2": (f"inputs larger than L2 (working set {working_set_mb(reps):.0f} MB > 126 MB)"
+                              if working_set_mb(reps) > 126 else
+                              f"working set {working_set_mb(reps):.0f} MB fits L2; no flush"),
+                       "pp_config": dict(zip(("threads_per_particle", "skin", "list_capacity"),
+                                             ctx.pp_config()))},
             "gpu_launches": launches, "clocks": clocks}
 
     if not args.no_extras and rank == 0:

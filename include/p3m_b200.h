@@ -38,6 +38,7 @@ extern "C" {
 #define P3M_EBOX (-4)          /* particle outside [-L, 2L) or non-finite     */
 #define P3M_ENONFINITE (-5)    /* NaN/Inf in forces or energies               */
 #define P3M_ESTATE (-6)        /* call out of order (e.g. no state uploaded)  */
+#define P3M_ENBOVF (-7)        /* neighbour-list capacity exceeded            */
 
 /* arithmetic of the bulk stages (PP pair loop, assignment, FFT, gather) */
 #define P3M_FP64 0             /* everything in FP64: the plain method        */
@@ -63,6 +64,7 @@ typedef struct {
     double dt;          /* time step                                         */
     double t_desired;   /* thermostat target temperature (1/Gamma)           */
     double af, uf, kf;  /* acceleration, energy and kinetic-energy factors    */
+    double skin;        /* Verlet-list skin (< 0: default 0.5; <= rc/2)       */
 } p3m_replica_desc;
 
 /* ---- context ---------------------------------------------------------- */
@@ -184,11 +186,13 @@ int p3m_check(p3m_ctx *ctx);
 /* Wait for all work on the context's stream. */
 int p3m_sync(p3m_ctx *ctx);
 
-/* PP work decomposition: threads per i-particle (1, 2, 4) and CTAs per cell
- * (1..4). p3m_create picks a default from the cell count; the autotuner of the
- * Python package times the candidates and installs the fastest. */
-int p3m_set_pp_config(p3m_ctx *ctx, int tpi, int split);
-int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, int *split);
+/* PP configuration: threads per particle in the force kernel (1, 2, 4, 8)
+ * and the Verlet-list skin for every replica (< 0: each replica's own /
+ * default). p3m_create picks tpi from the particle count; the autotuner of
+ * the Python package times candidates and installs the fastest. Forces a
+ * list rebuild. get returns tpi, replica 0's skin and the list capacity. */
+int p3m_set_pp_config(p3m_ctx *ctx, int tpi, double skin);
+int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, double *skin, int *maxnb);
 
 /* Measurement: average device time (ms) of each step stage over `iters`
  * back-to-back launches, timed with CUDA events on the context's stream.

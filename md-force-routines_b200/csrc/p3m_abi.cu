@@ -25,6 +25,7 @@ struct p3m_ctx {
     int ring_rows = 0;            // rows written (host-side tally)
     double *qmult = nullptr;      // [nq]
     int nq = 0, nqt_cap = 0;
+    int nq_consecutive = 0;       // qmult == 1, 2, ..., nq
     double *nqt_part = nullptr;   // [nblk][nq*6]
     double *nqt_ring = nullptr;   // [cap][nrep][nq*6]
     int nqt_rows = 0;
@@ -36,13 +37,16 @@ struct p3m_ctx {
     size_t hbuf_bytes = 0;
     bool state_set = false;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int ncell_cap = 0;            // cells allocated (grid with skin 0)
+    long long nlist_cap = 0;      // list entries allocated
+    int pp_nblk_cap = 0;          // PP blocks allocated (tpi = 8)
     long long launches = 0;
     std::string err;
 };
 
 static thread_local std::string g_err;
 
-#define P3M_VERSION 100
+#define P3M_VERSION 200
 
 #define CK(call)                                                                      \
     do {                                                                              \
@@ -102,19 +106,72 @@ static int check_device(p3m_ctx *ctx, int device)
 
 template <typename T> static size_t tsize() { return sizeof(T); }
 
-static int pp_default_split(int ncell, int ntot, int *tpi)
+// Default Verlet skin (a_ws): a list rebuild when a particle has moved skin/2.
+static const double kDefaultSkin = 0.5;
+
+// Yukawa-Ewald pair functions on the host, in FP64: g(r) = F(r) r^2 and
+// psi(r) = phi(r) r (F and phi of yukawa_pp.py:115,121-124, multiplied out so
+// both are finite at r = 0).
+static void pair_g_psi(double r, double kappa, double a, double *g, double *psi)
 {
-    const int target = 148 * 8;
-    const int navg = ntot / (ncell > 0 ? ncell : 1);
-    if (ncell >= target) {
-        *tpi = 1;
-        return navg > 128 ? 2 : 1;
+    const double up = a * r + 0.5 * kappa / a, um = a * r - 0.5 * kappa / a;
+    const double ep = exp(kappa * r) * erfc(up), em = exp(-kappa * r) * erfc(um);
+    *psi = 0.5 * (ep + em);
+    *g = 0.5 * (ep * (1.0 - kappa * r) + em * (1.0 + kappa * r)) +
+         (a / sqrt(M_PI)) * r * (exp(-up * up) * exp(kappa * r) + exp(-um * um) * exp(-kappa * r));
+}
+
+// Cubic per interval through the samples at u = 0, 1/3, 2/3, 1 (monomial
+// coefficients in u), for g and psi: 2 float4 per interval.
+static void build_pp_table(const p3m_replica_desc &d, float4 *out)
+{
+    const double h = d.rc / PP_TABLE_N;
+    for (int i = 0; i < PP_TABLE_N; ++i) {
+        double fg[4], fp[4];
+        for (int k = 0; k < 4; ++k) pair_g_psi((i + k / 3.0) * h, d.kappa, d.alpha, &fg[k], &fp[k]);
+        auto coef = [](const double *f, float4 &c) {
+            c.x = (float)f[0];
+            c.y = (float)((-11.0 * f[0] + 18.0 * f[1] - 9.0 * f[2] + 2.0 * f[3]) / 2.0);
+            c.z = (float)((18.0 * f[0] - 45.0 * f[1] + 36.0 * f[2] - 9.0 * f[3]) / 2.0);
+            c.w = (float)((-9.0 * f[0] + 27.0 * f[1] - 27.0 * f[2] + 9.0 * f[3]) / 2.0);
+        };
+        coef(fg, out[2 * i]);
+        coef(fp, out[2 * i + 1]);
     }
-    *tpi = 4;
-    int chunks = (navg + 31) / 32;
-    int want = (target + ncell - 1) / ncell;
-    int split = chunks < want ? chunks : want;
-    return split < 1 ? 1 : split;
+}
+
+// Cell grid (cells >= rc + skin, at least 3 per side), list capacity and
+// PP block layout of every replica for a given skin and threads-per-particle.
+// Updates ctx->rh and ctx->s counts; the caller uploads and (re)allocates.
+static void plan_lists(p3m_ctx *ctx, double skin_override, int tpi)
+{
+    DevState &s = ctx->s;
+    int cell = 0, blk = 0;
+    double maxmean = 0.0;
+    const int ppb = pp_particles_per_block(tpi);
+    for (int r = 0; r < ctx->nrep; ++r) {
+        const p3m_replica_desc &d = ctx->desc[r];
+        RepDev &R = ctx->rh[r];
+        double skin = skin_override >= 0.0 ? skin_override : (d.skin >= 0.0 ? d.skin : kDefaultSkin);
+        const double smax = d.box / 3.0 * (1.0 - 1e-12) - d.rc;  // keeps >= 3 cells per side
+        if (skin > smax) skin = smax > 0.0 ? smax : 0.0;
+        R.skin = skin;
+        R.rcl = d.rc + skin;
+        R.nc = (int)floor(d.box / R.rcl);
+        if (R.nc < 3) R.nc = 3;
+        R.cellw = d.box / R.nc;
+        R.inv_cellw = 1.0 / R.cellw;
+        R.cell_off = cell;
+        cell += R.nc * R.nc * R.nc;
+        R.pp_blk_off = blk;
+        blk += (d.n + ppb - 1) / ppb;
+        const double mean = 4.0 / 3.0 * M_PI * d.n / (d.box * d.box * d.box) * R.rcl * R.rcl * R.rcl;
+        if (mean > maxmean) maxmean = mean;
+    }
+    s.ncell = cell;
+    s.pp_tpi = tpi;
+    s.pp_nblk = blk;
+    s.maxnb = ((int)ceil(1.5 * maxmean + 64.0) + 7) / 8 * 8;
 }
 
 extern "C" int p3m_version(void) { return P3M_VERSION; }
@@ -135,7 +192,8 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
             if (g) cudaGraphExecDestroy(g);
     DevState &s = ctx->s;
     void *ptrs[] = {s.reps, s.pos, s.vel, s.acc, s.charge, s.prep, s.cell_key, s.cell_count,
-                    s.cell_start, s.cell_cursor, s.cell_tmp, s.cell_perm, s.cell_slot, s.xs_cell,
+                    s.cell_start, s.cell_cursor, s.cell_tmp, s.cell_perm, s.cell_slot, s.xq, s.nnb,
+                    s.nlist, s.rebuild, s.pos_ref, s.pp_tables,
                     s.acc_pp, s.brick_key, s.brick_count, s.brick_start, s.brick_cursor,
                     s.brick_perm, s.brick_slot, s.tiles, s.spec, s.ek, s.green, s.efield,
                     s.acc_pm, s.twiddle, s.u_pp_part, s.u_pm_part, s.kin_part, s.rep_out,
@@ -154,7 +212,7 @@ template <typename T> static int alloc_bulk(p3m_ctx *ctx)
     using T4 = typename V4<T>::t;
     using C = typename C2<T>::t;
     DevState &s = ctx->s;
-    CK(valloc(&s.xs_cell, (size_t)s.ntot * sizeof(double4)));
+    CK(valloc(&s.xq, (size_t)s.ntot * (sizeof(T) == 4 ? sizeof(uint4) : sizeof(ulonglong4))));
     CK(valloc(&s.acc_pp, (size_t)s.ntot * sizeof(T4)));
     if (s.has_mesh) {
         CK(valloc(&s.acc_pm, (size_t)s.ntot * sizeof(T4)));
@@ -206,6 +264,8 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
             snprintf(why, sizeof why, "replica %d: only charge-assignment order 6 is supported", r);
         else if (d.m_alias < 0 || d.m_alias > 7)
             snprintf(why, sizeof why, "replica %d: m_alias must be in [0, 7]", r);
+        else if (d.skin > 0.5 * d.rc)
+            snprintf(why, sizeof why, "replica %d: skin must be <= rc/2 (negative: default)", r);
         if (why[0]) return fail(nullptr, P3M_EARG, "p3m_create", why);
     }
     p3m_ctx *ctx = new p3m_ctx();
@@ -225,7 +285,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     s.has_mesh = with_mesh;
     ctx->rh.resize(n_reps);
     long long mesh = 0, spec = 0, tile = 0;
-    int p = 0, cell = 0, brick = 0, wa = 0, wb = 0, wc = 0, blk = 0, maxm = 0;
+    int p = 0, cell = 0, brick = 0, wa = 0, wb = 0, wc = 0, wp = 0, blk = 0, maxm = 0, maxp = 0;
     for (int r = 0; r < n_reps; ++r) {
         const p3m_replica_desc &d = reps[r];
         RepDev &R = ctx->rh[r];
@@ -236,15 +296,11 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
         R.kappa = d.kappa;
         R.alpha = d.alpha;
         R.rc = d.rc;
-        R.nc = (int)floor(d.box / d.rc);
-        R.cellw = d.box / R.nc;
-        R.cell_off = cell;
         R.dt = d.dt;
         R.t_desired = d.t_desired;
         R.af = d.af;
         R.uf = d.uf;
         R.kf = d.kf;
-        R.inv_cellw = 1.0 / R.cellw;
         R.inv_L = 1.0 / d.box;
         R.inv_V = 1.0 / (d.box * d.box * d.box);
         R.blk_off = blk;
@@ -262,26 +318,44 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
             R.wa_off = wa;
             R.wb_off = wb;
             R.wc_off = wc;
+            R.wp_off = wp;
             brick += R.nb * R.nb * R.nb;
             mesh += (long long)M * M * M;
             spec += (long long)(M / 2 + 1) * M * M;
             tile += (long long)R.nb * R.nb * R.nb * TILE3;
             wa += M * (M / (2 * PENCIL));
-            wb += (M / 2 + 1) * (M / PENCIL);
-            wc += (M / 2 + 1) * (M / PENCIL);
+            if (M <= plane_max_mesh()) {
+                wp += M / 2 + 1;
+                if (M > maxp) maxp = M;
+            } else {
+                wb += (M / 2 + 1) * (M / PENCIL);
+                wc += (M / 2 + 1) * (M / PENCIL);
+            }
             if (M > maxm) maxm = M;
         } else {
             R.brick_off = brick;
             R.wa_off = wa;
             R.wb_off = wb;
             R.wc_off = wc;
+            R.wp_off = wp;
         }
         p += d.n;
-        cell += R.nc * R.nc * R.nc;
+        {
+            const int ncmax = (int)floor(d.box / d.rc);  // the finest grid any skin can ask for
+            cell += ncmax * ncmax * ncmax;
+        }
         blk += (d.n + PBLK - 1) / PBLK;
     }
+    {
+        int qb = 0;
+        for (int r = 0; r < n_reps; ++r) {
+            ctx->rh[r].nq_blk_off = qb;
+            qb += (reps[r].n + nqt_particles_per_block() - 1) / nqt_particles_per_block();
+        }
+        s.nq_nblk = qb;
+    }
     s.ntot = p;
-    s.ncell = cell;
+    ctx->ncell_cap = cell;
     s.nbrick = brick;
     s.nmesh = mesh;
     s.nspec = spec;
@@ -289,9 +363,11 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     s.wa = wa;
     s.wb = wb;
     s.wc = wc;
+    s.wp = wp;
+    s.max_plane = maxp;
     s.nblk = blk;
     s.max_mesh = maxm;
-    s.pp_split = pp_default_split(cell, p, &s.pp_tpi);
+    plan_lists(ctx, -1.0, p >= 148 * 256 * 2 ? 1 : (p >= 148 * 64 ? 2 : 4));
 
     auto cleanup = [&](int code) {
         std::string e = ctx->err;
@@ -310,6 +386,12 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
     CKC(dalloc(&s.reps, n_reps));
     CKC(cudaMemcpy(s.reps, ctx->rh.data(), sizeof(RepDev) * n_reps, cudaMemcpyHostToDevice));
+    {
+        std::vector<float4> tab((size_t)n_reps * 2 * PP_TABLE_N);
+        for (int r = 0; r < n_reps; ++r) build_pp_table(reps[r], tab.data() + (size_t)r * 2 * PP_TABLE_N);
+        CKC(dalloc(&s.pp_tables, tab.size()));
+        CKC(cudaMemcpy(s.pp_tables, tab.data(), sizeof(float4) * tab.size(), cudaMemcpyHostToDevice));
+    }
     CKC(dalloc(&s.pos, (size_t)3 * p));
     CKC(dalloc(&s.vel, (size_t)3 * p));
     CKC(dalloc(&s.acc, (size_t)3 * p));
@@ -324,9 +406,14 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
         CKC(cudaMemcpy(s.prep, pr.data(), sizeof(int) * p, cudaMemcpyHostToDevice));
     }
     CKC(dalloc(&s.cell_key, (size_t)p));
-    CKC(dalloc(&s.cell_count, (size_t)cell));
-    CKC(dalloc(&s.cell_start, (size_t)cell + 1));
-    CKC(dalloc(&s.cell_cursor, (size_t)cell));
+    CKC(dalloc(&s.cell_count, (size_t)ctx->ncell_cap));
+    CKC(dalloc(&s.cell_start, (size_t)ctx->ncell_cap + 1));
+    CKC(dalloc(&s.cell_cursor, (size_t)ctx->ncell_cap));
+    CKC(dalloc(&s.nnb, (size_t)p));
+    ctx->nlist_cap = (long long)((p + 31) / 32) * 32 * s.maxnb;
+    CKC(dalloc(&s.nlist, (size_t)ctx->nlist_cap));
+    CKC(dalloc(&s.rebuild, (size_t)n_reps));
+    CKC(dalloc(&s.pos_ref, (size_t)3 * p));
     CKC(dalloc(&s.cell_tmp, (size_t)p));
     CKC(dalloc(&s.cell_perm, (size_t)p));
     CKC(dalloc(&s.cell_slot, (size_t)p));
@@ -336,9 +423,15 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(dalloc(&s.brick_cursor, (size_t)brick));
     CKC(dalloc(&s.brick_perm, (size_t)p));
     CKC(dalloc(&s.brick_slot, (size_t)p));
-    if (with_mesh) CKC(dalloc(&s.tiles, (size_t)tile));
-    CKC(dalloc(&s.u_pp_part, (size_t)cell * 4));
-    CKC(dalloc(&s.u_pm_part, (size_t)wc));
+    if (with_mesh)
+        CKC(valloc(&s.tiles, (size_t)tile * (precision == P3M_FP32 ? sizeof(float) : sizeof(double))));
+    {
+        int nb8 = 0;
+        for (int r = 0; r < n_reps; ++r) nb8 += (reps[r].n + pp_particles_per_block(8) - 1) / pp_particles_per_block(8);
+        ctx->pp_nblk_cap = nb8;
+        CKC(dalloc(&s.u_pp_part, (size_t)nb8));
+    }
+    CKC(dalloc(&s.u_pm_part, (size_t)wc + wp));
     CKC(dalloc(&s.kin_part, (size_t)blk));
     CKC(dalloc(&s.rep_out, (size_t)8 * n_reps));
     CKC(dalloc(&s.status, 1));
@@ -353,6 +446,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(dalloc(&ctx->ep, (size_t)3 * p));
     int arc = (precision == P3M_FP32) ? alloc_bulk<float>(ctx) : alloc_bulk<double>(ctx);
     if (arc != P3M_OK) return cleanup(arc);
+    launch_set_flags(s.rebuild, n_reps, 1, ctx->st);  // no lists exist yet
     CKC(cudaGetLastError());
     CKC(cudaDeviceSynchronize());
 #undef CKC
@@ -364,17 +458,27 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
 // internal sequences (enqueue only)
 // ---------------------------------------------------------------------------
 
+// Cell sort and list build. keys = true (compat calls, initial forces):
+// force a rebuild and key every particle here. keys = false (inside a step):
+// the drift kernel keyed the bricks and raised the rebuild flag if needed;
+// the cell part runs only when the flag is set.
 template <typename T> static void seq_sort(p3m_ctx *ctx, bool keys)
 {
     DevState &s = ctx->s;
     if (keys) {
+        launch_set_flags(s.rebuild, s.nrep, 1, ctx->st);
         launch_keys<T>(s, ctx->st);
+        ctx->launches += 2;
+    } else {
+        launch_cell_keys(s, ctx->st);
         ctx->launches++;
     }
     launch_scan(s, ctx->st);
     launch_scatter(s, ctx->st);
     launch_fix_cells<T>(s, ctx->st);
-    ctx->launches += 3;
+    launch_quantize<T>(s, ctx->st);     // sorted coordinates of this step
+    launch_build_lists<T>(s, ctx->st);  // from those coordinates (rebuild steps)
+    ctx->launches += 5;
 }
 
 template <typename T> static void seq_pp(p3m_ctx *ctx)
@@ -392,7 +496,7 @@ template <typename T> static void seq_pm(p3m_ctx *ctx)
     launch_reduce_pm(s, ctx->st);
     launch_fft_inverse<T>(s, ctx->st);
     launch_gather<T>(s, ctx->st);
-    ctx->launches += 8;
+    ctx->launches += 3 + fft_kernel_count(s);
 }
 
 // Compute the influence function of every replica that has none yet.
@@ -443,8 +547,8 @@ template <typename T> static void seq_step(p3m_ctx *ctx, int mode, int record_nq
         ctx->launches++;
     }
     if (record_nqt && ctx->nq > 0) {
-        launch_nqt<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nqt_part, ctx->nqt_ring, ctx->counters,
-                      ctx->nqt_cap, ctx->st);
+        launch_nqt<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nq_consecutive, ctx->nqt_part,
+                      ctx->nqt_ring, ctx->counters, ctx->nqt_cap, ctx->st);
         ctx->launches += 2;
     }
 }
@@ -479,6 +583,9 @@ static int finish(p3m_ctx *ctx)
         CK(cudaMemset(ctx->s.status, 0, sizeof(int)));
         if (st & ST_BOX) return fail(ctx, P3M_EBOX, "particle outside [-L, 2L) or non-finite position", "");
         if (st & ST_NONFINITE) return fail(ctx, P3M_ENONFINITE, "non-finite force or energy", "");
+        if (st & ST_NBOVF)
+            return fail(ctx, P3M_ENBOVF, "a particle has more neighbours than the list holds",
+                        "raise the capacity with a smaller skin or report the density");
     }
     return P3M_OK;
 }
@@ -735,7 +842,8 @@ static int do_update(p3m_ctx *ctx, int mode, int it, double *pos, double *vel, d
     RET(h2d(ctx, s.acc, acc, b));
     if (s.has_mesh) RET(ensure_green<T>(ctx));
     launch_set_counters(ctx->counters, 0, -1, it, ctx->st);
-    ctx->launches++;
+    launch_set_flags(s.rebuild, s.nrep, 1, ctx->st);  // the caller's arrays may hold any state
+    ctx->launches += 2;
     seq_step<T>(ctx, mode, 0);
     RET(d2h(ctx, pos, s.pos, b));
     RET(d2h(ctx, vel, s.vel, b));
@@ -782,7 +890,7 @@ static int do_nqt(p3m_ctx *ctx, int replica, const double *pos, const double *qv
     for (int k = 0; k < nq; ++k) qmult[k] = qv[k] * R.L / (2.0 * 3.141592653589793238);
     RET(h2d(ctx, s.pos + 3 * (size_t)R.p_off, pos, sizeof(double) * 3 * R.n));
     CK(cudaMemcpyAsync(qm, qmult.data(), sizeof(double) * nq, cudaMemcpyHostToDevice, ctx->st));
-    launch_nqt<T>(s, s.pos, qm, nq, part, o, nullptr, 0, ctx->st);
+    launch_nqt<T>(s, s.pos, qm, nq, 0, part, o, nullptr, 0, ctx->st);
     ctx->launches += 2;
     RET(d2h(ctx, out, o + (size_t)replica * nq * 6, sizeof(double) * nq * 6));
     RET(finish(ctx));
@@ -815,6 +923,7 @@ extern "C" int p3m_set_state(p3m_ctx *ctx, int replica, const double *pos, const
     if (pos) RET(h2d(ctx, ctx->s.pos + o, pos, b));
     if (vel) RET(h2d(ctx, ctx->s.vel + o, vel, b));
     if (acc) RET(h2d(ctx, ctx->s.acc + o, acc, b));
+    if (pos) launch_set_flags(ctx->s.rebuild, ctx->s.nrep, 1, ctx->st);
     ctx->state_set = true;
     return finish(ctx);
 }
@@ -867,7 +976,10 @@ extern "C" int p3m_set_nqt(p3m_ctx *ctx, const double *qmult, int nq, int capaci
     if (nq == 0) return P3M_OK;
     CK(dalloc(&ctx->qmult, (size_t)nq));
     CK(cudaMemcpy(ctx->qmult, qmult, sizeof(double) * nq, cudaMemcpyHostToDevice));
-    CK(dalloc(&ctx->nqt_part, (size_t)ctx->s.nblk * nq * 6));
+    ctx->nq_consecutive = 1;
+    for (int k = 0; k < nq; ++k)
+        if (qmult[k] != (double)(k + 1)) ctx->nq_consecutive = 0;
+    CK(dalloc(&ctx->nqt_part, (size_t)ctx->s.nq_nblk * nq * 6));
     CK(dalloc(&ctx->nqt_ring, (size_t)capacity * ctx->nrep * nq * 6));
     // ring positions restart at 0
     launch_set_counters(ctx->counters, -1, 0, 0, ctx->st);
@@ -900,7 +1012,7 @@ template <typename T> static int do_run(p3m_ctx *ctx, int n_steps, int mode, int
             const long long before = ctx->launches;
             CK(cudaGraphLaunch(ctx->graph[gi][gr], ctx->st));
             // count the kernels the graph holds (same sequence as seq_step)
-            ctx->launches = before + (long long)(8 + (s.has_mesh ? 8 : 0) + (gi ? 1 : 0) +
+            ctx->launches = before + (long long)(11 + (s.has_mesh ? 3 + fft_kernel_count(s) : 0) + (gi ? 1 : 0) +
                                                  ((gr && ctx->nq > 0) ? 2 : 0));
         } else {
             seq_step<T>(ctx, mode, rec);
@@ -981,26 +1093,39 @@ extern "C" int p3m_sync(p3m_ctx *ctx)
     return P3M_OK;
 }
 
-extern "C" int p3m_set_pp_config(p3m_ctx *ctx, int tpi, int split)
+extern "C" int p3m_set_pp_config(p3m_ctx *ctx, int tpi, double skin)
 {
     if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
-    if (!(tpi == 1 || tpi == 2 || tpi == 4) || split < 1 || split > 4)
-        return fail(ctx, P3M_EARG, "p3m_set_pp_config", "tpi in {1,2,4}, split in [1,4]");
+    if (!(tpi == 1 || tpi == 2 || tpi == 4 || tpi == 8))
+        return fail(ctx, P3M_EARG, "p3m_set_pp_config", "tpi must be 1, 2, 4 or 8");
+    for (int r = 0; r < ctx->nrep; ++r)
+        if (skin > 0.5 * ctx->desc[r].rc)
+            return fail(ctx, P3M_EARG, "p3m_set_pp_config", "skin must be <= rc/2 (negative: default)");
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->st));
-    ctx->s.pp_tpi = tpi;
-    ctx->s.pp_split = split;
     for (auto &row : ctx->graph)
         for (auto &g : row)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-    return P3M_OK;
+    DevState &s = ctx->s;
+    plan_lists(ctx, skin, tpi);
+    const long long need = (long long)((s.ntot + 31) / 32) * 32 * s.maxnb;
+    if (need > ctx->nlist_cap) {
+        cudaFree(s.nlist);
+        s.nlist = nullptr;
+        CK(dalloc(&s.nlist, (size_t)need));
+        ctx->nlist_cap = need;
+    }
+    CK(cudaMemcpy(s.reps, ctx->rh.data(), sizeof(RepDev) * ctx->nrep, cudaMemcpyHostToDevice));
+    launch_set_flags(s.rebuild, s.nrep, 1, ctx->st);
+    return finish(ctx);
 }
 
-extern "C" int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, int *split)
+extern "C" int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, double *skin, int *maxnb)
 {
-    if (!ctx || !tpi || !split) return fail(ctx, P3M_EARG, "p3m_get_pp_config", "NULL argument");
+    if (!ctx || !tpi || !skin || !maxnb) return fail(ctx, P3M_EARG, "p3m_get_pp_config", "NULL argument");
     *tpi = ctx->s.pp_tpi;
-    *split = ctx->s.pp_split;
+    *skin = ctx->rh[0].skin;
+    *maxnb = ctx->s.maxnb;
     return P3M_OK;
 }
 
@@ -1031,11 +1156,14 @@ template <typename T> static void enqueue_stage(p3m_ctx *ctx, int k)
     case 1: seq_sort<T>(ctx, true); break;
     case 2: seq_pp<T>(ctx); break;
     case 3: launch_assign<T>(s, ctx->st); ctx->launches++; break;
-    case 4: launch_fft_forward<T>(s, ctx->st); ctx->launches += 3; break;
+    case 4:
+        launch_fft_forward<T>(s, ctx->st);
+        ctx->launches += fft_kernel_count(s) - 1 - (s.wb > 0 ? 1 : 0);
+        break;
     case 5:
         launch_fft_forward<T>(s, ctx->st);
         launch_fft_inverse<T>(s, ctx->st);
-        ctx->launches += 5;
+        ctx->launches += fft_kernel_count(s);
         break;
     case 6: launch_gather<T>(s, ctx->st); ctx->launches++; break;
     case 7:
@@ -1045,8 +1173,8 @@ template <typename T> static void enqueue_stage(p3m_ctx *ctx, int k)
         break;
     case 8:
         if (ctx->nq > 0) {
-            launch_nqt<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nqt_part, ctx->tmp_nq ? ctx->tmp_nq : ctx->nqt_part,
-                          nullptr, 0, ctx->st);
+            launch_nqt<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nq_consecutive, ctx->nqt_part,
+                          ctx->tmp_nq ? ctx->tmp_nq : ctx->nqt_part, nullptr, 0, ctx->st);
             ctx->launches += 2;
         }
         break;

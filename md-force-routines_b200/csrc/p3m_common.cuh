@@ -25,7 +25,11 @@ constexpr int PBLK = 256;    // particles per block in replica-aligned particle 
 enum : int {
     ST_BOX = 1,        // particle outside [-L, 2L) or position not finite
     ST_NONFINITE = 2,  // NaN/Inf in forces or energies
+    ST_NBOVF = 4,      // a particle has more list neighbours than the list holds
 };
+
+// Intervals of the tabulated FP32 pair functions on [0, rc].
+constexpr int PP_TABLE_N = 1024;
 
 // Per-replica constants. Offsets index the concatenated device arrays.
 struct RepDev {
@@ -38,10 +42,14 @@ struct RepDev {
     long long tile_off;    // offset into assignment tiles (nb^3 TILE^3)
     // work-item offsets of the mesh passes (prefix sums over replicas)
     int wa_off;            // x-R2C / x-C2R items: M * M/(2 PENCIL)
-    int wb_off;            // y-line items: (M/2+1) * M/PENCIL
-    int wc_off;            // z-line items: (M/2+1) * M/PENCIL
+    int wb_off;            // y-line items: (M/2+1) * M/PENCIL (multi-pass replicas)
+    int wc_off;            // z-line items: (M/2+1) * M/PENCIL (multi-pass replicas)
+    int wp_off;            // plane items: M/2+1 (replicas with M <= PLANE_MAX)
     int blk_off;           // offset of this replica's particle blocks (PBLK each)
+    int pp_blk_off;        // offset of this replica's blocks in the PP force kernel
+    int nq_blk_off;        // offset of this replica's blocks in the n(q,t) kernel
     double L, kappa, alpha, rc, cellw, h, dt, t_desired, af, uf, kf;
+    double skin, rcl;      // Verlet skin and list cutoff rc + skin
     double inv_cellw, inv_h, inv_L, inv_V;
 };
 
@@ -112,6 +120,24 @@ __device__ __forceinline__ void raise_status(int *status, int bit)
     atomicOr(status, bit);
 }
 
+// Asynchronous global -> shared copies (cp.async, 4 or 8 bytes per thread),
+// so a block can have all of a tile's loads in flight at once.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem_dst, const void *gmem_src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gmem_src), "n"(BYTES));
+}
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src));
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // One periodic fold by a box length (positions are kept in [-L, 2L)).
 __device__ __forceinline__ double fold_box(double x, double L)
 {
@@ -129,6 +155,7 @@ __device__ __forceinline__ int fold_index(int i, int M)
 
 // PP cell and mesh brick of a particle (see p3m_sort.cu). Raises ST_BOX and
 // files the particle under cell 0 when it is outside [-L, 2L) or not finite.
+// cell == nullptr skips the cell key.
 __device__ __forceinline__ void particle_keys(const RepDev &R, double x, double y, double z,
                                               int has_mesh, int *cell, int *brick, int *status)
 {
@@ -138,11 +165,13 @@ __device__ __forceinline__ void particle_keys(const RepDev &R, double x, double 
         raise_status(status, ST_BOX);
         x = y = z = 0.0;
     }
-    const double xw = fold_box(x, L), yw = fold_box(y, L), zw = fold_box(z, L);
-    const int cx = min((int)floor(xw / R.cellw), R.nc - 1);
-    const int cy = min((int)floor(yw / R.cellw), R.nc - 1);
-    const int cz = min((int)floor(zw / R.cellw), R.nc - 1);
-    *cell = R.cell_off + cx + R.nc * (cy + R.nc * cz);
+    if (cell) {
+        const double xw = fold_box(x, L), yw = fold_box(y, L), zw = fold_box(z, L);
+        const int cx = min((int)floor(xw / R.cellw), R.nc - 1);
+        const int cy = min((int)floor(yw / R.cellw), R.nc - 1);
+        const int cz = min((int)floor(zw / R.cellw), R.nc - 1);
+        *cell = R.cell_off + cx + R.nc * (cy + R.nc * cz);
+    }
     *brick = -1;
     if (has_mesh && R.M > 0) {
         const int ix = fold_index((int)floor(x / R.h), R.M);

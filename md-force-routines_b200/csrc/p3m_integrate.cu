@@ -34,24 +34,29 @@ __device__ __forceinline__ double wrap_once(double x, double L)
 
 __global__ void k_kick_drift(const RepDev *__restrict__ reps, const int *__restrict__ prep,
                              double *__restrict__ pos, double *__restrict__ vel,
-                             const double *__restrict__ acc, int ntot, int *__restrict__ cell_key,
-                             int *__restrict__ cell_count, int *__restrict__ brick_key,
-                             int *__restrict__ brick_count, int has_mesh, int *status)
+                             const double *__restrict__ acc, const double *__restrict__ pos_ref,
+                             int ntot, int *__restrict__ brick_key, int *__restrict__ brick_count,
+                             int has_mesh, int *rebuild, int *status)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
-        const RepDev &R = reps[prep[i]];
+        const int r = prep[i];
+        const RepDev &R = reps[r];
         double x[3];
+        double d2 = 0.0;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             double v = kick(vel[3 * i + d], acc[3 * i + d], R.dt);
             vel[3 * i + d] = v;
             x[d] = wrap_once(__dadd_rn(pos[3 * i + d], __dmul_rn(v, R.dt)), R.L);
             pos[3 * i + d] = x[d];
+            // displacement since the last list rebuild, minimum image
+            double dd = x[d] - pos_ref[3 * i + d];
+            dd -= R.L * rint(dd * R.inv_L);
+            d2 += dd * dd;
         }
-        int c, b;
-        particle_keys(R, x[0], x[1], x[2], has_mesh, &c, &b, status);
-        cell_key[i] = c;
-        atomicAdd(&cell_count[c], 1);
+        if (d2 > 0.25 * R.skin * R.skin && !rebuild[r]) atomicOr(rebuild + r, 1);
+        int b;
+        particle_keys(R, x[0], x[1], x[2], has_mesh, nullptr, &b, status);
         if (b >= 0) {
             brick_key[i] = b;
             atomicAdd(&brick_count[b], 1);
@@ -121,7 +126,7 @@ k_kick_finish(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
 __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nblk,
                               const double *__restrict__ kin_part, double *__restrict__ rep_out,
                               int mode, int *__restrict__ counters, double *__restrict__ ring,
-                              int ring_cap, int *status)
+                              int ring_cap, int *rebuild, int *status)
 {
     // counters: [0] steps since the run started, [1] ring position, [2] step
     // index of the run's first step (thermostat_p3m_ord6.py:15 tests it<=1999)
@@ -162,10 +167,22 @@ __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nbl
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0 && mode != 2) {
-        counters[0] += 1;
-        counters[1] = step + 1;
+    if (threadIdx.x == 0) {
+        if (mode != 2) {
+            counters[0] += 1;
+            counters[1] = step + 1;
+        }
     }
+    // this step's lists are built (count them); the next drift decides again
+    for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
+        if (rebuild[r] && mode != 2) rep_out[8 * r + RO_REBUILDS] += 1.0;
+        rebuild[r] = 0;
+    }
+}
+
+__global__ void k_set_flags(int *flag, int n, int value)
+{
+    for (int r = threadIdx.x; r < n; r += blockDim.x) flag[r] = value;
 }
 
 __global__ void k_set_counters(int *counters, int run_step, int ring_pos, int it0)
@@ -223,64 +240,109 @@ __global__ void k_scale_vel(const RepDev *__restrict__ reps, const int *__restri
     }
 }
 
-// n(q,t) partial sums: per replica-aligned block, for each wave number q_m =
-// m 2 pi / L (m = qmult[iq]) and axis, sum_i exp(-i q x_i)
-// (yukawa_MD_p3m_ord6.py:215-219). The phase is reduced in FP64 as
-// frac(m x / L) before the sine/cosine of the bulk precision T.
+// n(q,t) partial sums: per replica-aligned block of NQ_PPT * PBLK particles,
+// for each wave number q_m = m 2 pi / L (m = qmult[iq]) and axis,
+// sum_i exp(-i q x_i) (yukawa_MD_p3m_ord6.py:215-219). Each thread sums
+// NQ_PPT particles before the block reduction. The phase is reduced in FP64
+// as frac(m x / L) before the sine/cosine of the bulk precision T; when the
+// multiples are 1, 2, ..., nq (`consecutive`), exp(-i m theta) follows from
+// exp(-i theta) by complex multiplication instead.
+constexpr int NQ_PPT = 4;
+
+template <typename T>
+__device__ __forceinline__ void sincospi_t(double two_t, T *s, T *c)
+{
+    if (sizeof(T) == 4) {
+        float sf, cf;
+        sincospif((float)two_t, &sf, &cf);
+        *s = (T)sf;
+        *c = (T)cf;
+    } else {
+        double sd, cd;
+        sincospi(two_t, &sd, &cd);
+        *s = (T)sd;
+        *c = (T)cd;
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(PBLK)
 k_nqt_partial(const RepDev *__restrict__ reps, int nrep, const double *__restrict__ pos,
-              const double *__restrict__ qmult, int nq, double *__restrict__ part)
+              const double *__restrict__ qmult, int nq, int consecutive, double *__restrict__ part)
 {
     extern __shared__ double nsm[];  // [nwarps][nq*6]
     const int b = blockIdx.x;
-    const int r = block_replica(reps, nrep, b);
+    const int r = find_rep(b, nrep, [&](int k) { return reps[k].nq_blk_off; });
     const RepDev &R = reps[r];
-    const int i = R.p_off + (b - R.blk_off) * PBLK + threadIdx.x;
-    const bool have = i < R.p_off + R.n;
+    const int first = R.p_off + (b - R.nq_blk_off) * (PBLK * NQ_PPT);
+    const int end = R.p_off + R.n;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    double xl[3] = {0, 0, 0};
-    if (have) {
-        xl[0] = pos[3 * i + 0] * R.inv_L;
-        xl[1] = pos[3 * i + 1] * R.inv_L;
-        xl[2] = pos[3 * i + 2] * R.inv_L;
+    double xl[NQ_PPT][3];
+    bool have[NQ_PPT];
+#pragma unroll
+    for (int m = 0; m < NQ_PPT; ++m) {
+        const int i = first + threadIdx.x + m * PBLK;
+        have[m] = i < end;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) xl[m][d] = have[m] ? pos[3 * i + d] * R.inv_L : 0.0;
+    }
+    // per-particle base rotation exp(-i 2 pi x/L) for the recurrence
+    T c1[NQ_PPT][3], s1[NQ_PPT][3], cm[NQ_PPT][3], sm[NQ_PPT][3];
+    if (consecutive) {
+#pragma unroll
+        for (int m = 0; m < NQ_PPT; ++m)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                T st, ct;
+                const double t = xl[m][d] - floor(xl[m][d]);
+                sincospi_t<T>(2.0 * t, &st, &ct);
+                c1[m][d] = ct;
+                s1[m][d] = -st;
+                cm[m][d] = (T)1;
+                sm[m][d] = (T)0;
+            }
     }
     for (int iq = 0; iq < nq; ++iq) {
-        const double m = qmult[iq];
+        const double mq = qmult[iq];
+        double acc[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            double c = 0.0, sn = 0.0;
-            if (have) {
-                double t = m * xl[d];
-                t = t - floor(t);
-                T st, ct;
-                if (sizeof(T) == 4) {
-                    float sf, cf;
-                    sincospif((float)(2.0 * t), &sf, &cf);
-                    st = (T)sf;
-                    ct = (T)cf;
+        for (int m = 0; m < NQ_PPT; ++m) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                T c, sn;
+                if (consecutive) {
+                    // exp(-i (k+1) theta) = exp(-i k theta) exp(-i theta)
+                    const T nc = cm[m][d] * c1[m][d] - sm[m][d] * s1[m][d];
+                    const T ns = cm[m][d] * s1[m][d] + sm[m][d] * c1[m][d];
+                    cm[m][d] = nc;
+                    sm[m][d] = ns;
+                    c = nc;
+                    sn = ns;
                 } else {
-                    double sd, cd;
-                    sincospi(2.0 * t, &sd, &cd);
-                    st = (T)sd;
-                    ct = (T)cd;
+                    double t = mq * xl[m][d];
+                    t = t - floor(t);
+                    T st, ct;
+                    sincospi_t<T>(2.0 * t, &st, &ct);
+                    c = ct;
+                    sn = -st;
                 }
-                c = (double)ct;
-                sn = -(double)st;
+                if (have[m]) {
+                    acc[2 * d + 0] += (double)c;
+                    acc[2 * d + 1] += (double)sn;
+                }
             }
-            c = warp_sum(c);
-            sn = warp_sum(sn);
-            if (lane == 0) {
-                nsm[w * nq * 6 + iq * 6 + 2 * d + 0] = c;
-                nsm[w * nq * 6 + iq * 6 + 2 * d + 1] = sn;
-            }
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const double v = warp_sum(acc[k]);
+            if (lane == 0) nsm[w * nq * 6 + iq * 6 + k] = v;
         }
     }
     __syncthreads();
     for (int k = threadIdx.x; k < nq * 6; k += blockDim.x) {
-        double s = 0.0;
-        for (int ww = 0; ww < nw; ++ww) s += nsm[ww * nq * 6 + k];
-        part[(long long)b * nq * 6 + k] = s;
+        double t = 0.0;
+        for (int ww = 0; ww < nw; ++ww) t += nsm[ww * nq * 6 + k];
+        part[(long long)b * nq * 6 + k] = t;
     }
 }
 
@@ -291,7 +353,7 @@ __global__ void k_nqt_reduce(const RepDev *__restrict__ reps, int nrep, int nblk
 {
     const int r = blockIdx.x;
     const RepDev &R = reps[r];
-    const int b0 = R.blk_off, b1 = (r + 1 < nrep) ? reps[r + 1].blk_off : nblk;
+    const int b0 = R.nq_blk_off, b1 = (r + 1 < nrep) ? reps[r + 1].nq_blk_off : nblk;
     double *o = out;
     if (counters) {
         // ring layout [step][replica][nq][3][2]; the step was already advanced
@@ -373,9 +435,14 @@ static int pgrid(int n) { int g = (n + 255) / 256; return g < 1 ? 1 : (g > 148 *
 
 void launch_kick_drift(const DevState &s, cudaStream_t st)
 {
-    k_kick_drift<<<pgrid(s.ntot), 256, 0, st>>>(s.reps, s.prep, s.pos, s.vel, s.acc, s.ntot,
-                                                s.cell_key, s.cell_count, s.brick_key,
-                                                s.brick_count, s.has_mesh, s.status);
+    k_kick_drift<<<pgrid(s.ntot), 256, 0, st>>>(s.reps, s.prep, s.pos, s.vel, s.acc, s.pos_ref,
+                                                s.ntot, s.brick_key, s.brick_count, s.has_mesh,
+                                                s.rebuild, s.status);
+}
+
+void launch_set_flags(int *flag, int n, int value, cudaStream_t st)
+{
+    k_set_flags<<<1, 256, 0, st>>>(flag, n, value);
 }
 
 template <typename T>
@@ -392,7 +459,7 @@ void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring
                         cudaStream_t st)
 {
     k_step_reduce<<<1, 1024, 0, st>>>(s.reps, s.nrep, s.nblk, s.kin_part, s.rep_out, mode,
-                                      counters, ring, ring_cap, s.status);
+                                      counters, ring, ring_cap, s.rebuild, s.status);
 }
 
 void launch_set_counters(int *counters, int run_step, int ring_pos, int it0, cudaStream_t st)
@@ -416,14 +483,17 @@ void launch_scale_vel(const DevState &s, cudaStream_t st)
 }
 
 template <typename T>
-void launch_nqt(const DevState &s, const double *pos, const double *qmult, int nq, double *part,
-                double *out, const int *counters, int ring_cap, cudaStream_t st)
+void launch_nqt(const DevState &s, const double *pos, const double *qmult, int nq, int consecutive,
+                double *part, double *out, const int *counters, int ring_cap, cudaStream_t st)
 {
     const size_t smem = (size_t)(PBLK / 32) * nq * 6 * sizeof(double);
-    k_nqt_partial<T><<<s.nblk, PBLK, smem, st>>>(s.reps, s.nrep, pos, qmult, nq, part);
-    k_nqt_reduce<<<s.nrep, 256, 0, st>>>(s.reps, s.nrep, s.nblk, part, nq, out, counters,
+    k_nqt_partial<T><<<s.nq_nblk, PBLK, smem, st>>>(s.reps, s.nrep, pos, qmult, nq, consecutive,
+                                                    part);
+    k_nqt_reduce<<<s.nrep, 256, 0, st>>>(s.reps, s.nrep, s.nq_nblk, part, nq, out, counters,
                                          ring_cap);
 }
+
+int nqt_particles_per_block() { return PBLK * NQ_PPT; }
 
 template <typename T> void configure_integrate_kernels(int max_nq)
 {
@@ -443,8 +513,8 @@ int gf_opt_blocks(int M) { return (int)(((long long)M * M * M + 255) / 256); }
 
 #define P3M_INST(T)                                                                             \
     template void launch_kick_finish<T>(const DevState &, int, double *, cudaStream_t);          \
-    template void launch_nqt<T>(const DevState &, const double *, const double *, int, double *, \
-                                double *, const int *, int, cudaStream_t);                     \
+    template void launch_nqt<T>(const DevState &, const double *, const double *, int, int,      \
+                                double *, double *, const int *, int, cudaStream_t);            \
     template void configure_integrate_kernels<T>(int);                                          \
     template void launch_combine<T>(const DevState &, int, int, int, double *, double *,         \
                                     cudaStream_t);

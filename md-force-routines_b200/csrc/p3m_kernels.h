@@ -15,11 +15,15 @@ struct DevState {
     int nrep = 0, ntot = 0, ncell = 0, nbrick = 0;
     long long nmesh = 0, nspec = 0, ntile = 0;
     int wa = 0, wb = 0, wc = 0;  // total work items of the mesh passes
-    int pp_split = 1;            // CTAs per PP cell (autotuned)
-    int pp_tpi = 1;              // threads per i-particle in the PP loop
+    int wp = 0;                  // plane items (fused y/z passes)
+    int max_plane = 0;           // largest M among plane replicas
+    int pp_tpi = 1;              // threads per particle in the PP force kernel
+    int pp_nblk = 0;             // blocks of the PP force kernel (replica-aligned)
+    int maxnb = 0;               // list capacity per particle
     int has_mesh = 0;
     int max_mesh = 0;            // largest M over replicas
     int nblk = 0;                // replica-aligned particle blocks (PBLK each)
+    int nq_nblk = 0;             // replica-aligned blocks of the n(q,t) kernel
     RepDev *reps = nullptr;      // [nrep]
     // particle state, FP64 (ntot,3) row-major in original order
     double *pos = nullptr, *vel = nullptr, *acc = nullptr, *charge = nullptr;
@@ -27,13 +31,18 @@ struct DevState {
     // cell sort
     int *cell_key = nullptr, *cell_count = nullptr, *cell_start = nullptr;
     int *cell_cursor = nullptr, *cell_tmp = nullptr, *cell_perm = nullptr, *cell_slot = nullptr;
-    void *xs_cell = nullptr;     // double4 sorted positions relative to the cell origin
+    void *xq = nullptr;          // integer coordinates in sorted order (uint4 / ulonglong4)
+    int *nnb = nullptr;          // list length per sorted particle
+    int *nlist = nullptr;        // neighbour lists (sorted indices), warp-interleaved
+    int *rebuild = nullptr;      // per-replica flags: rebuild cells and lists this step
+    double *pos_ref = nullptr;   // positions at the last rebuild (ntot,3)
+    float4 *pp_tables = nullptr; // FP32 pair-function tables [nrep][2 PP_TABLE_N]
     void *acc_pp = nullptr;      // V4<T> PP acceleration, cell-sorted order
     // brick sort
     int *brick_key = nullptr, *brick_count = nullptr, *brick_start = nullptr;
     int *brick_cursor = nullptr, *brick_perm = nullptr, *brick_slot = nullptr;
     // mesh
-    unsigned long long *tiles = nullptr;  // fixed-point assignment tiles (int64)
+    void *tiles = nullptr;       // T assignment tiles [brick][TILE^3]
     void *spec = nullptr;        // C2<T> half spectrum rho_k / phi_k, [kx][z][y]
     void *ek = nullptr;          // C2<T> 3 field spectra, [3][kx][z][y]
     void *green = nullptr;       // T influence function / V, [kx][z][y]
@@ -41,14 +50,15 @@ struct DevState {
     void *acc_pm = nullptr;      // V4<T> PM acceleration, brick-sorted order
     void *twiddle = nullptr;     // C2<T> exp(-2 pi i k / 256), k < 128
     // reductions
-    double *u_pp_part = nullptr;  // [ncell * pp_split]
-    double *u_pm_part = nullptr;  // [wc]
+    double *u_pp_part = nullptr;  // [pp_nblk]
+    double *u_pm_part = nullptr;  // [wc + wp]
     double *kin_part = nullptr;   // per particle block
     double *rep_out = nullptr;    // [nrep * 8] per-replica scalars of the last step
     int *status = nullptr;
 };
 
-enum RepOut { RO_UPP = 0, RO_UPM = 1, RO_USELF = 2, RO_U = 3, RO_K = 4, RO_T = 5, RO_FACT = 6 };
+enum RepOut { RO_UPP = 0, RO_UPM = 1, RO_USELF = 2, RO_U = 3, RO_K = 4, RO_T = 5, RO_FACT = 6,
+              RO_REBUILDS = 7 };
 
 // fixed-point scale of the deterministic charge assignment
 constexpr double ASSIGN_SCALE = 1099511627776.0;  // 2^40
@@ -56,10 +66,14 @@ constexpr double ASSIGN_SCALE = 1099511627776.0;  // 2^40
 template <typename T> void configure_pp_kernels();
 template <typename T> void configure_mesh_kernels();
 template <typename T> void launch_keys(const DevState &s, cudaStream_t st);
+void launch_cell_keys(const DevState &s, cudaStream_t st);
 void launch_scan(const DevState &s, cudaStream_t st);
 void launch_scatter(const DevState &s, cudaStream_t st);
 template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st);
+template <typename T> void launch_quantize(const DevState &s, cudaStream_t st);
+template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st);
 template <typename T> void launch_pp(const DevState &s, cudaStream_t st);
+int pp_particles_per_block(int tpi);
 void launch_reduce_pp(const DevState &s, cudaStream_t st);
 
 template <typename T> void launch_assign(const DevState &s, cudaStream_t st);
@@ -67,6 +81,8 @@ template <typename T> void launch_fft_forward(const DevState &s, cudaStream_t st
 template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st);
 template <typename T> void launch_gather(const DevState &s, cudaStream_t st);
 void launch_reduce_pm(const DevState &s, cudaStream_t st);
+int fft_kernel_count(const DevState &s);
+int plane_max_mesh();
 
 template <typename T> void launch_green_from_host_layout(const DevState &s, int rep,
                                                          const double *gk_dev,
@@ -85,12 +101,14 @@ template <typename T> void launch_kick_finish(const DevState &s, int do_kick, do
 void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring, int ring_cap,
                         cudaStream_t st);
 void launch_set_counters(int *counters, int run_step, int ring_pos, int it0, cudaStream_t st);
+void launch_set_flags(int *flag, int n, int value, cudaStream_t st);
 void launch_scale_vel(const DevState &s, cudaStream_t st);
 template <typename T> void launch_combine(const DevState &s, int use_pp, int use_pm, int scale_af,
                                           double *out, double *ep_out, cudaStream_t st);
 template <typename T> void launch_nqt(const DevState &s, const double *pos, const double *qmult,
-                                      int nq, double *part, double *out, const int *counters,
-                                      int ring_cap, cudaStream_t st);
+                                      int nq, int consecutive, double *part, double *out,
+                                      const int *counters, int ring_cap, cudaStream_t st);
+int nqt_particles_per_block();
 template <typename T> void configure_integrate_kernels(int max_nq);
 int gf_opt_blocks(int M);
 double fp32_fma_tflops(int device);

@@ -112,7 +112,7 @@ template <typename T>
 __global__ void __launch_bounds__(256)
 k_assign(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_start,
          const int *__restrict__ brick_perm, const double *__restrict__ pos,
-         const double *__restrict__ charge, unsigned long long *__restrict__ tiles, int nbrick)
+         const double *__restrict__ charge, T *__restrict__ tiles, int nbrick)
 {
     extern __shared__ __align__(16) unsigned long long tile[];
     for (int b = blockIdx.x; b < nbrick; b += gridDim.x) {
@@ -157,34 +157,34 @@ k_assign(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
             }
         }
         __syncthreads();
-        unsigned long long *dst = tiles + R.tile_off + (long long)local * TILE3;
-        for (int k = threadIdx.x; k < TILE3; k += blockDim.x) dst[k] = tile[k];
+        // the tile's exact integer sums, rounded once to T
+        T *dst = tiles + R.tile_off + (long long)local * TILE3;
+        for (int k = threadIdx.x; k < TILE3; k += blockDim.x)
+            dst[k] = (T)((double)(long long)tile[k] * (1.0 / ASSIGN_SCALE));
     }
 }
 
-// Charge on node (x,y,z) of replica R: the integer sum of the (up to 8)
-// brick tiles that cover it, converted from fixed point.
-__device__ __forceinline__ long long rho_fixed(const RepDev &R,
-                                               const unsigned long long *__restrict__ tiles,
-                                               int x, int y, int z)
+// Charge on node (x,y,z) of replica R: the sum of the (up to 8) brick tiles
+// that cover it, in a fixed order (dz, dy, dx), with all loads independent.
+template <typename T>
+__device__ __forceinline__ T rho_at(const RepDev &R, const T *__restrict__ tiles, int x, int y, int z)
 {
     const int nb = R.nb;
     const int bx = x / BRICK, by = y / BRICK, bz = z / BRICK;
     const int ox = x - bx * BRICK, oy = y - by * BRICK, oz = z - bz * BRICK;
-    unsigned long long s = 0;
-    const int ndx = ox < HALO ? 2 : 1, ndy = oy < HALO ? 2 : 1, ndz = oz < HALO ? 2 : 1;
-    for (int dz = 0; dz < ndz; ++dz) {
-        const int tz = oz + dz * BRICK, cz = (bz - dz + nb) % nb;
-        for (int dy = 0; dy < ndy; ++dy) {
-            const int ty = oy + dy * BRICK, cy = (by - dy + nb) % nb;
-            for (int dx = 0; dx < ndx; ++dx) {
-                const int tx = ox + dx * BRICK, cx = (bx - dx + nb) % nb;
-                const long long brick = cx + nb * (cy + (long long)nb * cz);
-                s += tiles[R.tile_off + brick * TILE3 + (tz * TILE + ty) * TILE + tx];
-            }
-        }
+    const bool hx = ox < HALO, hy = oy < HALO, hz = oz < HALO;
+    const int cx[2] = {bx, (bx - 1 + nb) % nb}, cy[2] = {by, (by - 1 + nb) % nb},
+              cz[2] = {bz, (bz - 1 + nb) % nb};
+    T v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+        const bool use = (!dx || hx) && (!dy || hy) && (!dz || hz);
+        const long long brick = cx[dx] + nb * (cy[dy] + (long long)nb * cz[dz]);
+        const int t = ((oz + dz * BRICK) * TILE + (oy + dy * BRICK)) * TILE + ox + dx * BRICK;
+        v[k] = use ? __ldg(tiles + R.tile_off + brick * TILE3 + t) : (T)0;
     }
-    return (long long)s;
+    return ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
 }
 
 // ---------------------------------------------------------------------------
@@ -196,7 +196,7 @@ __device__ __forceinline__ long long rho_fixed(const RepDev &R,
 // two real rows share one complex line.
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS)
-k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const unsigned long long *__restrict__ tiles,
+k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const T *__restrict__ tiles,
             cplx<T> *__restrict__ spec, const cplx<T> *__restrict__ twg, int nitems)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -212,8 +212,7 @@ k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const unsigned long long 
         __syncthreads();
         for (int e = threadIdx.x; e < 2 * PENCIL * M; e += blockDim.x) {
             const int x = e % M, j = e / M;
-            const long long f = rho_fixed(R, tiles, x, y0 + j, z);
-            const T v = (T)((double)f * (1.0 / ASSIGN_SCALE));
+            const T v = rho_at<T>(R, tiles, x, y0 + j, z);
             T *dst = reinterpret_cast<T *>(&buf[brev(x, logM) * LS + (j >> 1)]);
             dst[j & 1] = v;
         }
@@ -343,6 +342,119 @@ k_fft_z_green(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restri
     }
 }
 
+// Passes B-D fused for meshes whose kx planes fit in shared memory
+// (M <= PLANE_MAX): one CTA per (replica, kx) loads the plane rho_k(kx,z,y),
+// transforms it along y and z, forms the U_f partial and phi = (G/V) rho_k,
+// and transforms back: E_z = IFFT_y IFFT_z(-i kz phi), E_y = IFFT_y(-i ky
+// IFFT_z(phi)), E_x = -i kx IFFT_y IFFT_z(phi) -- seven line-FFT sweeps in
+// shared memory, one plane read and three plane writes. The plane is stored
+// [z][y] with a padded row (M+1); radix-2 DIT needs bit-reversed input, so the
+// load and the multiplies write bit-reversed positions.
+constexpr int PLANE_MAX = 64;
+
+template <typename T>
+__device__ void fft_plane_lines(cplx<T> *buf, int logM, int ls, int es, const cplx<T> *tw,
+                                bool inverse)
+{
+    const int M = 1 << logM;
+    const int nb = M * (M >> 1);
+    for (int s = 0; s < logM; ++s) {
+        const int half = 1 << s;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            const int l = b & (M - 1), j = b >> logM;
+            const int k = j & (half - 1);
+            const int i0 = ((j >> s) << (s + 1)) + k, i1 = i0 + half;
+            cplx<T> w = tw[k << (7 - s)];
+            if (inverse) w.y = -w.y;
+            cplx<T> *p0 = buf + l * ls + i0 * es, *p1 = buf + l * ls + i1 * es;
+            const cplx<T> a = *p0, c = *p1;
+            const cplx<T> t = cmul<T>(w, c);
+            *p0 = make_c<T>(a.x + t.x, a.y + t.y);
+            *p1 = make_c<T>(a.x - t.x, a.y - t.y);
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS)
+k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict__ spec,
+            const T *__restrict__ green, cplx<T> *__restrict__ ek, long long nspec,
+            double *__restrict__ u_part, const cplx<T> *__restrict__ twg, int nitems)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *tw = reinterpret_cast<cplx<T> *>(smem_raw);
+    __shared__ double red[32];
+    load_twiddles<T>(tw, twg);
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int r = find_rep(item, nrep, [&](int k) { return reps[k].wp_off; });
+        const RepDev &R = reps[r];
+        const int M = R.M, logM = R.logM, kx = item - R.wp_off;
+        const int LD = M + 1;
+        cplx<T> *A = tw + 128;
+        cplx<T> *B = A + M * LD;
+        const long long lbase = R.spec_off + (long long)kx * M * M;
+        const int MM = M * M;
+        __syncthreads();
+        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
+            const int z = e >> logM, y = e & (M - 1);
+            A[brev(z, logM) * LD + brev(y, logM)] = spec[lbase + e];
+        }
+        __syncthreads();
+        fft_plane_lines<T>(A, logM, LD, 1, tw, false);  // along y
+        fft_plane_lines<T>(A, logM, 1, LD, tw, false);  // along z
+        const double wkx = (kx == 0 || kx == (M >> 1)) ? 1.0 : 2.0;
+        double u = 0.0;
+        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
+            const int z = e >> logM, y = e & (M - 1);
+            const cplx<T> rk = A[z * LD + y];
+            const T g = green[lbase + e];
+            u += wkx * (double)g * ((double)rk.x * rk.x + (double)rk.y * rk.y);
+            B[brev(z, logM) * LD + brev(y, logM)] = make_c<T>(g * rk.x, g * rk.y);
+        }
+        __syncthreads();
+        const T twopi_L = (T)(6.283185307179586477 * R.inv_L);
+        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
+            const int zb = e >> logM, yb = e & (M - 1);
+            const int z = brev(zb, logM);
+            const T kz = (z == (M >> 1)) ? (T)0 : twopi_L * (T)freq(z, M);
+            const cplx<T> ph = B[zb * LD + yb];
+            A[zb * LD + yb] = make_c<T>(kz * ph.y, -kz * ph.x);  // -i kz phi
+        }
+        __syncthreads();
+        fft_plane_lines<T>(A, logM, 1, LD, tw, true);  // z, of -i kz phi
+        fft_plane_lines<T>(B, logM, 1, LD, tw, true);  // z, of phi: psi
+        fft_plane_lines<T>(A, logM, LD, 1, tw, true);  // y: E_z
+        cplx<T> *Ez = ek + 2 * nspec + lbase;
+        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
+            const int z = e >> logM, y = e & (M - 1);
+            Ez[e] = A[z * LD + y];
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
+            const int z = e >> logM, yb = e & (M - 1);
+            const int y = brev(yb, logM);
+            const T ky = (y == (M >> 1)) ? (T)0 : twopi_L * (T)freq(y, M);
+            const cplx<T> ps = B[z * LD + yb];
+            A[z * LD + yb] = make_c<T>(ky * ps.y, -ky * ps.x);  // -i ky psi
+        }
+        __syncthreads();
+        fft_plane_lines<T>(A, logM, LD, 1, tw, true);  // y: E_y
+        fft_plane_lines<T>(B, logM, LD, 1, tw, true);  // y: IFFT(psi)
+        const T kxv = (kx == (M >> 1)) ? (T)0 : twopi_L * (T)kx;
+        cplx<T> *Ey = ek + nspec + lbase;
+        cplx<T> *Ex = ek + lbase;
+        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
+            const int z = e >> logM, y = e & (M - 1);
+            Ey[e] = A[z * LD + y];
+            const cplx<T> ps = B[z * LD + y];
+            Ex[e] = make_c<T>(kxv * ps.y, -kxv * ps.x);
+        }
+        const double ut = block_sum(u, red);
+        if (threadIdx.x == 0) u_part[item] = ut;
+    }
+}
+
 // Pass E: C2R along x of the three field spectra, written as real meshes
 // efield[c][z][y][x]. Item = (replica, component, z, 32-row tile); rows
 // 2l and 2l+1 share complex line l: Z[k] = Xa[k] + i Xb[k] over the
@@ -393,65 +505,97 @@ k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
 // Gather
 // ---------------------------------------------------------------------------
 
-// Field at each particle (brick-sorted order): E = sum over the 216 stencil
-// nodes of E[node] wz wy wx (yukawa_pm_ord6.py:298-300). Written as
-// (Ex, Ey, Ez, Z) so the caller forms acc = Z E (:308-310).
+// Field at each particle (yukawa_pm_ord6.py:298-300): E = sum over the 216
+// stencil nodes of E[node] wz wy wx, written as (Ex, Ey, Ez, Z) in
+// brick-sorted order so the caller forms acc = Z E (:308-310). One CTA per
+// brick: each field component's TILE^3 neighbourhood of the brick is staged
+// in shared memory (coalesced rows), and every particle of the brick reads
+// its 216 nodes from there; each thread keeps the weights of up to GPT
+// particles across the three components.
+constexpr int G_THREADS = 256;
+
 template <typename T>
-__global__ void __launch_bounds__(128)
-k_gather(const RepDev *__restrict__ reps, const int *__restrict__ prep,
+__global__ void __launch_bounds__(G_THREADS)
+k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_start,
          const int *__restrict__ brick_perm, const double *__restrict__ pos,
          const double *__restrict__ charge, const T *__restrict__ efield, long long nmesh,
-         typename V4<T>::t *__restrict__ acc_pm, int ntot)
+         typename V4<T>::t *__restrict__ acc_pm, int nbrick)
 {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ntot; p += gridDim.x * blockDim.x) {
-        const int i = brick_perm[p];
-        const RepDev &R = reps[prep[i]];
-        if (R.M == 0) continue;
-        const int M = R.M;
-        double ox, oy, oz;
-        const int ix = base_offset(pos[3 * i + 0], R.h, ox);
-        const int iy = base_offset(pos[3 * i + 1], R.h, oy);
-        const int iz = base_offset(pos[3 * i + 2], R.h, oz);
-        T wx[6], wy[6], wz[6];
-        weights6<T>((T)ox, wx);
-        weights6<T>((T)oy, wy);
-        weights6<T>((T)oz, wz);
-        int xs[6];
-#pragma unroll
-        for (int c = 0; c < 6; ++c) xs[c] = wrapM(ix + c, M);
-        const T *Ex = efield + R.mesh_off;
-        const T *Ey = Ex + nmesh;
-        const T *Ez = Ey + nmesh;
-        T ex = 0, ey = 0, ez = 0;
-#pragma unroll 1
-        for (int g = 0; g < 6; ++g) {
-            const long long zo = (long long)wrapM(iz + g, M) * M;
-#pragma unroll
-            for (int a = 0; a < 6; ++a) {
-                const long long ro = (zo + wrapM(iy + a, M)) * M;
-                const T wzy = wz[g] * wy[a];
-#pragma unroll
-                for (int c = 0; c < 6; ++c) {
-                    const long long o = ro + xs[c];
-                    const T wgt = wzy * wx[c];
-                    ex += __ldg(Ex + o) * wgt;
-                    ey += __ldg(Ey + o) * wgt;
-                    ez += __ldg(Ez + o) * wgt;
+    extern __shared__ __align__(16) unsigned char g_smem[];
+    T *tile = reinterpret_cast<T *>(g_smem);
+    for (int b = blockIdx.x; b < nbrick; b += gridDim.x) {
+        const int r = find_rep(b, nrep, [&](int k) { return reps[k].brick_off; });
+        const RepDev &R = reps[r];
+        const int nb = R.nb, M = R.M, local = b - R.brick_off;
+        const int bx = (local % nb) * BRICK, by = ((local / nb) % nb) * BRICK,
+                  bz = (local / (nb * nb)) * BRICK;
+        const int p0 = brick_start[b], p1 = brick_start[b + 1];
+        for (int c0 = p0; c0 < p1; c0 += G_THREADS) {
+            T wx[6], wy[6], wz[6];
+            int base = -1;  // local tile offset of the stencil's first node, or -1
+            T e[3] = {(T)0, (T)0, (T)0};
+            const int p = c0 + threadIdx.x;
+            if (p < p1) {
+                const int i = brick_perm[p];
+                double ox, oy, oz;
+                const int ix = base_offset(pos[3 * i + 0], R.h, ox);
+                const int iy = base_offset(pos[3 * i + 1], R.h, oy);
+                const int iz = base_offset(pos[3 * i + 2], R.h, oz);
+                const int lx = wrapM(ix, M) - bx, ly = wrapM(iy, M) - by, lz = wrapM(iz, M) - bz;
+                // (a particle outside [-L, 2L) was flagged by the key pass)
+                if ((unsigned)lx < (unsigned)BRICK && (unsigned)ly < (unsigned)BRICK &&
+                    (unsigned)lz < (unsigned)BRICK) {
+                    base = (lz * TILE + ly) * TILE + lx;
+                    weights6<T>((T)ox, wx);
+                    weights6<T>((T)oy, wy);
+                    weights6<T>((T)oz, wz);
                 }
             }
+            for (int comp = 0; comp < 3; ++comp) {
+                const T *E = efield + comp * nmesh + R.mesh_off;
+                __syncthreads();
+                for (int k = threadIdx.x; k < TILE3; k += G_THREADS) {
+                    const int tx = k % TILE, ty = (k / TILE) % TILE, tz = k / (TILE * TILE);
+                    const int gx = (bx + tx) & (M - 1), gy = (by + ty) & (M - 1),
+                              gz = (bz + tz) & (M - 1);
+                    cp_async<sizeof(T)>(tile + k, E + ((long long)gz * M + gy) * M + gx);
+                }
+                cp_async_wait_all();
+                __syncthreads();
+                if (base >= 0) {
+                    // separable contraction: sum_g wz sum_a wy sum_c wx E
+                    T acc = 0;
+#pragma unroll
+                    for (int g = 0; g < 6; ++g) {
+                        T sg = 0;
+#pragma unroll
+                        for (int a = 0; a < 6; ++a) {
+                            const T *row = tile + base + (g * TILE + a) * TILE;
+                            T sa = 0;
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) sa += wx[c] * row[c];
+                            sg += wy[a] * sa;
+                        }
+                        acc += wz[g] * sg;
+                    }
+                    e[comp] = acc;
+                }
+            }
+            if (p < p1) {
+                typename V4<T>::t out;
+                out.x = e[0];
+                out.y = e[1];
+                out.z = e[2];
+                out.w = (T)charge[brick_perm[p]];
+                acc_pm[p] = out;
+            }
         }
-        typename V4<T>::t out;
-        out.x = ex;
-        out.y = ey;
-        out.z = ez;
-        out.w = (T)charge[i];
-        acc_pm[p] = out;
     }
 }
 
 // Per-replica U_f = 1/2 sum over the replica's pass-C partials.
 __global__ void k_reduce_pm(const RepDev *__restrict__ reps, int nrep,
-                            const double *__restrict__ u_part, int wc_total,
+                            const double *__restrict__ u_part, int wc_total, int wp_total,
                             double *__restrict__ rep_out)
 {
     const int lane = threadIdx.x & 31;
@@ -461,9 +605,13 @@ __global__ void k_reduce_pm(const RepDev *__restrict__ reps, int nrep,
             if (lane == 0) rep_out[8 * r + RO_UPM] = 0.0;
             continue;
         }
+        // multi-pass items [wc_off, ...) and plane items (stored after wc_total)
         const int b = reps[r].wc_off, e = (r + 1 < nrep) ? reps[r + 1].wc_off : wc_total;
+        const int pb = wc_total + reps[r].wp_off,
+                  pe = wc_total + ((r + 1 < nrep) ? reps[r + 1].wp_off : wp_total);
         double t = 0.0;
         for (int k = b + lane; k < e; k += 32) t += u_part[k];
+        for (int k = pb + lane; k < pe; k += 32) t += u_part[k];
         t = warp_sum(t);
         if (lane == 0) rep_out[8 * r + RO_UPM] = 0.5 * t;
     }
@@ -492,8 +640,7 @@ __global__ void k_green_from_shifted(const RepDev *__restrict__ reps, int rep,
 
 template <typename T>
 __global__ void k_tiles_to_mesh(const RepDev *__restrict__ reps, int rep,
-                                const unsigned long long *__restrict__ tiles,
-                                double *__restrict__ rho)
+                                const T *__restrict__ tiles, double *__restrict__ rho)
 {
     const RepDev &R = reps[rep];
     const int M = R.M;
@@ -501,8 +648,7 @@ __global__ void k_tiles_to_mesh(const RepDev *__restrict__ reps, int rep,
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
          e += (long long)gridDim.x * blockDim.x) {
         const int x = (int)(e % M), y = (int)((e / M) % M), z = (int)(e / ((long long)M * M));
-        const long long f = rho_fixed(R, tiles, x, y, z);
-        rho[e] = (double)f * (1.0 / ASSIGN_SCALE);
+        rho[e] = (double)rho_at<T>(R, tiles, x, y, z);
     }
 }
 
@@ -531,6 +677,11 @@ template <typename T> static size_t fft_smem(int maxM, int nbuf)
     return (128 + (size_t)nbuf * maxM * LS) * sizeof(cplx<T>);
 }
 
+template <typename T> static size_t plane_smem(int M)
+{
+    return (128 + 2 * (size_t)M * (M + 1)) * sizeof(cplx<T>);
+}
+
 template <typename K> static void set_smem(K kernel, size_t bytes)
 {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -545,13 +696,15 @@ template <typename T> void configure_mesh_kernels()
     set_smem(k_fft_y<T>, fft_smem<T>(256, 1));
     set_smem(k_fft_z_green<T>, fft_smem<T>(256, 2));
     set_smem(k_fft_x_c2r<T>, fft_smem<T>(256, 1));
+    set_smem(k_gather<T>, TILE3 * sizeof(T));
+    set_smem(k_fft_plane<T>, plane_smem<T>(PLANE_MAX));
 }
 
 template <typename T> void launch_assign(const DevState &s, cudaStream_t st)
 {
     const size_t smem = TILE3 * sizeof(unsigned long long);
     k_assign<T><<<grid_items(s.nbrick, 148 * 16), 256, smem, st>>>(
-        s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, s.tiles, s.nbrick);
+        s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (T *)s.tiles, s.nbrick);
 }
 
 template <typename T> void launch_fft_forward(const DevState &s, cudaStream_t st)
@@ -559,21 +712,32 @@ template <typename T> void launch_fft_forward(const DevState &s, cudaStream_t st
     using C = cplx<T>;
     const int maxM = s.max_mesh;
     const size_t sm1 = fft_smem<T>(maxM, 1), sm2 = fft_smem<T>(maxM, 2);
-    k_fft_x_r2c<T><<<grid_items(s.wa), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, s.tiles, (C *)s.spec,
-                                                                (const C *)s.twiddle, s.wa);
-    k_fft_y<T><<<grid_items(s.wb), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, (C *)s.spec, s.nspec, 1,
-                                                            (const C *)s.twiddle, s.wb, false);
-    k_fft_z_green<T><<<grid_items(s.wc), FFT_THREADS, sm2, st>>>(
-        s.reps, s.nrep, (const C *)s.spec, (const T *)s.green, (C *)s.ek, s.nspec, s.u_pm_part,
-        (const C *)s.twiddle, s.wc);
+    k_fft_x_r2c<T><<<grid_items(s.wa), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, (const T *)s.tiles,
+                                                                (C *)s.spec, (const C *)s.twiddle, s.wa);
+    if (s.wb > 0) {
+        k_fft_y<T><<<grid_items(s.wb), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, (C *)s.spec, s.nspec,
+                                                                1, (const C *)s.twiddle, s.wb, false);
+        k_fft_z_green<T><<<grid_items(s.wc), FFT_THREADS, sm2, st>>>(
+            s.reps, s.nrep, (const C *)s.spec, (const T *)s.green, (C *)s.ek, s.nspec, s.u_pm_part,
+            (const C *)s.twiddle, s.wc);
+    }
+    if (s.wp > 0) {
+        k_fft_plane<T><<<grid_items(s.wp), FFT_THREADS, plane_smem<T>(s.max_plane), st>>>(
+            s.reps, s.nrep, (const C *)s.spec, (const T *)s.green, (C *)s.ek, s.nspec,
+            s.u_pm_part + s.wc, (const C *)s.twiddle, s.wp);
+    }
 }
+
+int fft_kernel_count(const DevState &s) { return 2 + (s.wb > 0 ? 3 : 0) + (s.wp > 0 ? 1 : 0); }
+int plane_max_mesh() { return PLANE_MAX; }
 
 template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st)
 {
     using C = cplx<T>;
     const size_t sm1 = fft_smem<T>(s.max_mesh, 1);
-    k_fft_y<T><<<grid_items(3 * s.wb), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, (C *)s.ek, s.nspec, 3,
-                                                                (const C *)s.twiddle, s.wb, true);
+    if (s.wb > 0)
+        k_fft_y<T><<<grid_items(3 * s.wb), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, (C *)s.ek, s.nspec,
+                                                                    3, (const C *)s.twiddle, s.wb, true);
     k_fft_x_c2r<T><<<grid_items(3 * s.wa), FFT_THREADS, sm1, st>>>(
         s.reps, s.nrep, (const C *)s.ek, s.nspec, (T *)s.efield, s.nmesh, (const C *)s.twiddle,
         s.wa);
@@ -581,14 +745,15 @@ template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st
 
 template <typename T> void launch_gather(const DevState &s, cudaStream_t st)
 {
-    k_gather<T><<<grid_items((s.ntot + 127) / 128, 148 * 16), 128, 0, st>>>(
-        s.reps, s.prep, s.brick_perm, s.pos, s.charge, (const T *)s.efield, s.nmesh,
-        (typename V4<T>::t *)s.acc_pm, s.ntot);
+    k_gather<T><<<grid_items(s.nbrick, 148 * 16), G_THREADS, TILE3 * sizeof(T), st>>>(
+        s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (const T *)s.efield,
+        s.nmesh, (typename V4<T>::t *)s.acc_pm, s.nbrick);
 }
 
 void launch_reduce_pm(const DevState &s, cudaStream_t st)
 {
-    k_reduce_pm<<<(s.nrep + 3) / 4, 128, 0, st>>>(s.reps, s.nrep, s.u_pm_part, s.wc, s.rep_out);
+    k_reduce_pm<<<(s.nrep + 3) / 4, 128, 0, st>>>(s.reps, s.nrep, s.u_pm_part, s.wc, s.wp,
+                                                  s.rep_out);
 }
 
 template <typename T>
@@ -599,7 +764,7 @@ void launch_green_from_host_layout(const DevState &s, int rep, const double *gk_
 
 template <typename T> void launch_tiles_to_mesh(const DevState &s, int rep, double *rho, cudaStream_t st)
 {
-    k_tiles_to_mesh<T><<<592, 256, 0, st>>>(s.reps, rep, s.tiles, rho);
+    k_tiles_to_mesh<T><<<592, 256, 0, st>>>(s.reps, rep, (const T *)s.tiles, rho);
 }
 
 template <typename T>

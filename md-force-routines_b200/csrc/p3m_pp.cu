@@ -1,128 +1,134 @@
-// Short-range (PP) Yukawa-Ewald forces over linked cells.
+// Short-range (PP) Yukawa-Ewald forces over Verlet neighbour lists.
 //
 // Computes what yukawa_pp.py:6-139 computes: for every pair closer than r_c
-// (minimum image through the 27-cell periodic stencil, :54-94)
+// (minimum image; the reference finds them through a 27-cell periodic
+// stencil, :54-94)
 //   phi(r) = (1/2r) [e^{kr} erfc(ar + k/2a) + e^{-kr} erfc(ar - k/2a)]   (:115)
 //   F(r)   = f1 + f2 + f3                                               (:121-124)
-// The energy is sum_{i<j} phi. The reference visits each pair once and
-// applies Newton's third law; here every particle sums over all of its
-// neighbours itself (full list), so each thread owns its particle's force and
-// no atomics are needed. Z is ignored, as in the reference.
+// The energy is sum_{i<j} phi. Every particle sums over all its neighbours
+// itself (full list), so each thread owns its particle's force: no atomics,
+// and the summation order is fixed by the list.
 //
-// Both exponentials share one factor: with u+- = ar +- k/2a,
-//   e^{+-kr} erfc(u+-) = erfcx(u+-) exp(-(a^2 r^2 + k^2/4a^2))
-// so a pair costs one exp and two erfcx (CUDA's exp/erfcx, no re-derived
-// math), and f3 = (2a/sqrt(pi)) exp(...)/r.
+// Positions enter as integer fixed-point coordinates, q = frac(x/L) 2^B
+// (B = 32 on the FP32 path, 64 on the FP64 path). The difference of two
+// coordinates is exact, and its two's-complement wrap-around is the minimum
+// image, so no periodic shifts are needed anywhere; converting the (small)
+// difference to floating point rounds it once, relative to dx itself.
 //
-// Layout of the work: one CTA per (home cell, split). The CTA stages the 27
-// neighbour cells' particles, shifted into the home cell's frame, in shared
-// memory; each thread first filters the staged particles by distance into a
-// per-thread list of in-range neighbours (indices in shared memory), then
-// evaluates the pair terms only for the listed ones, so a warp does not pay
-// the transcendental cost for the ~85% of candidates outside the cutoff.
-// Per-thread partial forces are added with Kahan compensation at flush
-// granularity; energies are accumulated in FP64.
+// Lists are rebuilt only when some particle has moved more than skin/2 since
+// the last rebuild (the check is fused into the drift kernel); the rebuild
+// kernels run in every step's launch sequence and return at once otherwise.
+// A list holds every pair closer than rc + skin at rebuild time, so it holds
+// every pair closer than rc until the next rebuild.
+//
+// Pair terms: the FP64 path evaluates the reference's formula directly,
+// written with the shared Gaussian factor
+//   e^{+-kr} erfc(u+-) = erfcx(u+-) exp(-(a^2 r^2 + k^2/4a^2)),  u+- = ar +- k/2a,
+// using CUDA's exp and erfcx. The FP32 path interpolates two smooth functions
+// tabulated on [0, rc] from FP64 values computed on the host,
+//   g(r) = F(r) r^2     psi(r) = phi(r) r
+// (both finite at r = 0), cubic per interval, and forms F/r = g/r^3 and
+// phi = psi/r.
 #include "p3m_kernels.h"
 
 namespace p3m {
 
-template <typename T> struct PairCoef {
-    T a, a2, k, k2a, ce, c3, rc2;
+// ---------------------------------------------------------------------------
+// coordinates
+// ---------------------------------------------------------------------------
+template <typename T> struct Coord;
+template <> struct Coord<float> {
+    using Q = uint4;
+    using U = unsigned int;
+    using I = int;
+    static constexpr double scale = 4294967296.0;  // 2^32
+    __device__ static U q(double t) { return __double2uint_rz(t * scale); }
+};
+template <> struct Coord<double> {
+    using Q = ulonglong4;
+    using U = unsigned long long;
+    using I = long long;
+    static constexpr double scale = 18446744073709551616.0;  // 2^64
+    __device__ static U q(double t) { return __double2ull_rz(t * scale); }
 };
 
-__device__ __forceinline__ float p_rsqrt(float x) { return rsqrtf(x); }
-__device__ __forceinline__ double p_rsqrt(double x) { return rsqrt(x); }
-__device__ __forceinline__ float p_exp(float x) { return expf(x); }
-__device__ __forceinline__ double p_exp(double x) { return exp(x); }
-__device__ __forceinline__ float p_erfcx(float x) { return erfcxf(x); }
-__device__ __forceinline__ double p_erfcx(double x) { return erfcx(x); }
+// frac(x / L) in [0, 1)
+__device__ __forceinline__ double unit_coord(double x, double inv_L)
+{
+    double t = x * inv_L;
+    t -= floor(t);
+    return t < 1.0 ? t : 0.0;
+}
 
-// Pair terms at squared distance r2: F(r)/r and phi(r).
+// Sorted-order integer coordinates, every step: xq[s] = q(pos[cell_perm[s]]);
+// .w holds the replica index.
 template <typename T>
-__device__ __forceinline__ void yukawa_ewald_pair(T r2, const PairCoef<T> &c, T &f_over_r, T &phi)
+__global__ void k_quantize(const RepDev *__restrict__ reps, const int *__restrict__ prep,
+                           const int *__restrict__ cell_perm, const double *__restrict__ pos,
+                           typename Coord<T>::Q *__restrict__ xq, int ntot)
 {
-    T rinv = p_rsqrt(r2);
-    T r = r2 * rinv;
-    T ar = c.a * r;
-    T E = p_exp(-(c.a2 * r2 + c.ce));
-    T xp = p_erfcx(ar + c.k2a);
-    T xm = p_erfcx(ar - c.k2a);
-    T kr = c.k * r;
-    T hE = (T)0.5 * rinv * E;
-    phi = hE * (xp + xm);
-    T fr = hE * rinv * (xp * ((T)1 - kr) + xm * ((T)1 + kr)) + c.c3 * rinv * E;
-    f_over_r = fr * rinv;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < ntot; s += gridDim.x * blockDim.x) {
+        const int i = cell_perm[s];
+        const int r = prep[i];
+        const double il = reps[r].inv_L;
+        typename Coord<T>::Q q;
+        q.x = Coord<T>::q(unit_coord(pos[3 * i + 0], il));
+        q.y = Coord<T>::q(unit_coord(pos[3 * i + 1], il));
+        q.z = Coord<T>::q(unit_coord(pos[3 * i + 2], il));
+        q.w = r;
+        xq[s] = q;
+    }
 }
 
-template <typename T> struct PPCfg;
-template <> struct PPCfg<float> { static constexpr int SCAP = 1536, LCAP = 96; };
-template <> struct PPCfg<double> { static constexpr int SCAP = 1536, LCAP = 96; };
-
-constexpr int PP_THREADS = 128;
-
-// Shared-memory bytes of the PP kernel: staged neighbours (FP64: one double4;
-// FP32: a hi and a lo float4 per particle) and the per-thread lists.
-template <typename T> constexpr size_t pp_smem_bytes()
+// dx of two coordinates (minimum image) in units of L / 2^B
+template <typename T>
+__device__ __forceinline__ typename Coord<T>::I qdiff(typename Coord<T>::U a, typename Coord<T>::U b)
 {
-    return (size_t)PPCfg<T>::SCAP * 32 + (size_t)PPCfg<T>::LCAP * PP_THREADS * sizeof(unsigned short);
+    return (typename Coord<T>::I)(a - b);
 }
 
-// Positions come in as FP64 offsets from the cell origin (double4). The FP64
-// path stages them as they are. The FP32 path stages each coordinate as a
-// pair of floats (hi = fl(x), lo = fl(x - hi)): the cutoff filter uses hi
-// alone, and the pair terms use dx = (xi_hi - xj_hi) + (xi_lo - xj_lo), whose
-// error is a rounding of dx itself rather than of the (larger) coordinates --
-// with plain FP32 coordinates the position rounding alone gives a ~3e-6
-// relative force error.
-template <typename T, int TPI>
-__global__ void __launch_bounds__(PP_THREADS)
-k_pp(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
-     const double4 *__restrict__ xs, typename V4<T>::t *__restrict__ acc_out,
-     double *__restrict__ u_part, int ncell, int split)
+// Index of list entry k of sorted particle s: lists are interleaved by warps
+// of 32 consecutive particles so a warp's k-th entries are contiguous.
+__device__ __forceinline__ long long list_index(int s, int k, int maxnb)
 {
-    using T4 = typename V4<T>::t;
-    constexpr bool F32 = sizeof(T) == 4;
-    constexpr int SCAP = PPCfg<T>::SCAP, LCAP = PPCfg<T>::LCAP;
-    constexpr int ICH = PP_THREADS / TPI;  // i-particles per CTA pass
-    extern __shared__ __align__(16) unsigned char pp_smem[];
-    T4 *stage = reinterpret_cast<T4 *>(pp_smem);               // FP64: double4; FP32: hi
-    float4 *stage_lo = reinterpret_cast<float4 *>(pp_smem + (size_t)SCAP * 16);  // FP32 only
-    unsigned short *list = reinterpret_cast<unsigned short *>(pp_smem + (size_t)SCAP * 32);
+    return ((long long)(s >> 5) * maxnb + k) * 32 + (s & 31);
+}
+
+// ---------------------------------------------------------------------------
+// list build (rebuild steps only)
+// ---------------------------------------------------------------------------
+constexpr int LB_THREADS = 128;
+constexpr int LB_SCAP = 2048;
+
+template <typename T>
+__global__ void __launch_bounds__(LB_THREADS)
+k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
+              const typename Coord<T>::Q *__restrict__ xq, int *__restrict__ nnb,
+              int *__restrict__ nlist, int maxnb, int ncell, const int *__restrict__ rebuild,
+              int *status)
+{
+    using Q = typename Coord<T>::Q;
+    extern __shared__ __align__(16) unsigned char lb_smem[];
+    Q *stage = reinterpret_cast<Q *>(lb_smem);
     __shared__ int pre[28];
     __shared__ int nstart[27];
-    __shared__ double shx[27], shy[27], shz[27];
-    __shared__ double red[32];
-
     const int tid = threadIdx.x;
-    const int il = tid / TPI, sub = tid % TPI;
-
-    for (int item = blockIdx.x; item < ncell * split; item += gridDim.x) {
-        const int hc = item / split, part = item % split;
+    for (int hc = blockIdx.x; hc < ncell; hc += gridDim.x) {
         const int r = find_rep(hc, nrep, [&](int k) { return reps[k].cell_off; });
+        if (!rebuild[r]) continue;  // uniform over the block
         const RepDev &R = reps[r];
         const int nc = R.nc, local = hc - R.cell_off;
         const int cx = local % nc, cy = (local / nc) % nc, cz = local / (nc * nc);
         const int hstart = cell_start[hc], nhome = cell_start[hc + 1] - hstart;
-
-        PairCoef<T> c;
-        c.a = (T)R.alpha;
-        c.a2 = (T)(R.alpha * R.alpha);
-        c.k = (T)R.kappa;
-        c.k2a = (T)(0.5 * R.kappa / R.alpha);
-        c.ce = (T)(0.25 * R.kappa * R.kappa / (R.alpha * R.alpha));
-        c.c3 = (T)(2.0 * R.alpha / 1.7724538509055160273);
-        c.rc2 = (T)(R.rc * R.rc);
-
+        const float sc = (float)(R.L / Coord<T>::scale);
+        const float rl2 = (float)(R.rcl * R.rcl);
         __syncthreads();
         if (tid < 27) {
-            int dx = tid % 3 - 1, dy = (tid / 3) % 3 - 1, dz = tid / 9 - 1;
-            int nx = (cx + dx + nc) % nc, ny = (cy + dy + nc) % nc, nz = (cz + dz + nc) % nc;
-            int nb = R.cell_off + nx + nc * (ny + nc * nz);
+            const int dx = tid % 3 - 1, dy = (tid / 3) % 3 - 1, dz = tid / 9 - 1;
+            const int nx = (cx + dx + nc) % nc, ny = (cy + dy + nc) % nc, nz = (cz + dz + nc) % nc;
+            const int nb = R.cell_off + nx + nc * (ny + nc * nz);
             nstart[tid] = cell_start[nb];
             pre[tid + 1] = cell_start[nb + 1] - cell_start[nb];
-            shx[tid] = dx * R.cellw;
-            shy[tid] = dy * R.cellw;
-            shz[tid] = dz * R.cellw;
         }
         __syncthreads();
         if (tid == 0) {
@@ -131,134 +137,254 @@ k_pp(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_sta
         }
         __syncthreads();
         const int total = pre[27];
-
-        double u_thread = 0.0;
-        const int nchunks = (nhome + ICH - 1) / ICH;
-        for (int ch = part; ch < nchunks; ch += split) {
-            const int i = ch * ICH + il;
-            const bool have_i = i < nhome;
-            T4 xi;          // FP64: position; FP32: hi part
-            float4 xl;      // FP32: lo part
-            if (have_i) {
-                const double4 p = xs[hstart + i];
-                if constexpr (F32) {
-                    xi.x = (float)p.x; xi.y = (float)p.y; xi.z = (float)p.z; xi.w = 0.f;
-                    xl.x = (float)(p.x - (double)xi.x);
-                    xl.y = (float)(p.y - (double)xi.y);
-                    xl.z = (float)(p.z - (double)xi.z);
-                    xl.w = 0.f;
-                } else {
-                    xi.x = p.x; xi.y = p.y; xi.z = p.z; xi.w = 0.0;
-                }
-            } else {
-                xi.x = xi.y = xi.z = (T)1e18;
-                xi.w = (T)0;
-                xl.x = xl.y = xl.z = xl.w = 0.f;
-            }
-            T fx = 0, fy = 0, fz = 0, gx = 0, gy = 0, gz = 0;  // sums and Kahan terms
-
-            for (int w0 = 0; w0 < total; w0 += SCAP) {
-                const int wlen = min(SCAP, total - w0);
+        for (int i0 = 0; i0 < nhome; i0 += LB_THREADS) {
+            const int i = i0 + tid;
+            const bool have = i < nhome;
+            const int s = hstart + i;
+            Q xi;
+            if (have) xi = xq[s];
+            int cnt = 0;
+            for (int w0 = 0; w0 < total; w0 += LB_SCAP) {
+                const int wlen = min(LB_SCAP, total - w0);
                 __syncthreads();
-                for (int k = tid; k < wlen; k += PP_THREADS) {
-                    int g = w0 + k;
+                for (int k = tid; k < wlen; k += LB_THREADS) {
+                    const int g = w0 + k;
                     int cc = 0;
                     while (pre[cc + 1] <= g) ++cc;
-                    const double4 p = xs[nstart[cc] + g - pre[cc]];
-                    const double x = p.x + shx[cc], y = p.y + shy[cc], z = p.z + shz[cc];
-                    T4 h;
-                    h.x = (T)x; h.y = (T)y; h.z = (T)z; h.w = (T)0;
-                    stage[k] = h;
-                    if constexpr (F32) {
-                        stage_lo[k] = make_float4((float)(x - (double)h.x), (float)(y - (double)h.y),
-                                                  (float)(z - (double)h.z), 0.f);
-                    }
+                    const int j = nstart[cc] + g - pre[cc];
+                    Q q = xq[j];
+                    q.w = j;  // the staged copy carries the sorted index
+                    stage[k] = q;
                 }
                 __syncthreads();
-
-                int cnt = 0;
-                auto flush = [&]() {
-                    int mmax = __reduce_max_sync(0xffffffffu, cnt);
-                    T px = 0, py = 0, pz = 0;
-                    T pu = 0;
-                    for (int e = 0; e < mmax; ++e) {
-                        if (e < cnt) {
-                            const int k = list[e * PP_THREADS + tid];
-                            const T4 q = stage[k];
-                            T dx = xi.x - q.x, dy = xi.y - q.y, dz = xi.z - q.z;
-                            if constexpr (F32) {
-                                const float4 ql = stage_lo[k];
-                                dx += xl.x - ql.x;
-                                dy += xl.y - ql.y;
-                                dz += xl.z - ql.z;
-                            }
-                            T r2 = dx * dx + dy * dy + dz * dz;
-                            T fr, ph;
-                            yukawa_ewald_pair<T>(r2, c, fr, ph);
-                            px += fr * dx;
-                            py += fr * dy;
-                            pz += fr * dz;
-                            pu += ph;
-                        }
-                    }
-                    // Kahan-compensated add of the flush partials
-                    T yx = px - gx, tx = fx + yx; gx = (tx - fx) - yx; fx = tx;
-                    T yy = py - gy, ty = fy + yy; gy = (ty - fy) - yy; fy = ty;
-                    T yz = pz - gz, tz = fz + yz; gz = (tz - fz) - yz; fz = tz;
-                    u_thread += (double)pu;
-                    cnt = 0;
-                };
-                for (int k0 = 0; k0 < wlen; k0 += 32) {
-                    const int kmax = min(k0 + 32, wlen);
-                    for (int k = k0 + sub; k < kmax; k += TPI) {
-                        T4 q = stage[k];
-                        T dx = xi.x - q.x, dy = xi.y - q.y, dz = xi.z - q.z;
-                        T r2 = dx * dx + dy * dy + dz * dz;
-                        if (r2 < c.rc2 && r2 > (T)0) {
-                            list[cnt * PP_THREADS + tid] = (unsigned short)k;
+                if (have) {
+                    for (int k = 0; k < wlen; ++k) {
+                        const Q q = stage[k];
+                        const float dx = (float)qdiff<T>(xi.x, q.x) * sc;
+                        const float dy = (float)qdiff<T>(xi.y, q.y) * sc;
+                        const float dz = (float)qdiff<T>(xi.z, q.z) * sc;
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 < rl2 && (int)q.w != s) {
+                            if (cnt < maxnb) nlist[list_index(s, cnt, maxnb)] = (int)q.w;
                             ++cnt;
                         }
                     }
-                    if (__any_sync(0xffffffffu, cnt > LCAP - 32)) flush();
                 }
-                flush();
             }
-            // combine the TPI partial sums of this i (fixed shuffle tree)
-#pragma unroll
-            for (int o = TPI / 2; o > 0; o >>= 1) {
-                fx += __shfl_xor_sync(0xffffffffu, fx, o);
-                fy += __shfl_xor_sync(0xffffffffu, fy, o);
-                fz += __shfl_xor_sync(0xffffffffu, fz, o);
-            }
-            if (have_i && sub == 0) {
-                T4 a;
-                a.x = fx;
-                a.y = fy;
-                a.z = fz;
-                a.w = (T)0;
-                acc_out[hstart + i] = a;
+            if (have) {
+                if (cnt > maxnb) {
+                    raise_status(status, ST_NBOVF);
+                    cnt = maxnb;
+                }
+                nnb[s] = cnt;
             }
         }
-        double u = block_sum(u_thread, red);
-        if (tid == 0) u_part[item] = u;
     }
+}
+
+// ---------------------------------------------------------------------------
+// pair terms
+// ---------------------------------------------------------------------------
+
+// FP64: the reference's pair terms (F(r)/r and phi(r)) at squared distance r2.
+__device__ __forceinline__ void pair_direct(double r2, const RepDev &R, double &f_over_r, double &phi)
+{
+    const double a = R.alpha, k = R.kappa;
+    const double rinv = rsqrt(r2);
+    const double r = r2 * rinv;
+    const double E = exp(-(a * a * r2 + 0.25 * k * k / (a * a)));
+    const double xp = erfcx(a * r + 0.5 * k / a);
+    const double xm = erfcx(a * r - 0.5 * k / a);
+    const double kr = k * r;
+    const double hE = 0.5 * rinv * E;
+    phi = hE * (xp + xm);
+    const double fr = hE * rinv * (xp * (1.0 - kr) + xm * (1.0 + kr)) +
+                      (2.0 * a / 1.7724538509055160273) * rinv * E;
+    f_over_r = fr * rinv;
+}
+
+// FP32: tabulated g and psi; tab holds 2 float4 (cubic coefficients in the
+// interval coordinate u in [0,1)) per interval.
+__device__ __forceinline__ void pair_table(float r2, const float4 *__restrict__ tab, float inv_h,
+                                           float &f_over_r, float &phi)
+{
+    const float rinv = rsqrtf(r2);
+    const float r = r2 * rinv;
+    const float t = r * inv_h;
+    const int i = min((int)t, PP_TABLE_N - 1);
+    const float u = t - (float)i;
+    const float4 cg = tab[2 * i], cp = tab[2 * i + 1];
+    const float g = fmaf(fmaf(fmaf(cg.w, u, cg.z), u, cg.y), u, cg.x);
+    const float ps = fmaf(fmaf(fmaf(cp.w, u, cp.z), u, cp.y), u, cp.x);
+    const float rinv2 = rinv * rinv;
+    f_over_r = g * rinv2 * rinv;
+    phi = ps * rinv;
+}
+
+// ---------------------------------------------------------------------------
+// forces from the lists
+// ---------------------------------------------------------------------------
+constexpr int PPL_THREADS = 256;
+
+template <typename T, int TPI>
+__global__ void __launch_bounds__(PPL_THREADS)
+k_pp_list(const RepDev *__restrict__ reps, int nrep, const typename Coord<T>::Q *__restrict__ xq,
+          const int *__restrict__ nnb, const int *__restrict__ nlist, int maxnb,
+          const float4 *__restrict__ tables, typename V4<T>::t *__restrict__ acc_out,
+          double *__restrict__ u_part)
+{
+    using Q = typename Coord<T>::Q;
+    constexpr bool F32 = sizeof(T) == 4;
+    constexpr int PPB = PPL_THREADS / TPI;  // particles per block
+    constexpr int CH = 32;                  // entries per Kahan flush
+    __shared__ double red[32];
+    extern __shared__ __align__(16) float4 ppl_tab[];  // FP32: this replica's table
+    const int b = blockIdx.x;
+    const int r = find_rep(b, nrep, [&](int k) { return reps[k].pp_blk_off; });
+    const RepDev &R = reps[r];
+    if constexpr (F32) {
+        // every block works on one replica: stage its pair-function table
+        const float4 *src = tables + (long long)r * 2 * PP_TABLE_N;
+        for (int k = threadIdx.x; k < 2 * PP_TABLE_N; k += PPL_THREADS) cp_async16(ppl_tab + k, src + k);
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    const int sub = threadIdx.x % TPI;
+    const int s = R.p_off + (b - R.pp_blk_off) * PPB + threadIdx.x / TPI;
+    const bool have = s < R.p_off + R.n;
+    // L / 2^B as a hi + lo pair: a plain FP32 scale would bias every dx of
+    // the replica by the same relative rounding, which adds up coherently
+    const double scd = R.L / Coord<T>::scale;
+    const T sc = (T)scd, sc_lo = (T)(scd - (double)sc);
+    const T rc2 = (T)(R.rc * R.rc);
+    const float4 *tab = ppl_tab;
+    const float inv_h = (float)(PP_TABLE_N / R.rc);
+
+    T fx = 0, fy = 0, fz = 0, gx = 0, gy = 0, gz = 0;
+    double u = 0.0;
+    if (have) {
+        const Q xi = xq[s];
+        const int n = nnb[s];
+        constexpr int UNR = 8;  // list entries in flight per thread
+        for (int k0 = 0; k0 < n; k0 += CH) {
+            const int k1 = min(k0 + CH, n);
+            T px = 0, py = 0, pz = 0, pu = 0;
+            for (int k = k0 + sub; k < k1; k += UNR * TPI) {
+                // independent loads first (missing entries point at the
+                // particle itself: r2 = 0 is skipped below)
+                int j[UNR];
+#pragma unroll
+                for (int v = 0; v < UNR; ++v) {
+                    const int kk = k + v * TPI;
+                    j[v] = kk < k1 ? __ldg(nlist + list_index(s, kk, maxnb)) : s;
+                }
+                Q q[UNR];
+#pragma unroll
+                for (int v = 0; v < UNR; ++v) q[v] = xq[j[v]];
+#pragma unroll
+                for (int v = 0; v < UNR; ++v) {
+                    const T ix = (T)qdiff<T>(xi.x, q[v].x), iy = (T)qdiff<T>(xi.y, q[v].y),
+                            iz = (T)qdiff<T>(xi.z, q[v].z);
+                    const T dx = ix * sc + ix * sc_lo;
+                    const T dy = iy * sc + iy * sc_lo;
+                    const T dz = iz * sc + iz * sc_lo;
+                    const T r2 = dx * dx + dy * dy + dz * dz;
+                    if (r2 < rc2 && r2 > (T)0) {
+                        T fr, ph;
+                        if constexpr (F32) {
+                            pair_table(r2, tab, inv_h, fr, ph);
+                        } else {
+                            pair_direct(r2, R, fr, ph);
+                        }
+                        px += fr * dx;
+                        py += fr * dy;
+                        pz += fr * dz;
+                        pu += ph;
+                    }
+                }
+            }
+            T yx = px - gx, tx = fx + yx; gx = (tx - fx) - yx; fx = tx;
+            T yy = py - gy, ty = fy + yy; gy = (ty - fy) - yy; fy = ty;
+            T yz = pz - gz, tz = fz + yz; gz = (tz - fz) - yz; fz = tz;
+            u += (double)pu;
+        }
+    }
+#pragma unroll
+    for (int o = TPI / 2; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (have && sub == 0) {
+        typename V4<T>::t a;
+        a.x = fx;
+        a.y = fy;
+        a.z = fz;
+        a.w = (T)0;
+        acc_out[s] = a;
+    }
+    const double ut = block_sum(u, red);
+    if (threadIdx.x == 0) u_part[b] = ut;
+}
+
+// Per-replica U_pp = 1/2 sum of the replica's block partials (index order).
+__global__ void k_reduce_pp(const RepDev *__restrict__ reps, int nrep,
+                            const double *__restrict__ u_part, int nblk_total,
+                            double *__restrict__ rep_out)
+{
+    const int lane = threadIdx.x & 31;
+    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nrep;
+         r += gridDim.x * (blockDim.x >> 5)) {
+        const int b0 = reps[r].pp_blk_off;
+        const int b1 = (r + 1 < nrep) ? reps[r + 1].pp_blk_off : nblk_total;
+        double t = 0.0;
+        for (int k = b0 + lane; k < b1; k += 32) t += u_part[k];
+        t = warp_sum(t);
+        if (lane == 0) rep_out[8 * r + RO_UPP] = 0.5 * t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static int qgrid(int n) { int g = (n + 255) / 256; return g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g); }
+
+int pp_particles_per_block(int tpi) { return PPL_THREADS / tpi; }
+
+template <typename T> void configure_pp_kernels()
+{
+    using Q = typename Coord<T>::Q;
+    cudaFuncSetAttribute(k_build_lists<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(LB_SCAP * sizeof(Q)));
+    const int tab = sizeof(T) == 4 ? (int)(2 * PP_TABLE_N * sizeof(float4)) : 0;
+    cudaFuncSetAttribute(k_pp_list<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
+    cudaFuncSetAttribute(k_pp_list<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
+    cudaFuncSetAttribute(k_pp_list<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
+    cudaFuncSetAttribute(k_pp_list<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
+}
+
+template <typename T> void launch_quantize(const DevState &s, cudaStream_t st)
+{
+    k_quantize<T><<<qgrid(s.ntot), 256, 0, st>>>(s.reps, s.prep, s.cell_perm, s.pos,
+                                                 (typename Coord<T>::Q *)s.xq, s.ntot);
+}
+
+template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st)
+{
+    using Q = typename Coord<T>::Q;
+    const int grid = s.ncell < 148 * 16 ? s.ncell : 148 * 16;
+    k_build_lists<T><<<grid, LB_THREADS, LB_SCAP * sizeof(Q), st>>>(
+        s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.ncell,
+        s.rebuild, s.status);
 }
 
 template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cudaStream_t st)
 {
-    using T4 = typename V4<T>::t;
-    int grid = s.ncell * s.pp_split;
-    k_pp<T, TPI><<<grid, PP_THREADS, pp_smem_bytes<T>(), st>>>(
-        s.reps, s.nrep, s.cell_start, (const double4 *)s.xs_cell, (T4 *)s.acc_pp, s.u_pp_part,
-        s.ncell, s.pp_split);
-}
-
-template <typename T> void configure_pp_kernels()
-{
-    const int smem = (int)pp_smem_bytes<T>();
-    cudaFuncSetAttribute(k_pp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_pp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_pp<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    using Q = typename Coord<T>::Q;
+    const size_t smem = sizeof(T) == 4 ? 2 * PP_TABLE_N * sizeof(float4) : 0;
+    k_pp_list<T, TPI><<<s.pp_nblk, PPL_THREADS, smem, st>>>(s.reps, s.nrep, (const Q *)s.xq, s.nnb,
+                                                         s.nlist, s.maxnb, s.pp_tables,
+                                                         (typename V4<T>::t *)s.acc_pp, s.u_pp_part);
 }
 
 template <typename T> void launch_pp(const DevState &s, cudaStream_t st)
@@ -266,37 +392,23 @@ template <typename T> void launch_pp(const DevState &s, cudaStream_t st)
     switch (s.pp_tpi) {
     case 2: launch_pp_tpi<T, 2>(s, st); break;
     case 4: launch_pp_tpi<T, 4>(s, st); break;
+    case 8: launch_pp_tpi<T, 8>(s, st); break;
     default: launch_pp_tpi<T, 1>(s, st);
-    }
-}
-
-// Per-replica U_pp = 1/2 sum over the replica's (cell, split) partials, in
-// index order (one warp per replica).
-__global__ void k_reduce_pp(const RepDev *__restrict__ reps, int nrep,
-                            const double *__restrict__ u_part, int split, int ncell_total,
-                            double *__restrict__ rep_out)
-{
-    const int lane = threadIdx.x & 31;
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nrep;
-         r += gridDim.x * (blockDim.x >> 5)) {
-        int b = reps[r].cell_off * split;
-        int e = (r + 1 < nrep ? reps[r + 1].cell_off : ncell_total) * split;
-        double t = 0.0;
-        for (int k = b + lane; k < e; k += 32) t += u_part[k];
-        t = warp_sum(t);
-        if (lane == 0) rep_out[8 * r + RO_UPP] = 0.5 * t;
     }
 }
 
 void launch_reduce_pp(const DevState &s, cudaStream_t st)
 {
-    k_reduce_pp<<<(s.nrep + 3) / 4, 128, 0, st>>>(s.reps, s.nrep, s.u_pp_part, s.pp_split,
-                                                  s.ncell, s.rep_out);
+    k_reduce_pp<<<(s.nrep + 3) / 4, 128, 0, st>>>(s.reps, s.nrep, s.u_pp_part, s.pp_nblk,
+                                                  s.rep_out);
 }
 
-template void configure_pp_kernels<float>();
-template void configure_pp_kernels<double>();
-template void launch_pp<float>(const DevState &, cudaStream_t);
-template void launch_pp<double>(const DevState &, cudaStream_t);
+#define P3M_INST(T)                                                         \
+    template void configure_pp_kernels<T>();                                 \
+    template void launch_quantize<T>(const DevState &, cudaStream_t);        \
+    template void launch_build_lists<T>(const DevState &, cudaStream_t);     \
+    template void launch_pp<T>(const DevState &, cudaStream_t);
+P3M_INST(float)
+P3M_INST(double)
 
 }  // namespace p3m

@@ -7,12 +7,16 @@
 // BRICK^3 block of base indices floor(x/h) (yukawa_pm_ord6.py:17-27), folded
 // into [0, M).
 //
-// The cell sort is deterministic: counts and offsets come from integer
-// atomics and a scan; the order inside a cell is then fixed by sorting each
-// cell's particle indices ascending (rank sort), so every rerun stages
-// neighbours in the same order and sums forces in the same order. The brick
-// sort keeps the atomic order because the assignment accumulates in integer
-// fixed point (order-independent) and the gather has no cross-particle sums.
+// The cell sort (the grid of the neighbour-list build, cells >= rc + skin)
+// runs only on rebuild steps, per replica: each replica has its own rebuild
+// flag, its cells are scanned within its own particle range, and the cell
+// kernels skip the work of replicas whose flag is clear -- so a replica's
+// lists, and its rounding, do not depend on the other replicas of a batch. It is deterministic: counts and offsets
+// come from integer atomics and a scan; the order inside a cell is then
+// fixed by sorting each cell's particle indices ascending (rank sort), so
+// every rerun builds the same lists. The brick sort runs every step and keeps
+// the atomic order because the assignment accumulates in integer fixed point
+// (order-independent) and the gather has no cross-particle sums.
 #include "p3m_kernels.h"
 
 namespace p3m {
@@ -36,14 +40,31 @@ __global__ void k_keys(const RepDev *__restrict__ reps, const int *__restrict__ 
     }
 }
 
-// Exclusive scan of one count array into start[0..n] (single block), zeroing
-// the counts and the scatter cursors for the next use.
-__device__ void block_scan_array(int *count, int *start, int *cursor, int n, int *sm)
+// Cell keys of a rebuild step (the drift kernel computed the brick keys).
+__global__ void k_cell_keys(const RepDev *__restrict__ reps, const int *__restrict__ prep,
+                            const double *__restrict__ pos, int ntot, int *__restrict__ cell_key,
+                            int *__restrict__ cell_count, const int *__restrict__ rebuild,
+                            int *status)
 {
-    int carry = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
+        const int r = prep[i];
+        if (!rebuild[r]) continue;
+        const RepDev &R = reps[r];
+        int c, b;
+        particle_keys(R, pos[3 * i + 0], pos[3 * i + 1], pos[3 * i + 2], 0, &c, &b, status);
+        cell_key[i] = c;
+        atomicAdd(&cell_count[c], 1);
+    }
+}
+
+// Exclusive scan of count[0..n) into start[0..n], offset by `base` (single
+// block), zeroing the counts and the scatter cursors for the next use.
+__device__ void block_scan_array(int *count, int *start, int *cursor, int n, int base, int *sm)
+{
+    int carry = base;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
-    for (int base = 0; base < n; base += blockDim.x) {
-        int i = base + tid;
+    for (int b0 = 0; b0 < n; b0 += blockDim.x) {
+        int i = b0 + tid;
         int v = (i < n) ? count[i] : 0;
         int x = v;
 #pragma unroll
@@ -75,25 +96,38 @@ __device__ void block_scan_array(int *count, int *start, int *cursor, int n, int
     if (tid == 0) start[n] = carry;
 }
 
-__global__ void k_scan(int *cell_count, int *cell_start, int *cell_cursor, int ncell,
-                       int *brick_count, int *brick_start, int *brick_cursor, int nbrick)
+// Block 0: the cells of every replica whose rebuild flag is set, each within
+// its own particle range [p_off, p_off + n). Block 1: all bricks.
+__global__ void k_scan(const RepDev *__restrict__ reps, int nrep, int *cell_count,
+                       int *cell_start, int *cell_cursor, int *brick_count, int *brick_start,
+                       int *brick_cursor, int nbrick, const int *__restrict__ rebuild)
 {
     __shared__ int sm[64];
-    if (blockIdx.x == 0)
-        block_scan_array(cell_count, cell_start, cell_cursor, ncell, sm);
-    else if (nbrick > 0)
-        block_scan_array(brick_count, brick_start, brick_cursor, nbrick, sm);
+    if (blockIdx.x == 0) {
+        for (int r = 0; r < nrep; ++r) {
+            if (!rebuild[r]) continue;
+            const RepDev &R = reps[r];
+            const int c0 = R.cell_off, nc = R.nc * R.nc * R.nc;
+            block_scan_array(cell_count + c0, cell_start + c0, cell_cursor + c0, nc, R.p_off, sm);
+            __syncthreads();
+        }
+    } else if (nbrick > 0) {
+        block_scan_array(brick_count, brick_start, brick_cursor, nbrick, 0, sm);
+    }
 }
 
 __global__ void k_scatter(const int *__restrict__ cell_key, const int *__restrict__ cell_start,
                           int *cell_cursor, int *__restrict__ cell_tmp,
                           const int *__restrict__ brick_key, const int *__restrict__ brick_start,
                           int *brick_cursor, int *__restrict__ brick_perm,
-                          int *__restrict__ brick_slot, int ntot, int has_mesh)
+                          int *__restrict__ brick_slot, int ntot, int has_mesh,
+                          const int *__restrict__ prep, const int *__restrict__ rebuild)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
-        int c = cell_key[i];
-        cell_tmp[cell_start[c] + atomicAdd(&cell_cursor[c], 1)] = i;
+        if (rebuild[prep[i]]) {
+            int c = cell_key[i];
+            cell_tmp[cell_start[c] + atomicAdd(&cell_cursor[c], 1)] = i;
+        }
         if (has_mesh) {
             int b = brick_key[i];
             int s = brick_start[b] + atomicAdd(&brick_cursor[b], 1);
@@ -103,21 +137,19 @@ __global__ void k_scatter(const int *__restrict__ cell_key, const int *__restric
     }
 }
 
-// One warp per cell: order the cell's particles by index and write their
-// positions relative to the cell origin (FP64) in that order.
+// One warp per cell: order the cell's particles by index, and remember every
+// particle's position at this rebuild (the reference point of the skin check).
 __global__ void k_fix_cells(const RepDev *__restrict__ reps, int nrep,
                             const int *__restrict__ cell_start, const int *__restrict__ cell_tmp,
                             const double *__restrict__ pos, int *__restrict__ cell_perm,
-                            int *__restrict__ cell_slot, double4 *__restrict__ xs, int ncell)
+                            int *__restrict__ cell_slot, double *__restrict__ pos_ref, int ncell,
+                            const int *__restrict__ rebuild)
 {
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     for (int c = blockIdx.x * wpb + (threadIdx.x >> 5); c < ncell; c += gridDim.x * wpb) {
-        const int r = find_rep(c, nrep, [&](int k) { return reps[k].cell_off; });
-        const RepDev &R = reps[r];
+        if (!rebuild[find_rep(c, nrep, [&](int k) { return reps[k].cell_off; })]) continue;
         const int start = cell_start[c], n = cell_start[c + 1] - start;
-        const int local = c - R.cell_off;
-        const int cx = local % R.nc, cy = (local / R.nc) % R.nc, cz = local / (R.nc * R.nc);
         for (int e0 = 0; e0 < n; e0 += 32) {
             int e = e0 + lane;
             int v = (e < n) ? cell_tmp[start + e] : 0x7fffffff;
@@ -127,10 +159,9 @@ __global__ void k_fix_cells(const RepDev *__restrict__ reps, int nrep,
                 int s = start + rank;
                 cell_perm[s] = v;
                 cell_slot[v] = s;
-                double x = fold_box(pos[3 * v + 0], R.L);
-                double y = fold_box(pos[3 * v + 1], R.L);
-                double z = fold_box(pos[3 * v + 2], R.L);
-                xs[s] = make_double4(x - cx * R.cellw, y - cy * R.cellw, z - cz * R.cellw, 0.0);
+                pos_ref[3 * v + 0] = pos[3 * v + 0];
+                pos_ref[3 * v + 1] = pos[3 * v + 1];
+                pos_ref[3 * v + 2] = pos[3 * v + 2];
             }
         }
     }
@@ -150,11 +181,17 @@ template <typename T> void launch_keys(const DevState &s, cudaStream_t st)
                                                       s.has_mesh, s.status);
 }
 
+void launch_cell_keys(const DevState &s, cudaStream_t st)
+{
+    k_cell_keys<<<grid_for(s.ntot, 256), 256, 0, st>>>(s.reps, s.prep, s.pos, s.ntot, s.cell_key,
+                                                       s.cell_count, s.rebuild, s.status);
+}
+
 void launch_scan(const DevState &s, cudaStream_t st)
 {
-    k_scan<<<2, 1024, 0, st>>>(s.cell_count, s.cell_start, s.cell_cursor, s.ncell,
+    k_scan<<<2, 1024, 0, st>>>(s.reps, s.nrep, s.cell_count, s.cell_start, s.cell_cursor,
                                s.brick_count, s.brick_start, s.brick_cursor,
-                               s.has_mesh ? s.nbrick : 0);
+                               s.has_mesh ? s.nbrick : 0, s.rebuild);
 }
 
 void launch_scatter(const DevState &s, cudaStream_t st)
@@ -162,7 +199,8 @@ void launch_scatter(const DevState &s, cudaStream_t st)
     k_scatter<<<grid_for(s.ntot, 256), 256, 0, st>>>(s.cell_key, s.cell_start, s.cell_cursor,
                                                       s.cell_tmp, s.brick_key, s.brick_start,
                                                       s.brick_cursor, s.brick_perm,
-                                                      s.brick_slot, s.ntot, s.has_mesh);
+                                                      s.brick_slot, s.ntot, s.has_mesh, s.prep,
+                                                      s.rebuild);
 }
 
 template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st)
@@ -170,8 +208,8 @@ template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st)
     const int wpb = 8;
     int blocks = (s.ncell + wpb - 1) / wpb;
     k_fix_cells<<<blocks, wpb * 32, 0, st>>>(s.reps, s.nrep, s.cell_start, s.cell_tmp, s.pos,
-                                             s.cell_perm, s.cell_slot, (double4 *)s.xs_cell,
-                                             s.ncell);
+                                             s.cell_perm, s.cell_slot, s.pos_ref, s.ncell,
+                                             s.rebuild);
 }
 
 template void launch_keys<float>(const DevState &, cudaStream_t);

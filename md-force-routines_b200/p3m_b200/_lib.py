@@ -21,6 +21,7 @@ P3M_ENODEV = -3
 P3M_EBOX = -4
 P3M_ENONFINITE = -5
 P3M_ESTATE = -6
+P3M_ENBOVF = -7
 
 FP64 = 0
 FP32 = 1
@@ -53,6 +54,7 @@ class ReplicaDesc(ctypes.Structure):
         ("af", ctypes.c_double),
         ("uf", ctypes.c_double),
         ("kf", ctypes.c_double),
+        ("skin", ctypes.c_double),
     ]
 
 
@@ -89,8 +91,9 @@ SIGNATURES = {
     "p3m_check": (_I, [_V]),
     "p3m_sync": (_I, [_V]),
     "p3m_stream": (_V, [_V]),
-    "p3m_set_pp_config": (_I, [_V, _I, _I]),
-    "p3m_get_pp_config": (_I, [_V, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "p3m_set_pp_config": (_I, [_V, _I, ctypes.c_double]),
+    "p3m_get_pp_config": (_I, [_V, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(_I)]),
     "p3m_profile_stages": (_I, [_V, _I, _D, _I, ctypes.POINTER(_I)]),
     "p3m_stage_name": (ctypes.c_char_p, [_I]),
     "p3m_fp32_peak": (_I, [_I, _D]),

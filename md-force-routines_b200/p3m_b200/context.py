@@ -28,13 +28,14 @@ class Replica:
     kf: float = 1.5
     p: int = 6
     m_alias: int = 3
+    skin: float = -1.0  # Verlet-list skin; negative: the library's default
     seed: int = field(default=0, compare=False)
 
     def desc(self) -> ReplicaDesc:
         return ReplicaDesc(int(self.N), int(self.M), int(self.p), int(self.m_alias),
                            float(self.L), float(self.kappa), float(self.alpha), float(self.rc),
                            float(self.dt), float(self.T_desired), float(self.af),
-                           float(self.uf), float(self.kf))
+                           float(self.uf), float(self.kf), float(self.skin))
 
 
 def _f64(a, shape=None):
@@ -243,13 +244,16 @@ class Context:
         self._ck(lib().p3m_profile_stages(self.handle, int(iters), dptr(ms), 16, ctypes.byref(n)))
         return {lib().p3m_stage_name(i).decode(): float(ms[i]) for i in range(n.value)}
 
-    def set_pp_config(self, tpi, split):
-        self._ck(lib().p3m_set_pp_config(self.handle, int(tpi), int(split)))
+    def set_pp_config(self, tpi, skin=-1.0):
+        """Threads per particle of the PP force kernel and the list skin."""
+        self._ck(lib().p3m_set_pp_config(self.handle, int(tpi), float(skin)))
 
     def pp_config(self):
-        t, s = ctypes.c_int(), ctypes.c_int()
-        self._ck(lib().p3m_get_pp_config(self.handle, ctypes.byref(t), ctypes.byref(s)))
-        return t.value, s.value
+        """-> (threads per particle, skin, list capacity)."""
+        t, s, m = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        self._ck(lib().p3m_get_pp_config(self.handle, ctypes.byref(t), ctypes.byref(s),
+                                         ctypes.byref(m)))
+        return t.value, s.value, m.value
 
 
 def gf_opt_device(kappa, alpha, p, m_alias, M, L, device=0):

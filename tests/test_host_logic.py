@@ -21,7 +21,7 @@ def test_replica_desc_layout():
 
     from p3m_b200._lib import ReplicaDesc
 
-    assert ctypes.sizeof(ReplicaDesc) == 4 * 4 + 9 * 8
+    assert ctypes.sizeof(ReplicaDesc) == 4 * 4 + 10 * 8
 
 
 def test_non_cubic_rejected_before_device():
