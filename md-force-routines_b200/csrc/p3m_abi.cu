@@ -195,7 +195,7 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
                     s.cell_start, s.cell_cursor, s.cell_tmp, s.cell_perm, s.cell_slot, s.xq, s.nnb,
                     s.nlist, s.rebuild, s.pos_ref, s.pp_tables,
                     s.acc_pp, s.brick_key, s.brick_count, s.brick_start, s.brick_cursor,
-                    s.brick_perm, s.brick_slot, s.tiles, s.spec, s.ek, s.green, s.efield,
+                    s.brick_perm, s.brick_slot, s.brick_tmp, s.tiles, s.spec, s.ek, s.green, s.efield,
                     s.acc_pm, s.twiddle, s.u_pp_part, s.u_pm_part, s.kin_part, s.rep_out,
                     s.status, ctx->counters, ctx->ring, ctx->qmult, ctx->nqt_part,
                     ctx->nqt_ring, ctx->scratch, ctx->ep, ctx->tmp_nq};
@@ -422,6 +422,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(dalloc(&s.brick_start, (size_t)brick + 1));
     CKC(dalloc(&s.brick_cursor, (size_t)brick));
     CKC(dalloc(&s.brick_perm, (size_t)p));
+    CKC(dalloc(&s.brick_tmp, (size_t)p));
     CKC(dalloc(&s.brick_slot, (size_t)p));
     if (with_mesh)
         CKC(valloc(&s.tiles, (size_t)tile * (precision == P3M_FP32 ? sizeof(float) : sizeof(double))));
@@ -479,6 +480,10 @@ template <typename T> static void seq_sort(p3m_ctx *ctx, bool keys)
     launch_quantize<T>(s, ctx->st);     // sorted coordinates of this step
     launch_build_lists<T>(s, ctx->st);  // from those coordinates (rebuild steps)
     ctx->launches += 5;
+    if (s.has_mesh) {
+        launch_fix_bricks(s, ctx->st);
+        ctx->launches++;
+    }
 }
 
 template <typename T> static void seq_pp(p3m_ctx *ctx)
@@ -1012,7 +1017,7 @@ template <typename T> static int do_run(p3m_ctx *ctx, int n_steps, int mode, int
             const long long before = ctx->launches;
             CK(cudaGraphLaunch(ctx->graph[gi][gr], ctx->st));
             // count the kernels the graph holds (same sequence as seq_step)
-            ctx->launches = before + (long long)(11 + (s.has_mesh ? 3 + fft_kernel_count(s) : 0) + (gi ? 1 : 0) +
+            ctx->launches = before + (long long)(11 + (s.has_mesh ? 4 + fft_kernel_count(s) : 0) + (gi ? 1 : 0) +
                                                  ((gr && ctx->nq > 0) ? 2 : 0));
         } else {
             seq_step<T>(ctx, mode, rec);

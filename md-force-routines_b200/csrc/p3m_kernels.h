@@ -40,7 +40,8 @@ struct DevState {
     void *acc_pp = nullptr;      // V4<T> PP acceleration, cell-sorted order
     // brick sort
     int *brick_key = nullptr, *brick_count = nullptr, *brick_start = nullptr;
-    int *brick_cursor = nullptr, *brick_perm = nullptr, *brick_slot = nullptr;
+    int *brick_cursor = nullptr, *brick_tmp = nullptr, *brick_perm = nullptr,
+        *brick_slot = nullptr;
     // mesh
     void *tiles = nullptr;       // T assignment tiles [brick][TILE^3]
     void *spec = nullptr;        // C2<T> half spectrum rho_k / phi_k, [kx][z][y]
@@ -60,8 +61,6 @@ struct DevState {
 enum RepOut { RO_UPP = 0, RO_UPM = 1, RO_USELF = 2, RO_U = 3, RO_K = 4, RO_T = 5, RO_FACT = 6,
               RO_REBUILDS = 7 };
 
-// fixed-point scale of the deterministic charge assignment
-constexpr double ASSIGN_SCALE = 1099511627776.0;  // 2^40
 
 template <typename T> void configure_pp_kernels();
 template <typename T> void configure_mesh_kernels();
@@ -70,6 +69,7 @@ void launch_cell_keys(const DevState &s, cudaStream_t st);
 void launch_scan(const DevState &s, cudaStream_t st);
 void launch_scatter(const DevState &s, cudaStream_t st);
 template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st);
+void launch_fix_bricks(const DevState &s, cudaStream_t st);
 template <typename T> void launch_quantize(const DevState &s, cudaStream_t st);
 template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st);
 template <typename T> void launch_pp(const DevState &s, cudaStream_t st);

@@ -23,10 +23,10 @@
 //   efield  T     [3][z][y][x]      real field meshes, x fastest
 //
 // Assignment is deterministic: each CTA owns one brick of BRICK^3 base
-// cells and accumulates its particles' 216-node stencils into a shared-memory
-// tile of TILE^3 nodes in 64-bit fixed point (scale 2^40), so the sum does
-// not depend on the order in which threads add. Overlapping tile halos are
-// summed (again as integers) when the first FFT pass reads the mesh.
+// cells and adds its particles' 216-node stencils into a shared-memory tile
+// of TILE^3 nodes in a fixed particle order without atomics (see k_assign).
+// Overlapping tile halos are summed in a fixed order when the first FFT pass
+// reads the mesh.
 //
 // The FFT is an in-place radix-2 decimation-in-time transform of 16 lines
 // at a time held in shared memory ([element][line], line stride padded to
@@ -108,59 +108,111 @@ __device__ __forceinline__ int wrapM(int i, int M)
     return i < 0 ? i + M : i;
 }
 
+// One CTA of A_WARPS warps per brick. The brick's particles come in a fixed
+// order (ascending particle index, from the brick sort); their weights are
+// computed once per chunk; then warp w adds the stencils of all particles,
+// in that order, to the tile planes z = w (mod A_WARPS) only -- exactly two of
+// each particle's six planes, 72 nodes, spread over the lanes. No two warps
+// touch the same node and each warp adds its particles one after another, so
+// every node receives its contributions in the same order on every run and
+// no atomics are needed.
+constexpr int A_WARPS = 3;
+constexpr int A_THREADS = 32 * A_WARPS;
+constexpr int A_CHUNK = 128;   // particles per weight chunk
+
+template <typename T> struct AssignW {
+    T wx[6], wy[6], wz[6];  // wx carries the charge
+    int base;               // (lz * TILE + ly) * TILE + lx, or -1
+    int lz;
+};
+
+template <typename T> constexpr size_t assign_smem()
+{
+    return (size_t)TILE3 * sizeof(T) + (size_t)A_CHUNK * sizeof(AssignW<T>);
+}
+
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(A_THREADS)
 k_assign(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_start,
          const int *__restrict__ brick_perm, const double *__restrict__ pos,
-         const double *__restrict__ charge, T *__restrict__ tiles, int nbrick)
+         const double *__restrict__ charge, T *__restrict__ tiles, int nbrick, int *status)
 {
-    extern __shared__ __align__(16) unsigned long long tile[];
+    extern __shared__ __align__(16) unsigned char a_smem[];
+    T *tile = reinterpret_cast<T *>(a_smem);
+    AssignW<T> *W = reinterpret_cast<AssignW<T> *>(a_smem + (size_t)TILE3 * sizeof(T));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // this lane's nodes of a particle's two planes: node = lane + 32 pass < 72
+    int l_off[3];
+    bool l_ok[3];
+    int l_pl[3];
+#pragma unroll
+    for (int ps = 0; ps < 3; ++ps) {
+        const int n = lane + 32 * ps;
+        l_ok[ps] = n < 72;
+        const int pl = n / 36, rem = n % 36, dy = rem / 6, dx = rem % 6;
+        l_pl[ps] = pl;
+        l_off[ps] = (3 * pl * TILE + dy) * TILE + dx;  // relative to (p1, ly, lx)
+    }
     for (int b = blockIdx.x; b < nbrick; b += gridDim.x) {
         const int r = find_rep(b, nrep, [&](int k) { return reps[k].brick_off; });
         const RepDev &R = reps[r];
         const int nb = R.nb, M = R.M, local = b - R.brick_off;
         const int bx = (local % nb) * BRICK, by = ((local / nb) % nb) * BRICK,
                   bz = (local / (nb * nb)) * BRICK;
+        const int p0 = brick_start[b];
+        const int n = brick_start[b + 1] - p0;
         __syncthreads();
-        for (int k = threadIdx.x; k < TILE3; k += blockDim.x) tile[k] = 0ull;
-        __syncthreads();
-        const int p0 = brick_start[b], p1 = brick_start[b + 1];
-        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-            const int i = brick_perm[p];
-            double ox, oy, oz;
-            int ix = base_offset(pos[3 * i + 0], R.h, ox);
-            int iy = base_offset(pos[3 * i + 1], R.h, oy);
-            int iz = base_offset(pos[3 * i + 2], R.h, oz);
-            const int lx = wrapM(ix, M) - bx, ly = wrapM(iy, M) - by, lz = wrapM(iz, M) - bz;
-            // a particle outside [-L, 2L) was filed under brick 0 by the key
-            // pass (and flagged there); it must not reach outside this tile
-            if ((unsigned)lx >= (unsigned)BRICK || (unsigned)ly >= (unsigned)BRICK ||
-                (unsigned)lz >= (unsigned)BRICK)
-                continue;
-            T wx[6], wy[6], wz[6];
-            weights6<T>((T)ox, wx);
-            weights6<T>((T)oy, wy);
-            weights6<T>((T)oz, wz);
-            const T q = (T)charge[i];
+        for (int k = threadIdx.x; k < TILE3; k += A_THREADS) tile[k] = (T)0;
+        for (int c0 = 0; c0 < n; c0 += A_CHUNK) {
+            const int cn = min(A_CHUNK, n - c0);
+            __syncthreads();
+            for (int k = threadIdx.x; k < cn; k += A_THREADS) {
+                const int i = brick_perm[p0 + c0 + k];
+                double ox, oy, oz;
+                const int ix = base_offset(pos[3 * i + 0], R.h, ox);
+                const int iy = base_offset(pos[3 * i + 1], R.h, oy);
+                const int iz = base_offset(pos[3 * i + 2], R.h, oz);
+                const int lx = wrapM(ix, M) - bx, ly = wrapM(iy, M) - by, lz = wrapM(iz, M) - bz;
+                AssignW<T> w;
+                // a particle outside [-L, 2L) was filed under brick 0 and
+                // flagged by the key pass; it must not reach outside the tile
+                if ((unsigned)lx < (unsigned)BRICK && (unsigned)ly < (unsigned)BRICK &&
+                    (unsigned)lz < (unsigned)BRICK) {
+                    weights6<T>((T)ox, w.wx);
+                    weights6<T>((T)oy, w.wy);
+                    weights6<T>((T)oz, w.wz);
+                    const T q = (T)charge[i];
 #pragma unroll
-            for (int g = 0; g < 6; ++g) {
+                    for (int c = 0; c < 6; ++c) w.wx[c] *= q;
+                    w.base = (lz * TILE + ly) * TILE + lx;
+                    w.lz = lz;
+                } else {
+                    w.base = -1;
+                    w.lz = 0;
+                }
+                W[k] = w;
+            }
+            __syncthreads();
+            for (int k = 0; k < cn; ++k) {
+                const AssignW<T> &w = W[k];
+                if (w.base < 0) continue;  // uniform over the block
+                // the first of this warp's two planes of the particle: lz <= p1 < lz + 3
+                const int d = ((warp - w.lz) % A_WARPS + A_WARPS) % A_WARPS;
+                const int first = w.base + d * TILE * TILE;
 #pragma unroll
-                for (int a = 0; a < 6; ++a) {
-                    const T qzy = q * wz[g] * wy[a];
-                    unsigned long long *row = &tile[((lz + g) * TILE + (ly + a)) * TILE + lx];
-#pragma unroll
-                    for (int c = 0; c < 6; ++c) {
-                        double v = (double)(qzy * wx[c]) * ASSIGN_SCALE;
-                        atomicAdd(row + c, (unsigned long long)__double2ll_rn(v));
+                for (int ps = 0; ps < 3; ++ps) {
+                    if (l_ok[ps]) {
+                        const int rem = (lane + 32 * ps) % 36;
+                        const T wgt = w.wz[d + 3 * l_pl[ps]] * w.wy[rem / 6] * w.wx[rem % 6];
+                        tile[first + l_off[ps]] += wgt;
                     }
                 }
+                __syncwarp();
             }
         }
         __syncthreads();
-        // the tile's exact integer sums, rounded once to T
         T *dst = tiles + R.tile_off + (long long)local * TILE3;
-        for (int k = threadIdx.x; k < TILE3; k += blockDim.x)
-            dst[k] = (T)((double)(long long)tile[k] * (1.0 / ASSIGN_SCALE));
+        for (int k = threadIdx.x; k < TILE3; k += A_THREADS) dst[k] = tile[k];
     }
 }
 
@@ -691,7 +743,7 @@ static int grid_items(int n, int cap = 148 * 8) { return n < cap ? (n > 0 ? n : 
 
 template <typename T> void configure_mesh_kernels()
 {
-    set_smem(k_assign<T>, TILE3 * sizeof(unsigned long long));
+    set_smem(k_assign<T>, assign_smem<T>());
     set_smem(k_fft_x_r2c<T>, fft_smem<T>(256, 1));
     set_smem(k_fft_y<T>, fft_smem<T>(256, 1));
     set_smem(k_fft_z_green<T>, fft_smem<T>(256, 2));
@@ -702,9 +754,10 @@ template <typename T> void configure_mesh_kernels()
 
 template <typename T> void launch_assign(const DevState &s, cudaStream_t st)
 {
-    const size_t smem = TILE3 * sizeof(unsigned long long);
-    k_assign<T><<<grid_items(s.nbrick, 148 * 16), 256, smem, st>>>(
-        s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (T *)s.tiles, s.nbrick);
+    const size_t smem = assign_smem<T>();
+    k_assign<T><<<grid_items(s.nbrick, 148 * 16), A_THREADS, smem, st>>>(
+        s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (T *)s.tiles, s.nbrick,
+        s.status);
 }
 
 template <typename T> void launch_fft_forward(const DevState &s, cudaStream_t st)

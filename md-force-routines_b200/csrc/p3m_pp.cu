@@ -210,9 +210,12 @@ __device__ __forceinline__ void pair_table(float r2, const float4 *__restrict__ 
 {
     const float rinv = rsqrtf(r2);
     const float r = r2 * rinv;
-    const float t = r * inv_h;
-    const int i = min((int)t, PP_TABLE_N - 1);
-    const float u = t - (float)i;
+    const float t = r * inv_h;  // in [0, PP_TABLE_N) inside the cutoff
+    // i = round(t - 1/2) and float(i) by the 1.5 * 2^23 rounding constant
+    // (exact for |t| < 2^22), without float <-> int conversions
+    const float tb = (t - 0.5f) + 12582912.0f;
+    const int i = min(__float_as_int(tb) - 0x4B400000, PP_TABLE_N - 1);
+    const float u = t - (tb - 12582912.0f);
     const float4 cg = tab[2 * i], cp = tab[2 * i + 1];
     const float g = fmaf(fmaf(fmaf(cg.w, u, cg.z), u, cg.y), u, cg.x);
     const float ps = fmaf(fmaf(fmaf(cp.w, u, cp.z), u, cp.y), u, cp.x);

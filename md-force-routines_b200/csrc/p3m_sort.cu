@@ -14,9 +14,9 @@
 // lists, and its rounding, do not depend on the other replicas of a batch. It is deterministic: counts and offsets
 // come from integer atomics and a scan; the order inside a cell is then
 // fixed by sorting each cell's particle indices ascending (rank sort), so
-// every rerun builds the same lists. The brick sort runs every step and keeps
-// the atomic order because the assignment accumulates in integer fixed point
-// (order-independent) and the gather has no cross-particle sums.
+// every rerun builds the same lists. The brick sort runs every step; each
+// brick's particles are then put in ascending index order the same way, so
+// the assignment adds them in a fixed order.
 #include "p3m_kernels.h"
 
 namespace p3m {
@@ -119,8 +119,8 @@ __global__ void k_scan(const RepDev *__restrict__ reps, int nrep, int *cell_coun
 __global__ void k_scatter(const int *__restrict__ cell_key, const int *__restrict__ cell_start,
                           int *cell_cursor, int *__restrict__ cell_tmp,
                           const int *__restrict__ brick_key, const int *__restrict__ brick_start,
-                          int *brick_cursor, int *__restrict__ brick_perm,
-                          int *__restrict__ brick_slot, int ntot, int has_mesh,
+                          int *brick_cursor, int *__restrict__ brick_tmp,
+                          int ntot, int has_mesh,
                           const int *__restrict__ prep, const int *__restrict__ rebuild)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
@@ -130,9 +130,7 @@ __global__ void k_scatter(const int *__restrict__ cell_key, const int *__restric
         }
         if (has_mesh) {
             int b = brick_key[i];
-            int s = brick_start[b] + atomicAdd(&brick_cursor[b], 1);
-            brick_perm[s] = i;
-            brick_slot[i] = s;
+            brick_tmp[brick_start[b] + atomicAdd(&brick_cursor[b], 1)] = i;
         }
     }
 }
@@ -162,6 +160,27 @@ __global__ void k_fix_cells(const RepDev *__restrict__ reps, int nrep,
                 pos_ref[3 * v + 0] = pos[3 * v + 0];
                 pos_ref[3 * v + 1] = pos[3 * v + 1];
                 pos_ref[3 * v + 2] = pos[3 * v + 2];
+            }
+        }
+    }
+}
+
+// One warp per brick: order the brick's particles by index.
+__global__ void k_fix_bricks(const int *__restrict__ brick_start, const int *__restrict__ brick_tmp,
+                             int *__restrict__ brick_perm, int *__restrict__ brick_slot, int nbrick)
+{
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int b = blockIdx.x * wpb + (threadIdx.x >> 5); b < nbrick; b += gridDim.x * wpb) {
+        const int start = brick_start[b], n = brick_start[b + 1] - start;
+        for (int e0 = 0; e0 < n; e0 += 32) {
+            const int e = e0 + lane;
+            const int v = (e < n) ? brick_tmp[start + e] : 0x7fffffff;
+            int rank = 0;
+            for (int f = 0; f < n; ++f) rank += (brick_tmp[start + f] < v) ? 1 : 0;
+            if (e < n) {
+                brick_perm[start + rank] = v;
+                brick_slot[v] = start + rank;
             }
         }
     }
@@ -198,9 +217,16 @@ void launch_scatter(const DevState &s, cudaStream_t st)
 {
     k_scatter<<<grid_for(s.ntot, 256), 256, 0, st>>>(s.cell_key, s.cell_start, s.cell_cursor,
                                                       s.cell_tmp, s.brick_key, s.brick_start,
-                                                      s.brick_cursor, s.brick_perm,
-                                                      s.brick_slot, s.ntot, s.has_mesh, s.prep,
-                                                      s.rebuild);
+                                                      s.brick_cursor, s.brick_tmp, s.ntot,
+                                                      s.has_mesh, s.prep, s.rebuild);
+}
+
+void launch_fix_bricks(const DevState &s, cudaStream_t st)
+{
+    const int wpb = 8;
+    k_fix_bricks<<<(s.nbrick + wpb - 1) / wpb, wpb * 32, 0, st>>>(s.brick_start, s.brick_tmp,
+                                                                 s.brick_perm, s.brick_slot,
+                                                                 s.nbrick);
 }
 
 template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st)
