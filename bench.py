@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--replicas", type=int, default=20)
     ap.add_argument("--equil", type=int, default=300,
                     help="untimed thermostat steps before the NVE warm-up")
+    ap.add_argument("--no-tune", action="store_true", help="skip the PP autotuner")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the FP64, e2e, roofline and CPU-baseline legs")
     return ap.parse_args()
@@ -276,7 +277,13 @@ def run_ours(args):
     # equilibration with the reference's thermostat (thermostat_p3m_ord6.vscale)
     # from the random initial state, then NVE warm-up (also builds the graph)
     ctx.run(args.equil, MODE_THERMOSTAT, it0=0, graph=True)
+    tuned = None
+    if not args.no_tune:
+        from p3m_b200.autotune import tune
+
+        tuned = tune(ctx, use_cache=False)
     ctx.run(max(args.warmup, 3), MODE_NVE, record_nqt=True, graph=True)
+    rb0 = sum(ctx.replica_stats(i)["rebuilds"] for i in range(len(reps)))
 
     def barrier():
         if world > 1:
@@ -298,6 +305,7 @@ def run_ours(args):
     ctx.sync()
     ms = e0.elapsed_time(e1)
     launches = ctx.launch_count() - n0
+    rebuilds = sum(ctx.replica_stats(i)["rebuilds"] for i in range(len(reps))) - rb0
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
@@ -321,7 +329,9 @@ def run_ours(args):
                               if working_set_mb(reps) > 126 else
                               f"working set {working_set_mb(reps):.0f} MB fits L2; no flush"),
                        "pp_config": dict(zip(("threads_per_particle", "skin", "list_capacity"),
-                                             ctx.pp_config()))},
+                                             ctx.pp_config())),
+                       "list_rebuilds_per_replica_step": rebuilds / (len(reps) * args.steps),
+                       "autotune_ms_per_step": tuned["ms_per_step"] if tuned else None},
             "gpu_launches": launches, "clocks": clocks}
 
     if not args.no_extras and rank == 0:

@@ -179,6 +179,10 @@ int p3m_get_energies(p3m_ctx *ctx, double *out, int max_steps, int *n_out);
  * interleaved (re,im) doubles. */
 int p3m_get_nqt(p3m_ctx *ctx, int replica, double *out, int max_steps, int *n_out);
 
+/* Last values of one replica (8 doubles): U_short, U_fft, U_self, U, K, T,
+ * thermostat factor, and the number of neighbour-list rebuilds so far. */
+int p3m_get_replica_stats(p3m_ctx *ctx, int replica, double *out);
+
 /* Device status word accumulated since the last call (P3M_OK or the first
  * error seen by a kernel), then cleared. Synchronises the stream. */
 int p3m_check(p3m_ctx *ctx);

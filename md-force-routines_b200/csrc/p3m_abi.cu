@@ -1083,6 +1083,16 @@ extern "C" int p3m_get_nqt(p3m_ctx *ctx, int replica, double *out, int max_steps
     return P3M_OK;
 }
 
+extern "C" int p3m_get_replica_stats(p3m_ctx *ctx, int replica, double *out)
+{
+    if (!ctx || !out) return fail(ctx, P3M_EARG, "p3m_get_replica_stats", "NULL argument");
+    if (replica < 0 || replica >= ctx->nrep) return fail(ctx, P3M_EARG, "p3m_get_replica_stats", "replica");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaMemcpy(out, ctx->s.rep_out + 8 * (size_t)replica, 8 * sizeof(double), cudaMemcpyDeviceToHost));
+    return P3M_OK;
+}
+
 extern "C" int p3m_check(p3m_ctx *ctx)
 {
     if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");

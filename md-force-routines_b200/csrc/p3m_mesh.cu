@@ -111,12 +111,12 @@ __device__ __forceinline__ int wrapM(int i, int M)
 // One CTA of A_WARPS warps per brick. The brick's particles come in a fixed
 // order (ascending particle index, from the brick sort); their weights are
 // computed once per chunk; then warp w adds the stencils of all particles,
-// in that order, to the tile planes z = w (mod A_WARPS) only -- exactly two of
-// each particle's six planes, 72 nodes, spread over the lanes. No two warps
+// in that order, to the tile planes z = w (mod 6) only -- exactly one of each
+// particle's six planes, 36 nodes, spread over the lanes. No two warps
 // touch the same node and each warp adds its particles one after another, so
 // every node receives its contributions in the same order on every run and
 // no atomics are needed.
-constexpr int A_WARPS = 3;
+constexpr int A_WARPS = 6;
 constexpr int A_THREADS = 32 * A_WARPS;
 constexpr int A_CHUNK = 128;   // particles per weight chunk
 
@@ -141,18 +141,10 @@ k_assign(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
     T *tile = reinterpret_cast<T *>(a_smem);
     AssignW<T> *W = reinterpret_cast<AssignW<T> *>(a_smem + (size_t)TILE3 * sizeof(T));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // this lane's nodes of a particle's two planes: node = lane + 32 pass < 72
-    int l_off[3];
-    bool l_ok[3];
-    int l_pl[3];
-#pragma unroll
-    for (int ps = 0; ps < 3; ++ps) {
-        const int n = lane + 32 * ps;
-        l_ok[ps] = n < 72;
-        const int pl = n / 36, rem = n % 36, dy = rem / 6, dx = rem % 6;
-        l_pl[ps] = pl;
-        l_off[ps] = (3 * pl * TILE + dy) * TILE + dx;  // relative to (p1, ly, lx)
-    }
+    // this lane's nodes (dy, dx) of a particle's plane: node = lane + 32 pass < 36
+    const int n0 = lane, n1 = lane + 32;
+    const int off0 = (n0 / 6) * TILE + n0 % 6, off1 = (n1 / 6) * TILE + n1 % 6;
+    const bool has1 = n1 < 36;
     for (int b = blockIdx.x; b < nbrick; b += gridDim.x) {
         const int r = find_rep(b, nrep, [&](int k) { return reps[k].brick_off; });
         const RepDev &R = reps[r];
@@ -196,17 +188,12 @@ k_assign(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
             for (int k = 0; k < cn; ++k) {
                 const AssignW<T> &w = W[k];
                 if (w.base < 0) continue;  // uniform over the block
-                // the first of this warp's two planes of the particle: lz <= p1 < lz + 3
+                // this warp's plane of the particle: lz <= lz + d < lz + 6
                 const int d = ((warp - w.lz) % A_WARPS + A_WARPS) % A_WARPS;
-                const int first = w.base + d * TILE * TILE;
-#pragma unroll
-                for (int ps = 0; ps < 3; ++ps) {
-                    if (l_ok[ps]) {
-                        const int rem = (lane + 32 * ps) % 36;
-                        const T wgt = w.wz[d + 3 * l_pl[ps]] * w.wy[rem / 6] * w.wx[rem % 6];
-                        tile[first + l_off[ps]] += wgt;
-                    }
-                }
+                T *plane = tile + w.base + d * TILE * TILE;
+                const T wz = w.wz[d];
+                plane[off0] += wz * w.wy[n0 / 6] * w.wx[n0 % 6];
+                if (has1) plane[off1] += wz * w.wy[n1 / 6] * w.wx[n1 % 6];
                 __syncwarp();
             }
         }
@@ -565,6 +552,7 @@ k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
 // its 216 nodes from there; each thread keeps the weights of up to GPT
 // particles across the three components.
 constexpr int G_THREADS = 256;
+template <typename T> constexpr int GNBUF = sizeof(T) == 4 ? 2 : 1;
 
 template <typename T>
 __global__ void __launch_bounds__(G_THREADS)
@@ -603,17 +591,30 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                     weights6<T>((T)oz, wz);
                 }
             }
-            for (int comp = 0; comp < 3; ++comp) {
+            // component tiles through NBUF buffers: with two, the copy of
+            // component c+1 is in flight while component c is summed
+            auto issue = [&](int comp) {
                 const T *E = efield + comp * nmesh + R.mesh_off;
-                __syncthreads();
+                T *dst = tile + (comp % GNBUF<T>) * TILE3;
                 for (int k = threadIdx.x; k < TILE3; k += G_THREADS) {
                     const int tx = k % TILE, ty = (k / TILE) % TILE, tz = k / (TILE * TILE);
                     const int gx = (bx + tx) & (M - 1), gy = (by + ty) & (M - 1),
                               gz = (bz + tz) & (M - 1);
-                    cp_async<sizeof(T)>(tile + k, E + ((long long)gz * M + gy) * M + gx);
+                    cp_async<sizeof(T)>(dst + k, E + ((long long)gz * M + gy) * M + gx);
                 }
-                cp_async_wait_all();
+                asm volatile("cp.async.commit_group;\n" ::: "memory");
+            };
+            __syncthreads();  // the previous chunk / brick is done with the buffers
+            issue(0);
+            for (int comp = 0; comp < 3; ++comp) {
+                if (GNBUF<T> == 2 && comp + 1 < 3) {
+                    issue(comp + 1);
+                    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+                } else {
+                    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                }
                 __syncthreads();
+                const T *tl = tile + (comp % GNBUF<T>) * TILE3;
                 if (base >= 0) {
                     // separable contraction: sum_g wz sum_a wy sum_c wx E
                     T acc = 0;
@@ -622,7 +623,7 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                         T sg = 0;
 #pragma unroll
                         for (int a = 0; a < 6; ++a) {
-                            const T *row = tile + base + (g * TILE + a) * TILE;
+                            const T *row = tl + base + (g * TILE + a) * TILE;
                             T sa = 0;
 #pragma unroll
                             for (int c = 0; c < 6; ++c) sa += wx[c] * row[c];
@@ -631,6 +632,12 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                         acc += wz[g] * sg;
                     }
                     e[comp] = acc;
+                }
+                if (GNBUF<T> == 1 && comp + 1 < 3) {
+                    __syncthreads();
+                    issue(comp + 1);
+                } else if (comp + 2 < 3) {
+                    __syncthreads();  // buffer (comp % 2) is refilled next
                 }
             }
             if (p < p1) {
@@ -748,7 +755,7 @@ template <typename T> void configure_mesh_kernels()
     set_smem(k_fft_y<T>, fft_smem<T>(256, 1));
     set_smem(k_fft_z_green<T>, fft_smem<T>(256, 2));
     set_smem(k_fft_x_c2r<T>, fft_smem<T>(256, 1));
-    set_smem(k_gather<T>, TILE3 * sizeof(T));
+    set_smem(k_gather<T>, GNBUF<T> * TILE3 * sizeof(T));
     set_smem(k_fft_plane<T>, plane_smem<T>(PLANE_MAX));
 }
 
@@ -798,7 +805,7 @@ template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st
 
 template <typename T> void launch_gather(const DevState &s, cudaStream_t st)
 {
-    k_gather<T><<<grid_items(s.nbrick, 148 * 16), G_THREADS, TILE3 * sizeof(T), st>>>(
+    k_gather<T><<<grid_items(s.nbrick, 148 * 16), G_THREADS, GNBUF<T> * TILE3 * sizeof(T), st>>>(
         s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (const T *)s.efield,
         s.nmesh, (typename V4<T>::t *)s.acc_pm, s.nbrick);
 }

@@ -97,9 +97,15 @@ __device__ __forceinline__ long long list_index(int s, int k, int maxnb)
 // ---------------------------------------------------------------------------
 // list build (rebuild steps only)
 // ---------------------------------------------------------------------------
-constexpr int LB_THREADS = 128;
-constexpr int LB_SCAP = 2048;
+constexpr int LB_THREADS = 256;
+constexpr int LB_TPI = 2;  // threads per particle: they scan alternate candidates
+template <typename T> __host__ __device__ constexpr int lb_scap() { return sizeof(T) == 4 ? 3072 : 1536; }
 
+// One CTA per cell. The 27 neighbour cells' coordinates are staged in shared
+// memory; thread `sub` of a particle's pair keeps the in-range candidates
+// with index = sub (mod 2) and writes its t-th one to list slot 2t + sub.
+// The shorter half is padded with the particle's own index, which the force
+// kernel skips (r = 0), so the list order is fixed and needs no merge.
 template <typename T>
 __global__ void __launch_bounds__(LB_THREADS)
 k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
@@ -108,11 +114,14 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
               int *status)
 {
     using Q = typename Coord<T>::Q;
+    constexpr int SCAP = lb_scap<T>();
     extern __shared__ __align__(16) unsigned char lb_smem[];
     Q *stage = reinterpret_cast<Q *>(lb_smem);
     __shared__ int pre[28];
     __shared__ int nstart[27];
     const int tid = threadIdx.x;
+    const int sub = tid % LB_TPI;
+    const int half_cap = maxnb / LB_TPI;
     for (int hc = blockIdx.x; hc < ncell; hc += gridDim.x) {
         const int r = find_rep(hc, nrep, [&](int k) { return reps[k].cell_off; });
         if (!rebuild[r]) continue;  // uniform over the block
@@ -137,15 +146,15 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
         }
         __syncthreads();
         const int total = pre[27];
-        for (int i0 = 0; i0 < nhome; i0 += LB_THREADS) {
-            const int i = i0 + tid;
+        for (int i0 = 0; i0 < nhome; i0 += LB_THREADS / LB_TPI) {
+            const int i = i0 + tid / LB_TPI;
             const bool have = i < nhome;
             const int s = hstart + i;
             Q xi;
             if (have) xi = xq[s];
             int cnt = 0;
-            for (int w0 = 0; w0 < total; w0 += LB_SCAP) {
-                const int wlen = min(LB_SCAP, total - w0);
+            for (int w0 = 0; w0 < total; w0 += SCAP) {
+                const int wlen = min(SCAP, total - w0);
                 __syncthreads();
                 for (int k = tid; k < wlen; k += LB_THREADS) {
                     const int g = w0 + k;
@@ -158,25 +167,30 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                 }
                 __syncthreads();
                 if (have) {
-                    for (int k = 0; k < wlen; ++k) {
+                    for (int k = sub; k < wlen; k += LB_TPI) {
                         const Q q = stage[k];
                         const float dx = (float)qdiff<T>(xi.x, q.x) * sc;
                         const float dy = (float)qdiff<T>(xi.y, q.y) * sc;
                         const float dz = (float)qdiff<T>(xi.z, q.z) * sc;
                         const float r2 = dx * dx + dy * dy + dz * dz;
                         if (r2 < rl2 && (int)q.w != s) {
-                            if (cnt < maxnb) nlist[list_index(s, cnt, maxnb)] = (int)q.w;
+                            if (cnt < half_cap)
+                                nlist[list_index(s, LB_TPI * cnt + sub, maxnb)] = (int)q.w;
                             ++cnt;
                         }
                     }
                 }
             }
+            // pad the shorter half with the particle itself (skipped as r = 0)
+            const int other = __shfl_xor_sync(0xffffffffu, cnt, 1);
+            int m = max(cnt, other);
+            if (m > half_cap) {
+                if (have && sub == 0) raise_status(status, ST_NBOVF);
+                m = half_cap;
+            }
             if (have) {
-                if (cnt > maxnb) {
-                    raise_status(status, ST_NBOVF);
-                    cnt = maxnb;
-                }
-                nnb[s] = cnt;
+                for (int t = cnt; t < m; ++t) nlist[list_index(s, LB_TPI * t + sub, maxnb)] = s;
+                if (sub == 0) nnb[s] = LB_TPI * m;
             }
         }
     }
@@ -358,7 +372,7 @@ template <typename T> void configure_pp_kernels()
 {
     using Q = typename Coord<T>::Q;
     cudaFuncSetAttribute(k_build_lists<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(LB_SCAP * sizeof(Q)));
+                         (int)(lb_scap<T>() * sizeof(Q)));
     const int tab = sizeof(T) == 4 ? (int)(2 * PP_TABLE_N * sizeof(float4)) : 0;
     cudaFuncSetAttribute(k_pp_list<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
     cudaFuncSetAttribute(k_pp_list<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
@@ -376,7 +390,7 @@ template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st
 {
     using Q = typename Coord<T>::Q;
     const int grid = s.ncell < 148 * 16 ? s.ncell : 148 * 16;
-    k_build_lists<T><<<grid, LB_THREADS, LB_SCAP * sizeof(Q), st>>>(
+    k_build_lists<T><<<grid, LB_THREADS, lb_scap<T>() * sizeof(Q), st>>>(
         s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.ncell,
         s.rebuild, s.status);
 }

@@ -89,6 +89,7 @@ SIGNATURES = {
     "p3m_get_energies": (_I, [_V, _D, _I, ctypes.POINTER(_I)]),
     "p3m_get_nqt": (_I, [_V, _I, _D, _I, ctypes.POINTER(_I)]),
     "p3m_check": (_I, [_V]),
+    "p3m_get_replica_stats": (_I, [_V, _I, _D]),
     "p3m_sync": (_I, [_V]),
     "p3m_stream": (_V, [_V]),
     "p3m_set_pp_config": (_I, [_V, _I, ctypes.c_double]),

@@ -224,6 +224,13 @@ class Context:
         o = out[: n.value]
         return o[..., 0] + 1j * o[..., 1]
 
+    def replica_stats(self, replica=0):
+        """{U_short, U_fft, U_self, U, K, T, factor, rebuilds} of one replica."""
+        out = np.zeros(8)
+        self._ck(lib().p3m_get_replica_stats(self.handle, int(replica), dptr(out)))
+        keys = ("U_short", "U_fft", "U_self", "U", "K", "T", "factor", "rebuilds")
+        return dict(zip(keys, (float(x) for x in out)))
+
     def check(self):
         self._ck(lib().p3m_check(self.handle))
 
