@@ -302,6 +302,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
         R.uf = d.uf;
         R.kf = d.kf;
         R.inv_L = 1.0 / d.box;
+        R.qmax = 1.0;
         R.inv_V = 1.0 / (d.box * d.box * d.box);
         R.blk_off = blk;
         R.M = d.mesh;
@@ -604,11 +605,22 @@ static int compat_check(p3m_ctx *ctx, int replica)
     return P3M_OK;
 }
 
+// Charges of a single-replica context (the compat calls); NULL keeps the
+// current ones. The replica's largest |Z| bounds the assignment's fixed point.
 static int upload_charge(p3m_ctx *ctx, const double *Z)
 {
     const int n = ctx->s.ntot;
-    if (Z) return h2d(ctx, ctx->s.charge, Z, sizeof(double) * n);
-    return P3M_OK;
+    if (!Z) return P3M_OK;
+    double qmax = 0.0;
+    for (int i = 0; i < n; ++i) qmax = fmax(qmax, fabs(Z[i]));
+    if (!(qmax < 1e300)) return fail(ctx, P3M_EARG, "charges", "not finite");
+    if (qmax != ctx->rh[0].qmax) {
+        ctx->rh[0].qmax = qmax > 0.0 ? qmax : 1.0;
+        CK(cudaMemcpyAsync(&ctx->s.reps[0].qmax, &ctx->rh[0].qmax, sizeof(double),
+                           cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    return h2d(ctx, ctx->s.charge, Z, sizeof(double) * n);
 }
 
 #define DISPATCH(fn, ...) (ctx->prec == P3M_FP32 ? fn<float>(__VA_ARGS__) : fn<double>(__VA_ARGS__))

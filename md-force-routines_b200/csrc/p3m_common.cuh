@@ -50,6 +50,7 @@ struct RepDev {
     int nq_blk_off;        // offset of this replica's blocks in the n(q,t) kernel
     double L, kappa, alpha, rc, cellw, h, dt, t_desired, af, uf, kf;
     double skin, rcl;      // Verlet skin and list cutoff rc + skin
+    double qmax;           // largest |charge| of the replica
     double inv_cellw, inv_h, inv_L, inv_V;
 };
 

@@ -203,6 +203,89 @@ k_assign(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
     }
 }
 
+// FP32 path: one CTA of 256 threads per brick, thread per particle, the 216
+// contributions added to a shared tile with 32-bit integer atomics -- integer
+// sums do not depend on the order of the adds, so the result is the same on
+// every run. Each contribution q w is scaled by S = 2^k, the largest power of
+// two with 0.17 n |q|max S <= 2^22 for the brick's n particles (0.17 bounds a
+// product of three order-6 weights), so no node sum can exceed 2^22 in
+// magnitude. t = q w S is split exactly into an integer part and a 16-bit
+// fraction with the 1.5 * 2^23 rounding constant (exact for |t| < 2^22, no
+// float <-> int conversions) and the two parts go to two int32 tiles: the node
+// value is (hi + lo / 2^16) / S, resolved to 2^-16 / S.
+constexpr int A32_THREADS = 256;
+constexpr float kRound = 12582912.0f;  // 1.5 * 2^23
+constexpr int kRoundBits = 0x4B400000;
+
+__global__ void __launch_bounds__(A32_THREADS)
+k_assign_i32(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_start,
+             const int *__restrict__ brick_perm, const double *__restrict__ pos,
+             const double *__restrict__ charge, float *__restrict__ tiles, int nbrick)
+{
+    extern __shared__ __align__(16) int a32_smem[];
+    int *thi = a32_smem;
+    int *tlo = a32_smem + TILE3;
+    for (int b = blockIdx.x; b < nbrick; b += gridDim.x) {
+        const int r = find_rep(b, nrep, [&](int k) { return reps[k].brick_off; });
+        const RepDev &R = reps[r];
+        const int nb = R.nb, M = R.M, local = b - R.brick_off;
+        const int bx = (local % nb) * BRICK, by = ((local / nb) % nb) * BRICK,
+                  bz = (local / (nb * nb)) * BRICK;
+        const int p0 = brick_start[b], n = brick_start[b + 1] - p0;
+        // S = 2^k with 0.17 n qmax S <= 2^22
+        const double bound = 0.17 * (double)(n > 0 ? n : 1) * R.qmax;
+        const int kexp = (int)floor(22.0 - log2(bound > 1e-300 ? bound : 1e-300));
+        const float S = ldexpf(1.0f, max(-100, min(kexp, 100)));
+        __syncthreads();
+        for (int k = threadIdx.x; k < TILE3; k += A32_THREADS) {
+            thi[k] = 0;
+            tlo[k] = 0;
+        }
+        __syncthreads();
+        for (int p = p0 + threadIdx.x; p < p0 + n; p += A32_THREADS) {
+            const int i = brick_perm[p];
+            double ox, oy, oz;
+            const int ix = base_offset(pos[3 * i + 0], R.h, ox);
+            const int iy = base_offset(pos[3 * i + 1], R.h, oy);
+            const int iz = base_offset(pos[3 * i + 2], R.h, oz);
+            const int lx = wrapM(ix, M) - bx, ly = wrapM(iy, M) - by, lz = wrapM(iz, M) - bz;
+            // a particle outside [-L, 2L) was filed under brick 0 and flagged
+            if ((unsigned)lx >= (unsigned)BRICK || (unsigned)ly >= (unsigned)BRICK ||
+                (unsigned)lz >= (unsigned)BRICK)
+                continue;
+            float wx[6], wy[6], wz[6];
+            weights6<float>((float)ox, wx);
+            weights6<float>((float)oy, wy);
+            weights6<float>((float)oz, wz);
+            const float qs = (float)charge[i] * S;
+            const int base = (lz * TILE + ly) * TILE + lx;
+#pragma unroll
+            for (int g = 0; g < 6; ++g) {
+#pragma unroll
+                for (int a = 0; a < 6; ++a) {
+                    const float qzy = qs * wz[g] * wy[a];
+                    const int row = base + (g * TILE + a) * TILE;
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) {
+                        const float t = qzy * wx[c];
+                        const float hb = (t - 0.5f) + kRound;       // floor(t), as a float
+                        const int hi = __float_as_int(hb) - kRoundBits;
+                        const float frac = t - (hb - kRound);         // in [0, 1], exact
+                        const int lo = __float_as_int(frac * 65536.0f + kRound) - kRoundBits;
+                        atomicAdd(thi + row + c, hi);
+                        atomicAdd(tlo + row + c, lo);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        float *dst = tiles + R.tile_off + (long long)local * TILE3;
+        const double inv = 1.0 / (double)S;
+        for (int k = threadIdx.x; k < TILE3; k += A32_THREADS)
+            dst[k] = (float)(((double)thi[k] + (double)tlo[k] * (1.0 / 65536.0)) * inv);
+    }
+}
+
 // Charge on node (x,y,z) of replica R: the sum of the (up to 8) brick tiles
 // that cover it, in a fixed order (dz, dy, dx), with all loads independent.
 template <typename T>
@@ -553,6 +636,12 @@ k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
 // particles across the three components.
 constexpr int G_THREADS = 256;
 template <typename T> constexpr int GNBUF = sizeof(T) == 4 ? 2 : 1;
+// Gather tiles keep rows of GTX nodes (TILE padded up) so each row is filled
+// with 16-byte copies: a brick starts on a multiple of 16 nodes and M is a
+// multiple of 16, so every 16-byte chunk -- wrapped ones included -- is
+// aligned in global and shared memory.
+constexpr int GTX = 24;
+constexpr int GTILE = TILE * TILE * GTX;
 
 template <typename T>
 __global__ void __launch_bounds__(G_THREADS)
@@ -585,7 +674,7 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                 // (a particle outside [-L, 2L) was flagged by the key pass)
                 if ((unsigned)lx < (unsigned)BRICK && (unsigned)ly < (unsigned)BRICK &&
                     (unsigned)lz < (unsigned)BRICK) {
-                    base = (lz * TILE + ly) * TILE + lx;
+                    base = (lz * TILE + ly) * GTX + lx;
                     weights6<T>((T)ox, wx);
                     weights6<T>((T)oy, wy);
                     weights6<T>((T)oz, wz);
@@ -594,13 +683,16 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
             // component tiles through NBUF buffers: with two, the copy of
             // component c+1 is in flight while component c is summed
             auto issue = [&](int comp) {
+                constexpr int EPC = 16 / sizeof(T);   // elements per 16-byte chunk
+                constexpr int CPR = GTX / EPC;        // chunks per tile row
                 const T *E = efield + comp * nmesh + R.mesh_off;
-                T *dst = tile + (comp % GNBUF<T>) * TILE3;
-                for (int k = threadIdx.x; k < TILE3; k += G_THREADS) {
-                    const int tx = k % TILE, ty = (k / TILE) % TILE, tz = k / (TILE * TILE);
-                    const int gx = (bx + tx) & (M - 1), gy = (by + ty) & (M - 1),
+                T *dst = tile + (comp % GNBUF<T>) * GTILE;
+                for (int k = threadIdx.x; k < TILE * TILE * CPR; k += G_THREADS) {
+                    const int ch = k % CPR, row = k / CPR;
+                    const int ty = row % TILE, tz = row / TILE;
+                    const int gx = (bx + ch * EPC) & (M - 1), gy = (by + ty) & (M - 1),
                               gz = (bz + tz) & (M - 1);
-                    cp_async<sizeof(T)>(dst + k, E + ((long long)gz * M + gy) * M + gx);
+                    cp_async16(dst + row * GTX + ch * EPC, E + ((long long)gz * M + gy) * M + gx);
                 }
                 asm volatile("cp.async.commit_group;\n" ::: "memory");
             };
@@ -614,7 +706,7 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
                 }
                 __syncthreads();
-                const T *tl = tile + (comp % GNBUF<T>) * TILE3;
+                const T *tl = tile + (comp % GNBUF<T>) * GTILE;
                 if (base >= 0) {
                     // separable contraction: sum_g wz sum_a wy sum_c wx E
                     T acc = 0;
@@ -623,7 +715,7 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                         T sg = 0;
 #pragma unroll
                         for (int a = 0; a < 6; ++a) {
-                            const T *row = tl + base + (g * TILE + a) * TILE;
+                            const T *row = tl + base + (g * TILE + a) * GTX;
                             T sa = 0;
 #pragma unroll
                             for (int c = 0; c < 6; ++c) sa += wx[c] * row[c];
@@ -751,16 +843,23 @@ static int grid_items(int n, int cap = 148 * 8) { return n < cap ? (n > 0 ? n : 
 template <typename T> void configure_mesh_kernels()
 {
     set_smem(k_assign<T>, assign_smem<T>());
+    set_smem(k_assign_i32, 2 * TILE3 * sizeof(int));
     set_smem(k_fft_x_r2c<T>, fft_smem<T>(256, 1));
     set_smem(k_fft_y<T>, fft_smem<T>(256, 1));
     set_smem(k_fft_z_green<T>, fft_smem<T>(256, 2));
     set_smem(k_fft_x_c2r<T>, fft_smem<T>(256, 1));
-    set_smem(k_gather<T>, GNBUF<T> * TILE3 * sizeof(T));
+    set_smem(k_gather<T>, GNBUF<T> * GTILE * sizeof(T));
     set_smem(k_fft_plane<T>, plane_smem<T>(PLANE_MAX));
 }
 
 template <typename T> void launch_assign(const DevState &s, cudaStream_t st)
 {
+    if (sizeof(T) == 4) {
+        k_assign_i32<<<grid_items(s.nbrick, 148 * 16), A32_THREADS, 2 * TILE3 * sizeof(int), st>>>(
+            s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (float *)s.tiles,
+            s.nbrick);
+        return;
+    }
     const size_t smem = assign_smem<T>();
     k_assign<T><<<grid_items(s.nbrick, 148 * 16), A_THREADS, smem, st>>>(
         s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (T *)s.tiles, s.nbrick,
@@ -805,7 +904,7 @@ template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st
 
 template <typename T> void launch_gather(const DevState &s, cudaStream_t st)
 {
-    k_gather<T><<<grid_items(s.nbrick, 148 * 16), G_THREADS, GNBUF<T> * TILE3 * sizeof(T), st>>>(
+    k_gather<T><<<grid_items(s.nbrick, 148 * 16), G_THREADS, GNBUF<T> * GTILE * sizeof(T), st>>>(
         s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (const T *)s.efield,
         s.nmesh, (typename V4<T>::t *)s.acc_pm, s.nbrick);
 }
