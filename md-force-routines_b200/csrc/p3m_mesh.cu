@@ -28,9 +28,9 @@
 // Overlapping tile halos are summed in a fixed order when the first FFT pass
 // reads the mesh.
 //
-// The FFT is an in-place radix-2 decimation-in-time transform of 16 lines
-// at a time held in shared memory ([element][line], line stride padded to
-// 17), the input permuted to bit-reversed order as it is loaded. Twiddles
+// The FFT is an in-place radix-2 decimation-in-time transform of lines held
+// in shared memory (padded strides), with up to three stages per register
+// pass, the input permuted to bit-reversed order as it is loaded. Twiddles
 // exp(-2 pi i k/256) come from an FP64-accurate table.
 #include "p3m_kernels.h"
 
@@ -52,29 +52,63 @@ __device__ __forceinline__ void load_twiddles(cplx<T> *tw, const cplx<T> *g)
     for (int k = threadIdx.x; k < 128; k += blockDim.x) tw[k] = g[k];
 }
 
-// In-place DIT FFT of PENCIL lines of length 2^logM: element n of line l at
-// buf[n * LS + l], input in bit-reversed order, output in natural order.
-// Unnormalised; inverse uses conjugate twiddles. Ends with a barrier.
-template <typename T>
-__device__ void fft_pencil(cplx<T> *buf, int logM, const cplx<T> *tw, bool inverse)
+// In-place radix-2 decimation-in-time FFT of `nlines` lines of length 2^logM
+// held in shared memory, element n of line l at buf[l * ls + n * es]; input
+// in bit-reversed order, output natural; unnormalised, the inverse uses
+// conjugate twiddles. Up to three consecutive radix-2 stages are done in
+// registers on groups of 8 (4, 2) elements, so the data passes through shared
+// memory -- and the block through a barrier -- once per three stages. Thread
+// b takes line b % nlines, so consecutive threads touch consecutive lines.
+// Ends with a barrier.
+template <typename T, int LOGR>
+__device__ __forceinline__ void fft_group_pass(cplx<T> *buf, int logM, int ls, int es, int nlines,
+                                               const cplx<T> *tw, bool inverse, int s)
 {
-    const int M = 1 << logM;
-    const int nb = PENCIL * (M >> 1);
-    for (int s = 0; s < logM; ++s) {
-        const int half = 1 << s;
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-            const int l = b & (PENCIL - 1), j = b >> 4;
-            const int k = j & (half - 1);
-            const int i0 = ((j >> s) << (s + 1)) + k, i1 = i0 + half;
-            cplx<T> w = tw[k << (7 - s)];
-            if (inverse) w.y = -w.y;
-            cplx<T> a = buf[i0 * LS + l], c = buf[i1 * LS + l];
-            cplx<T> t = cmul<T>(w, c);
-            buf[i0 * LS + l] = make_c<T>(a.x + t.x, a.y + t.y);
-            buf[i1 * LS + l] = make_c<T>(a.x - t.x, a.y - t.y);
+    constexpr int R = 1 << LOGR;
+    const int half = 1 << s;           // distance of the first stage's pairs
+    const int ngroups = nlines * ((1 << logM) >> LOGR);
+    for (int b = threadIdx.x; b < ngroups; b += blockDim.x) {
+        const int l = b % nlines, g = b / nlines;
+        const int k = g & (half - 1), blk = g >> s;
+        const int base = (blk << (s + LOGR)) + k;
+        cplx<T> x[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) x[r] = buf[l * ls + (base + r * half) * es];
+#pragma unroll
+        for (int t = 0; t < LOGR; ++t) {
+            // stage s + t: pairs (r, r + 2^t); twiddle W_{2^(s+t+1)}^{k + (r mod 2^t) half}
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (r & (1 << t)) continue;
+                const int e = k + (r & ((1 << t) - 1)) * half;
+                cplx<T> w = tw[e << (7 - (s + t))];
+                if (inverse) w.y = -w.y;
+                const cplx<T> a = x[r], c = cmul<T>(w, x[r + (1 << t)]);
+                x[r] = make_c<T>(a.x + c.x, a.y + c.y);
+                x[r + (1 << t)] = make_c<T>(a.x - c.x, a.y - c.y);
+            }
         }
-        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[l * ls + (base + r * half) * es] = x[r];
     }
+    __syncthreads();
+}
+
+template <typename T>
+__device__ void fft_lines(cplx<T> *buf, int logM, int ls, int es, int nlines, const cplx<T> *tw,
+                          bool inverse)
+{
+    int s = 0;
+    for (; s + 3 <= logM; s += 3) fft_group_pass<T, 3>(buf, logM, ls, es, nlines, tw, inverse, s);
+    if (logM - s == 2) fft_group_pass<T, 2>(buf, logM, ls, es, nlines, tw, inverse, s);
+    else if (logM - s == 1) fft_group_pass<T, 1>(buf, logM, ls, es, nlines, tw, inverse, s);
+}
+
+// PENCIL lines, element n of line l at buf[n * LS + l]
+template <typename T>
+__device__ __forceinline__ void fft_pencil(cplx<T> *buf, int logM, const cplx<T> *tw, bool inverse)
+{
+    fft_lines<T>(buf, logM, 1, LS, PENCIL, tw, inverse);
 }
 
 // ---------------------------------------------------------------------------
@@ -475,30 +509,6 @@ k_fft_z_green(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restri
 constexpr int PLANE_MAX = 64;
 
 template <typename T>
-__device__ void fft_plane_lines(cplx<T> *buf, int logM, int ls, int es, const cplx<T> *tw,
-                                bool inverse)
-{
-    const int M = 1 << logM;
-    const int nb = M * (M >> 1);
-    for (int s = 0; s < logM; ++s) {
-        const int half = 1 << s;
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-            const int l = b & (M - 1), j = b >> logM;
-            const int k = j & (half - 1);
-            const int i0 = ((j >> s) << (s + 1)) + k, i1 = i0 + half;
-            cplx<T> w = tw[k << (7 - s)];
-            if (inverse) w.y = -w.y;
-            cplx<T> *p0 = buf + l * ls + i0 * es, *p1 = buf + l * ls + i1 * es;
-            const cplx<T> a = *p0, c = *p1;
-            const cplx<T> t = cmul<T>(w, c);
-            *p0 = make_c<T>(a.x + t.x, a.y + t.y);
-            *p1 = make_c<T>(a.x - t.x, a.y - t.y);
-        }
-        __syncthreads();
-    }
-}
-
-template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS)
 k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict__ spec,
             const T *__restrict__ green, cplx<T> *__restrict__ ek, long long nspec,
@@ -523,8 +533,8 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
             A[brev(z, logM) * LD + brev(y, logM)] = spec[lbase + e];
         }
         __syncthreads();
-        fft_plane_lines<T>(A, logM, LD, 1, tw, false);  // along y
-        fft_plane_lines<T>(A, logM, 1, LD, tw, false);  // along z
+        fft_lines<T>(A, logM, LD, 1, M, tw, false);  // along y
+        fft_lines<T>(A, logM, 1, LD, M, tw, false);  // along z
         const double wkx = (kx == 0 || kx == (M >> 1)) ? 1.0 : 2.0;
         double u = 0.0;
         for (int e = threadIdx.x; e < MM; e += blockDim.x) {
@@ -544,9 +554,9 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
             A[zb * LD + yb] = make_c<T>(kz * ph.y, -kz * ph.x);  // -i kz phi
         }
         __syncthreads();
-        fft_plane_lines<T>(A, logM, 1, LD, tw, true);  // z, of -i kz phi
-        fft_plane_lines<T>(B, logM, 1, LD, tw, true);  // z, of phi: psi
-        fft_plane_lines<T>(A, logM, LD, 1, tw, true);  // y: E_z
+        fft_lines<T>(A, logM, 1, LD, M, tw, true);  // z, of -i kz phi
+        fft_lines<T>(B, logM, 1, LD, M, tw, true);  // z, of phi: psi
+        fft_lines<T>(A, logM, LD, 1, M, tw, true);  // y: E_z
         cplx<T> *Ez = ek + 2 * nspec + lbase;
         for (int e = threadIdx.x; e < MM; e += blockDim.x) {
             const int z = e >> logM, y = e & (M - 1);
@@ -561,8 +571,8 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
             A[z * LD + yb] = make_c<T>(ky * ps.y, -ky * ps.x);  // -i ky psi
         }
         __syncthreads();
-        fft_plane_lines<T>(A, logM, LD, 1, tw, true);  // y: E_y
-        fft_plane_lines<T>(B, logM, LD, 1, tw, true);  // y: IFFT(psi)
+        fft_lines<T>(A, logM, LD, 1, M, tw, true);  // y: E_y
+        fft_lines<T>(B, logM, LD, 1, M, tw, true);  // y: IFFT(psi)
         const T kxv = (kx == (M >> 1)) ? (T)0 : twopi_L * (T)kx;
         cplx<T> *Ey = ek + nspec + lbase;
         cplx<T> *Ex = ek + lbase;
