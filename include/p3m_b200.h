@@ -147,6 +147,20 @@ int p3m_vscale(p3m_ctx *ctx, int replica, int it, double *pos, double *vel, doub
 int p3m_nqt(p3m_ctx *ctx, int replica, const double *pos, const double *qv, int nq,
             double *out);
 
+/* s_of_q_w.py:3 n_of_q_w(n_q_t, N, dt, T): S(q,w) of one run, per axis.
+ * nqt (nt,3) complex128 as interleaved (re,im) in; out (nt,3) =
+ * |dt FFT_t n|^2 / (N T). nt: a power of two <= 2^21, or any length <= 2^20
+ * (Bluestein). Context-free: runs on `device`. */
+int p3m_sqw_series(int device, const double *nqt, int nt, double N, double dt, double T,
+                   double *out);
+
+/* s_of_q_w_avg.py:5 s_of_q_w_avg_mat(n_q_t_array, Nq, sqw_mat, N_avg, N, dt, T):
+ * nqt (nrun, nt, nq, 3) complex128 (the stacked n_q_t_<id>.npy files); out
+ * (nrun, ncols, nt) = the mean over axes of n_of_q_w on q columns
+ * col0 + i*col_stride (the reference: col0 0, col_stride 3, ncols Nq). */
+int p3m_sqw_runs(int device, const double *nqt, int nrun, int nt, int nq, int col0, int col_stride,
+                 int ncols, double N, double dt, double T, double *out);
+
 /* ---- device-resident ("fast") path over all replicas ----------------------- */
 
 /* Copy state in/out. Any of the pointers may be NULL. Arrays are (n,3). */
@@ -169,6 +183,17 @@ int p3m_set_nqt(p3m_ctx *ctx, const double *qmult, int nq, int capacity);
  * in a CUDA graph on first use and replay it. sync: wait for completion. */
 int p3m_run(p3m_ctx *ctx, int n_steps, int mode, int it0, int record_nqt, int use_graph,
             int sync);
+
+/* S(q,w) of the last nt recorded n(q,t) rows (s_of_q_w.py:3-20,
+ * s_of_q_w_avg.py:5-20, and the mean over runs of s_of_q_w_script.py:37):
+ * for the q columns col0 + i*col_stride (i < ncols) -- the reference uses
+ * every third column, its integer multiples of 2 pi/L -- the time FFT of each
+ * axis, |dt X|^2 / (N_r T) with T = nt dt, averaged over the three axes.
+ * out (ncols, nt): the mean over replicas (may be NULL); out_rep (R, ncols,
+ * nt): per replica (may be NULL). nt as for p3m_sqw_series and at most the
+ * ring capacity. */
+int p3m_sqw(p3m_ctx *ctx, double dt, int col0, int col_stride, int ncols, int nt, double *out,
+            double *out_rep);
 
 /* Per-step energies recorded by p3m_run, (steps, R, 4) doubles:
  * U, K, T (before any rescale), and the thermostat factor applied. Returns

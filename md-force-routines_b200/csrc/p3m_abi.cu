@@ -1,6 +1,7 @@
 // C ABI of libp3m_b200: contexts, device buffers, the compat entry points that
 // mirror the reference's Python functions, and the device-resident stepper.
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -546,16 +547,18 @@ template <typename T> static void seq_step(p3m_ctx *ctx, int mode, int record_nq
     seq_pp<T>(ctx);
     if (s.has_mesh) seq_pm<T>(ctx);
     launch_kick_finish<T>(s, 1, nullptr, ctx->st);
-    launch_step_reduce(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, ctx->st);
-    ctx->launches += 2;
-    if (mode == P3M_MODE_THERMOSTAT) {
-        launch_scale_vel(s, ctx->st);
-        ctx->launches++;
-    }
-    if (record_nqt && ctx->nq > 0) {
+    ctx->launches++;
+    const int rec = (record_nqt && ctx->nq > 0) ? 1 : 0;
+    if (rec) {  // positions of this step are final: row counters[3] of the ring
         launch_nqt<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nq_consecutive, ctx->nqt_part,
                       ctx->nqt_ring, ctx->counters, ctx->nqt_cap, ctx->st);
         ctx->launches += 2;
+    }
+    launch_step_reduce(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, ctx->st, rec);
+    ctx->launches++;
+    if (mode == P3M_MODE_THERMOSTAT) {
+        launch_scale_vel(s, ctx->st);
+        ctx->launches++;
     }
 }
 
@@ -1082,12 +1085,12 @@ extern "C" int p3m_get_nqt(p3m_ctx *ctx, int replica, double *out, int max_steps
     CK(cudaStreamSynchronize(ctx->st));
     int pos[4];
     CK(cudaMemcpy(pos, ctx->counters, sizeof pos, cudaMemcpyDeviceToHost));
-    const int total = ctx->nqt_rows < pos[1] ? ctx->nqt_rows : pos[1];
+    const int total = pos[3];  // rows recorded since p3m_set_nqt
     int n = total < ctx->nqt_cap ? total : ctx->nqt_cap;
     if (n > max_steps) n = max_steps;
     const size_t rowlen = (size_t)ctx->nq * 6;
     for (int k = 0; k < n; ++k) {
-        const int step = pos[1] - n + k;
+        const int step = total - n + k;
         const double *src = ctx->nqt_ring + ((size_t)(step % ctx->nqt_cap) * ctx->nrep + replica) * rowlen;
         CK(cudaMemcpy(out + (size_t)k * rowlen, src, sizeof(double) * rowlen, cudaMemcpyDeviceToHost));
     }
@@ -1298,4 +1301,230 @@ extern "C" int p3m_fp32_peak(int device, double *tflops)
     if (t <= 0) return fail(nullptr, P3M_ECUDA, "p3m_fp32_peak", "probe kernel failed");
     *tflops = t;
     return P3M_OK;
+}
+
+// ---------------------------------------------------------------------------
+// S(q, omega)
+// ---------------------------------------------------------------------------
+
+static int ilog2_ceil(int n)
+{
+    int l = 0;
+    while ((1 << l) < n) ++l;
+    return l;
+}
+
+// Chirp spectrum for Bluestein's transform of length nt with FFT length P,
+// in bit-reversed order (host, FP64).
+static void chirp_spectrum_br(int nt, int logP, std::vector<double2> &out)
+{
+    const int P = 1 << logP;
+    std::vector<std::complex<long double>> b(P, 0.0L);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int m = 0; m < nt; ++m) {
+        const long long q = ((long long)m * m) % (2LL * nt);
+        const std::complex<long double> c = std::polar(1.0L, pi * (long double)q / nt);
+        b[m] = c;
+        if (m > 0) b[P - m] = c;
+    }
+    // plain O(P log P) radix-2 DIT on the host (bit-reversed input)
+    std::vector<std::complex<long double>> x(P);
+    for (int n = 0; n < P; ++n) {
+        int r = 0;
+        for (int k = 0; k < logP; ++k) r |= ((n >> k) & 1) << (logP - 1 - k);
+        x[r] = b[n];
+    }
+    for (int s = 1; s <= logP; ++s) {
+        const int m = 1 << s, h = m >> 1;
+        for (int k = 0; k < h; ++k) {
+            const std::complex<long double> w = std::polar(1.0L, -2.0L * pi * k / m);
+            for (int j = k; j < P; j += m) {
+                const std::complex<long double> t = w * x[j + h];
+                x[j + h] = x[j] - t;
+                x[j] = x[j] + t;
+            }
+        }
+    }
+    out.resize(P);
+    for (int j = 0; j < P; ++j) {
+        int r = 0;
+        for (int k = 0; k < logP; ++k) r |= ((j >> k) & 1) << (logP - 1 - k);
+        out[j] = make_double2((double)x[r].real(), (double)x[r].imag());
+    }
+}
+
+static int plan_sqw(int nt, int *logP, int *bluestein)
+{
+    const bool pow2 = nt > 0 && (nt & (nt - 1)) == 0;
+    *bluestein = pow2 ? 0 : 1;
+    *logP = pow2 ? ilog2_ceil(nt) : ilog2_ceil(2 * nt - 1);
+    return (1 << *logP) <= sqw_max_points() ? P3M_OK : P3M_EARG;
+}
+
+static const char *kSqwLenMsg = "nt must be a power of two <= 2^21 or any length <= 2^20";
+
+// Runs k_sqw over replicas 0..nrep-1 of the series described by `a` (src,
+// strides, ring position, columns and nt set by the caller) on stream st:
+// uploads the chirp spectrum and the particle counts, takes a global-memory
+// transform scratch for lengths beyond shared memory (replicas in chunks of
+// at most 1 GiB of scratch), and copies out_rep (nrep * ncols * nt [* 3])
+// and, when `out` is not NULL, the mean over replicas to the host.
+static cudaError_t sqw_device(SqwArgs a, int nrep, const double *n_per_rep, cudaStream_t st,
+                              double *host_out_rep, double *host_out, long long *launches)
+{
+    std::vector<double2> chirp;
+    if (a.bluestein) chirp_spectrum_br(a.nt, a.logP, chirp);
+    const size_t P = (size_t)1 << a.logP;
+    const size_t per_rep = (size_t)a.ncols * a.nt * (a.per_axis ? 3 : 1);
+    int chunk = nrep;
+    if ((int)P > sqw_smem_points()) {
+        const size_t per = (size_t)a.ncols * P * sizeof(double2);
+        chunk = (int)std::max<size_t>(1, std::min<size_t>(nrep, ((size_t)1 << 30) / per));
+    }
+    double *d_rep = nullptr, *d_out = nullptr, *d_n = nullptr;
+    double2 *d_chirp = nullptr, *d_scr = nullptr;
+    cudaError_t e = cudaMalloc(&d_rep, (size_t)nrep * per_rep * sizeof(double));
+    if (e == cudaSuccess && host_out) e = cudaMalloc(&d_out, per_rep * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_n, (size_t)nrep * sizeof(double));
+    if (e == cudaSuccess && a.bluestein) e = cudaMalloc(&d_chirp, P * sizeof(double2));
+    if (e == cudaSuccess && (int)P > sqw_smem_points())
+        e = cudaMalloc(&d_scr, (size_t)chunk * a.ncols * P * sizeof(double2));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_n, n_per_rep, (size_t)nrep * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && a.bluestein)
+        e = cudaMemcpyAsync(d_chirp, chirp.data(), P * sizeof(double2), cudaMemcpyHostToDevice, st);
+    a.chirp_fft_br = d_chirp;
+    a.nrep_n = d_n;
+    a.out_rep = d_rep;
+    for (int r0 = 0; e == cudaSuccess && r0 < nrep; r0 += chunk) {
+        a.r0 = r0;
+        a.nrep_launch = std::min(chunk, nrep - r0);
+        launch_sqw(a, d_scr, st);
+        ++*launches;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && host_out) {
+        launch_sqw_mean(d_rep, nrep, (long long)per_rep, d_out, st);
+        ++*launches;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && host_out)
+        e = cudaMemcpy(host_out, d_out, per_rep * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && host_out_rep)
+        e = cudaMemcpy(host_out_rep, d_rep, (size_t)nrep * per_rep * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d_rep);
+    cudaFree(d_out);
+    cudaFree(d_n);
+    cudaFree(d_chirp);
+    cudaFree(d_scr);
+    return e;
+}
+
+extern "C" int p3m_sqw(p3m_ctx *ctx, double dt, int col0, int col_stride, int ncols, int nt,
+                       double *out, double *out_rep)
+{
+    if (!ctx || (!out && !out_rep)) return fail(ctx, P3M_EARG, "p3m_sqw", "NULL argument");
+    if (ctx->nq == 0) return fail(ctx, P3M_EARG, "p3m_sqw", "n(q,t) not configured");
+    if (ncols <= 0 || col0 < 0 || col_stride < 1 || col0 + (long long)(ncols - 1) * col_stride >= ctx->nq)
+        return fail(ctx, P3M_EARG, "p3m_sqw", "q columns out of range");
+    if (!(dt > 0)) return fail(ctx, P3M_EARG, "p3m_sqw", "dt must be > 0");
+    SqwArgs a{};
+    if (nt < 2 || plan_sqw(nt, &a.logP, &a.bluestein) != P3M_OK)
+        return fail(ctx, P3M_EARG, "p3m_sqw", kSqwLenMsg);
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    int pos[4];
+    CK(cudaMemcpy(pos, ctx->counters, sizeof pos, cudaMemcpyDeviceToHost));
+    const int total = pos[3];
+    if (total < nt || nt > ctx->nqt_cap)
+        return fail(ctx, P3M_EARG, "p3m_sqw", "fewer recorded n(q,t) rows than nt");
+    std::vector<double> nr(ctx->nrep);
+    for (int r = 0; r < ctx->nrep; ++r) nr[r] = ctx->desc[r].n;
+    a.src = (const double2 *)ctx->nqt_ring;
+    a.row_stride = (long long)ctx->nrep * ctx->nq * 3;
+    a.rep_stride = (long long)ctx->nq * 3;
+    a.cap = ctx->nqt_cap;
+    a.row0 = (total - nt) % ctx->nqt_cap;
+    a.col0 = col0;
+    a.col_stride = col_stride;
+    a.ncols = ncols;
+    a.nt = nt;
+    a.dt = dt;
+    a.per_axis = 0;
+    std::vector<double> rep;
+    double *host_rep = out_rep;
+    if (!host_rep) {
+        rep.resize((size_t)ctx->nrep * ncols * nt);
+        host_rep = rep.data();
+    }
+    long long nl = 0;
+    cudaError_t e = sqw_device(a, ctx->nrep, nr.data(), ctx->st, host_rep, out, &nl);
+    ctx->launches += nl;
+    if (e != cudaSuccess) return fail(ctx, P3M_ECUDA, "p3m_sqw", cudaGetErrorString(e));
+    return P3M_OK;
+}
+
+// Series held on the host as complex128 (re, im pairs): uploads them and runs
+// sqw_device on the legacy default stream; then rescales from T = nt dt to
+// the caller's T.
+static int sqw_host(const char *who, int device, const double *src, int nrun, int nt, int nq,
+                    int col0, int col_stride, int ncols, double N, double dt, double T, int per_axis,
+                    double *out_rep)
+{
+    SqwArgs a{};
+    if (nt < 2 || plan_sqw(nt, &a.logP, &a.bluestein) != P3M_OK)
+        return fail(nullptr, P3M_EARG, who, kSqwLenMsg);
+    int rc = check_device(nullptr, device);
+    if (rc != P3M_OK) return rc;
+    const size_t n_src = (size_t)nrun * nt * nq * 3;
+    double2 *d_src = nullptr;
+    cudaError_t e = cudaMalloc(&d_src, n_src * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMemcpy(d_src, src, n_src * sizeof(double2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        a.src = d_src;
+        a.row_stride = (long long)nq * 3;
+        a.rep_stride = (long long)nt * nq * 3;
+        a.cap = nt;
+        a.row0 = 0;
+        a.col0 = col0;
+        a.col_stride = col_stride;
+        a.ncols = ncols;
+        a.nt = nt;
+        a.dt = dt;
+        a.per_axis = per_axis;
+        std::vector<double> nr(nrun, N);
+        long long nl = 0;
+        e = sqw_device(a, nrun, nr.data(), 0, out_rep, nullptr, &nl);
+    }
+    cudaFree(d_src);
+    if (e != cudaSuccess) return fail(nullptr, P3M_ECUDA, who, cudaGetErrorString(e));
+    const double f = (nt * dt) / T;
+    const size_t n_out = (size_t)nrun * ncols * nt * (per_axis ? 3 : 1);
+    for (size_t i = 0; i < n_out; ++i) out_rep[i] *= f;
+    return P3M_OK;
+}
+
+extern "C" int p3m_sqw_series(int device, const double *nqt, int nt, double N, double dt, double T,
+                              double *out)
+{
+    if (!nqt || !out || !(N > 0) || !(T > 0) || !(dt > 0))
+        return fail(nullptr, P3M_EARG, "p3m_sqw_series", "bad argument");
+    std::vector<double> o((size_t)3 * (nt > 0 ? nt : 0));
+    const int rc = sqw_host("p3m_sqw_series", device, nqt, 1, nt, 1, 0, 1, 1, N, dt, T, 1, o.data());
+    if (rc != P3M_OK) return rc;
+    for (int k = 0; k < nt; ++k)
+        for (int ax = 0; ax < 3; ++ax) out[3 * (size_t)k + ax] = o[(size_t)ax * nt + k];
+    return P3M_OK;
+}
+
+extern "C" int p3m_sqw_runs(int device, const double *nqt, int nrun, int nt, int nq, int col0,
+                            int col_stride, int ncols, double N, double dt, double T, double *out)
+{
+    if (!nqt || !out || nrun < 1 || nq < 1 || !(N > 0) || !(T > 0) || !(dt > 0))
+        return fail(nullptr, P3M_EARG, "p3m_sqw_runs", "bad argument");
+    if (ncols <= 0 || col0 < 0 || col_stride < 1 || col0 + (long long)(ncols - 1) * col_stride >= nq)
+        return fail(nullptr, P3M_EARG, "p3m_sqw_runs", "q columns out of range");
+    return sqw_host("p3m_sqw_runs", device, nqt, nrun, nt, nq, col0, col_stride, ncols, N, dt, T, 0,
+                    out);
 }

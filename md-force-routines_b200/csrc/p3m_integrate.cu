@@ -126,10 +126,11 @@ k_kick_finish(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
 __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nblk,
                               const double *__restrict__ kin_part, double *__restrict__ rep_out,
                               int mode, int *__restrict__ counters, double *__restrict__ ring,
-                              int ring_cap, int *rebuild, int *status)
+                              int ring_cap, int recorded, int *rebuild, int *status)
 {
-    // counters: [0] steps since the run started, [1] ring position, [2] step
-    // index of the run's first step (thermostat_p3m_ord6.py:15 tests it<=1999)
+    // counters: [0] steps since the run started, [1] energy-ring position,
+    // [2] step index of the run's first step (thermostat_p3m_ord6.py:15 tests
+    // it <= 1999), [3] n(q,t) rows recorded
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int it = counters[2] + counters[0];
     const int step = counters[1];
@@ -171,6 +172,7 @@ __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nbl
         if (mode != 2) {
             counters[0] += 1;
             counters[1] = step + 1;
+            if (recorded) counters[3] += 1;
         }
     }
     // this step's lists are built (count them); the next drift decides again
@@ -188,7 +190,10 @@ __global__ void k_set_flags(int *flag, int n, int value)
 __global__ void k_set_counters(int *counters, int run_step, int ring_pos, int it0)
 {
     if (run_step >= 0) counters[0] = run_step;
-    if (ring_pos >= 0) counters[1] = ring_pos;
+    if (ring_pos >= 0) {
+        counters[1] = ring_pos;
+        counters[3] = ring_pos;
+    }
     counters[2] = it0;
 }
 
@@ -356,8 +361,8 @@ __global__ void k_nqt_reduce(const RepDev *__restrict__ reps, int nrep, int nblk
     const int b0 = R.nq_blk_off, b1 = (r + 1 < nrep) ? reps[r + 1].nq_blk_off : nblk;
     double *o = out;
     if (counters) {
-        // ring layout [step][replica][nq][3][2]; the step was already advanced
-        const int step = (counters[1] - 1 + ring_cap) % ring_cap;
+        // ring layout [row][replica][nq][3][2]; this step's row
+        const int step = counters[3] % ring_cap;
         o = out + (long long)step * nrep * nq * 6;
     }
     for (int k = threadIdx.x; k < nq * 6; k += blockDim.x) {
@@ -456,10 +461,10 @@ void launch_kick_finish(const DevState &s, int do_kick, double *ep_out, cudaStre
 }
 
 void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring, int ring_cap,
-                        cudaStream_t st)
+                        cudaStream_t st, int recorded)
 {
     k_step_reduce<<<1, 1024, 0, st>>>(s.reps, s.nrep, s.nblk, s.kin_part, s.rep_out, mode,
-                                      counters, ring, ring_cap, s.rebuild, s.status);
+                                      counters, ring, ring_cap, recorded, s.rebuild, s.status);
 }
 
 void launch_set_counters(int *counters, int run_step, int ring_pos, int it0, cudaStream_t st)

@@ -99,7 +99,7 @@ void launch_kick_drift(const DevState &s, cudaStream_t st);
 template <typename T> void launch_kick_finish(const DevState &s, int do_kick, double *ep_out,
                                               cudaStream_t st);
 void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring, int ring_cap,
-                        cudaStream_t st);
+                        cudaStream_t st, int recorded = 0);
 void launch_set_counters(int *counters, int run_step, int ring_pos, int it0, cudaStream_t st);
 void launch_set_flags(int *flag, int n, int value, cudaStream_t st);
 void launch_scale_vel(const DevState &s, cudaStream_t st);
@@ -112,6 +112,23 @@ int nqt_particles_per_block();
 template <typename T> void configure_integrate_kernels(int max_nq);
 int gf_opt_blocks(int M);
 double fp32_fma_tflops(int device);
+// S(q, omega) of recorded n(q,t) series (p3m_sqw.cu)
+struct SqwArgs {
+    const double2 *src;       // series element (row, r, col, ax) at row*row_stride + r*rep_stride + col*3 + ax
+    long long row_stride, rep_stride;
+    int cap, row0;            // row(t) = (row0 + t) % cap
+    int r0, nrep_launch;      // replicas r0 .. r0 + nrep_launch - 1
+    int col0, col_stride, ncols, nt, logP, bluestein;
+    const double2 *chirp_fft_br;  // Bluestein chirp spectrum, 2^logP points, bit-reversed
+    const double *nrep_n;     // particles per replica
+    double dt;
+    int per_axis;
+    double *out_rep;
+};
+int sqw_max_points();   // largest transform length
+int sqw_smem_points();  // largest transform length held in shared memory
+void launch_sqw(const SqwArgs &a, double2 *gscratch, cudaStream_t st);
+void launch_sqw_mean(const double *out_rep, int nrep, long long n, double *out, cudaStream_t st);
 
 
 }  // namespace p3m

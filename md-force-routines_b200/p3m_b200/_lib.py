@@ -89,6 +89,10 @@ SIGNATURES = {
     "p3m_get_energies": (_I, [_V, _D, _I, ctypes.POINTER(_I)]),
     "p3m_get_nqt": (_I, [_V, _I, _D, _I, ctypes.POINTER(_I)]),
     "p3m_check": (_I, [_V]),
+    "p3m_sqw": (_I, [_V, ctypes.c_double, _I, _I, _I, _I, _D, _D]),
+    "p3m_sqw_series": (_I, [_I, _D, _I, ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]),
+    "p3m_sqw_runs": (_I, [_I, _D, _I, _I, _I, _I, _I, _I, ctypes.c_double, ctypes.c_double,
+                          ctypes.c_double, _D]),
     "p3m_get_replica_stats": (_I, [_V, _I, _D]),
     "p3m_sync": (_I, [_V]),
     "p3m_stream": (_V, [_V]),

@@ -61,6 +61,7 @@ class Context:
         check(rc, None)
         self._h = h
         self._green_key = [None] * R
+        self._nq = 0
 
     # -- lifetime -------------------------------------------------------------
     @property
@@ -198,6 +199,7 @@ class Context:
 
     def set_nqt(self, qmult, capacity):
         qm = None if qmult is None or len(qmult) == 0 else _f64(qmult)
+        self._nq = 0 if qm is None else len(qm)
         self._ck(lib().p3m_set_nqt(self.handle, dptr(qm), 0 if qm is None else len(qm),
                                    int(capacity)))
 
@@ -223,6 +225,18 @@ class Context:
         self._ck(lib().p3m_get_nqt(self.handle, replica, dptr(out), max_steps, ctypes.byref(n)))
         o = out[: n.value]
         return o[..., 0] + 1j * o[..., 1]
+
+    def sqw(self, dt, nt, col0=0, col_stride=1, ncols=None, per_replica=False):
+        """S(q,w) of the last nt recorded n(q,t) rows, averaged over axes and
+        replicas: (ncols, nt); with per_replica also (R, ncols, nt)."""
+        nq = self._nq
+        if ncols is None:
+            ncols = (nq - col0 + col_stride - 1) // col_stride
+        out = np.empty((ncols, nt))
+        rep = np.empty((len(self.replicas), ncols, nt)) if per_replica else None
+        self._ck(lib().p3m_sqw(self.handle, float(dt), int(col0), int(col_stride), int(ncols),
+                               int(nt), dptr(out), dptr(rep)))
+        return (out, rep) if per_replica else out
 
     def replica_stats(self, replica=0):
         """{U_short, U_fft, U_self, U, K, T, factor, rebuilds} of one replica."""
@@ -270,6 +284,37 @@ def gf_opt_device(kappa, alpha, p, m_alias, M, L, device=0):
     check(lib().p3m_gf_opt(int(device), float(kappa), float(alpha), int(p), int(m_alias), int(M),
                            float(L), dptr(G), dptr(A)), None)
     return G, float(A[0])
+
+
+def _complex_ptr(a):
+    return a.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def sqw_series(n_q_t, N, dt, T, device=0):
+    """s_of_q_w.n_of_q_w on the device: (nt, 3) complex -> (nt, 3) =
+    |dt FFT_t n|^2 / (N T) per axis."""
+    a = np.ascontiguousarray(n_q_t, dtype=np.complex128)
+    if a.ndim != 2 or a.shape[1] != 3:
+        raise ValueError("n_q_t must have shape (nt, 3)")
+    nt = a.shape[0]
+    out = np.empty((nt, 3))
+    check(lib().p3m_sqw_series(int(device), _complex_ptr(a), nt, float(N), float(dt), float(T),
+                               dptr(out)), None)
+    return out
+
+
+def sqw_runs(n_q_t_array, Nq, N, dt, T, col0=0, col_stride=3, device=0):
+    """s_of_q_w_avg.s_of_q_w_avg_mat on the device: (runs, nt, nq, 3)
+    complex -> (runs, Nq, nt), the mean over axes of S(q,w) on q columns
+    col0 + i*col_stride."""
+    a = np.ascontiguousarray(n_q_t_array, dtype=np.complex128)
+    if a.ndim != 4 or a.shape[3] != 3:
+        raise ValueError("n_q_t_array must have shape (runs, nt, nq, 3)")
+    R, nt, nq = a.shape[:3]
+    out = np.empty((R, int(Nq), nt))
+    check(lib().p3m_sqw_runs(int(device), _complex_ptr(a), R, nt, nq, int(col0), int(col_stride),
+                             int(Nq), float(N), float(dt), float(T), dptr(out)), None)
+    return out
 
 
 def fp32_peak_tflops(device=0):
