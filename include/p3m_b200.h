@@ -161,6 +161,28 @@ int p3m_sqw_series(int device, const double *nqt, int nt, double N, double dt, d
 int p3m_sqw_runs(int device, const double *nqt, int nrun, int nt, int nq, int col0, int col_stride,
                  int ncols, double N, double dt, double T, double *out);
 
+/* ---- PPPM accuracy estimates. No counterpart in the reference, which sets
+ * alpha, r_c and M by hand (yukawa_MD_p3m_ord6.py:52-68) and whose only
+ * error measure is A_pm (yukawa_gf_opt.py:96). RMS per-particle force errors
+ * for n unit charges at random positions in a box of side `box`, in the
+ * reference's reduced units. */
+
+/* PP truncation at r_c: dF^2 = 4 pi (n/box^3) int_rc^inf F_sr(r)^2 r^2 dr,
+ * F_sr the Yukawa-Ewald short-range force of yukawa_pp.py:115-124 (host). */
+int p3m_pp_error(double n, double box, double kappa, double alpha, double rc, double *dF);
+
+/* Smallest r_c <= rc_max with p3m_pp_error <= tol; *rc = -1 when rc_max
+ * misses tol (host). */
+int p3m_pp_cutoff(double n, double box, double kappa, double alpha, double tol, double rc_max,
+                  double *rc);
+
+/* PM error of `count` parameter sets (device, FP64): the Q functional at the
+ * optimal influence function, dF^2 = n/V^2 sum_k [sum_m k_m^2 G_m^2 - A(k)]
+ * with the alias sum of yukawa_gf_opt.py:24-94; a_pm (may be NULL) receives
+ * sum_k A(k), the reference's A_pm for the same parameters. */
+int p3m_pm_error(int device, int count, const double *n, const double *box, const double *kappa,
+                 const double *alpha, const int *M, int p, int m_alias, double *dF, double *a_pm);
+
 /* ---- device-resident ("fast") path over all replicas ----------------------- */
 
 /* Copy state in/out. Any of the pointers may be NULL. Arrays are (n,3). */

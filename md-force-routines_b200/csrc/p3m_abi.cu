@@ -196,7 +196,7 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
                     s.cell_start, s.cell_cursor, s.cell_tmp, s.cell_perm, s.cell_slot, s.xq, s.nnb,
                     s.nlist, s.rebuild, s.pos_ref, s.pp_tables,
                     s.acc_pp, s.brick_key, s.brick_count, s.brick_start, s.brick_cursor,
-                    s.brick_perm, s.brick_slot, s.brick_tmp, s.tiles, s.spec, s.ek, s.green, s.efield,
+                    s.brick_perm, s.brick_slot, s.brick_hist, s.tiles, s.spec, s.ek, s.green, s.efield,
                     s.acc_pm, s.twiddle, s.u_pp_part, s.u_pm_part, s.kin_part, s.rep_out,
                     s.status, ctx->counters, ctx->ring, ctx->qmult, ctx->nqt_part,
                     ctx->nqt_ring, ctx->scratch, ctx->ep, ctx->tmp_nq};
@@ -285,7 +285,8 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     s.nrep = n_reps;
     s.has_mesh = with_mesh;
     ctx->rh.resize(n_reps);
-    long long mesh = 0, spec = 0, tile = 0;
+    long long mesh = 0, spec = 0, tile = 0, hist = 0;
+    int nchunk = 0, max_bricks = 0;
     int p = 0, cell = 0, brick = 0, wa = 0, wb = 0, wc = 0, wp = 0, blk = 0, maxm = 0, maxp = 0;
     for (int r = 0; r < n_reps; ++r) {
         const p3m_replica_desc &d = reps[r];
@@ -321,6 +322,11 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
             R.wb_off = wb;
             R.wc_off = wc;
             R.wp_off = wp;
+            R.sc_off = nchunk;
+            R.sh_off = hist;
+            nchunk += (d.n + SORT_CH - 1) / SORT_CH;
+            hist += (long long)((d.n + SORT_CH - 1) / SORT_CH) * R.nb * R.nb * R.nb;
+            if (R.nb * R.nb * R.nb > max_bricks) max_bricks = R.nb * R.nb * R.nb;
             brick += R.nb * R.nb * R.nb;
             mesh += (long long)M * M * M;
             spec += (long long)(M / 2 + 1) * M * M;
@@ -424,7 +430,9 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(dalloc(&s.brick_start, (size_t)brick + 1));
     CKC(dalloc(&s.brick_cursor, (size_t)brick));
     CKC(dalloc(&s.brick_perm, (size_t)p));
-    CKC(dalloc(&s.brick_tmp, (size_t)p));
+    s.nchunk = nchunk;
+    s.max_bricks = max_bricks;
+    CKC(dalloc(&s.brick_hist, (size_t)hist));
     CKC(dalloc(&s.brick_slot, (size_t)p));
     if (with_mesh)
         CKC(valloc(&s.tiles, (size_t)tile * (precision == P3M_FP32 ? sizeof(float) : sizeof(double))));
@@ -483,8 +491,8 @@ template <typename T> static void seq_sort(p3m_ctx *ctx, bool keys)
     launch_build_lists<T>(s, ctx->st);  // from those coordinates (rebuild steps)
     ctx->launches += 5;
     if (s.has_mesh) {
-        launch_fix_bricks(s, ctx->st);
-        ctx->launches++;
+        launch_sort_bricks(s, ctx->st);
+        ctx->launches += 3;
     }
 }
 
@@ -1527,4 +1535,78 @@ extern "C" int p3m_sqw_runs(int device, const double *nqt, int nrun, int nt, int
         return fail(nullptr, P3M_EARG, "p3m_sqw_runs", "q columns out of range");
     return sqw_host("p3m_sqw_runs", device, nqt, nrun, nt, nq, col0, col_stride, ncols, N, dt, T, 0,
                     out);
+}
+
+// ---------------------------------------------------------------------------
+// PPPM error estimates
+// ---------------------------------------------------------------------------
+
+extern "C" int p3m_pp_error(double n, double box, double kappa, double alpha, double rc, double *dF)
+{
+    if (!dF || !(n > 0) || !(box > 0) || !(kappa >= 0) || !(alpha > 0) || !(rc > 0))
+        return fail(nullptr, P3M_EARG, "p3m_pp_error", "bad argument");
+    *dF = pp_error_estimate(n, box, kappa, alpha, rc);
+    return P3M_OK;
+}
+
+extern "C" int p3m_pp_cutoff(double n, double box, double kappa, double alpha, double tol,
+                             double rc_max, double *rc)
+{
+    if (!rc || !(n > 0) || !(box > 0) || !(kappa >= 0) || !(alpha > 0) || !(tol > 0) || !(rc_max > 0))
+        return fail(nullptr, P3M_EARG, "p3m_pp_cutoff", "bad argument");
+    *rc = pp_cutoff_for(n, box, kappa, alpha, tol, rc_max);
+    return P3M_OK;
+}
+
+extern "C" int p3m_pm_error(int device, int count, const double *n, const double *box,
+                            const double *kappa, const double *alpha, const int *M, int p,
+                            int m_alias, double *dF, double *a_pm)
+{
+    if (count < 0 || (count > 0 && (!n || !box || !kappa || !alpha || !M || !dF)))
+        return fail(nullptr, P3M_EARG, "p3m_pm_error", "NULL argument");
+    if (p < 1 || p > 7 || m_alias < 0 || m_alias > 7)
+        return fail(nullptr, P3M_EARG, "p3m_pm_error", "p must be in [1, 7], m_alias in [0, 7]");
+    int maxb = 1;
+    for (int i = 0; i < count; ++i) {
+        if (!(n[i] > 0) || !(box[i] > 0) || !(kappa[i] >= 0) || !(alpha[i] > 0) || M[i] < 2 ||
+            M[i] > 512)
+            return fail(nullptr, P3M_EARG, "p3m_pm_error", "bad parameter set");
+        maxb = std::max(maxb, pm_error_blocks(M[i]));
+    }
+    if (count == 0) return P3M_OK;
+    int rc = check_device(nullptr, device);
+    if (rc != P3M_OK) return rc;
+    // partial sums of every set, [set][2][block]
+    const size_t stride = 2 * (size_t)maxb;
+    double *d_part = nullptr;
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&d_part, (size_t)count * stride * sizeof(double));
+    for (int i = 0; e == cudaSuccess && i < count; ++i) {
+        double *q = d_part + (size_t)i * stride;
+        launch_pm_error(kappa[i], alpha[i], p, m_alias, M[i], box[i], q, q + maxb, st);
+        e = cudaGetLastError();
+    }
+    std::vector<double> h;
+    if (e == cudaSuccess) {
+        h.resize((size_t)count * stride);
+        e = cudaMemcpyAsync(h.data(), d_part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_part);
+    if (st) cudaStreamDestroy(st);
+    if (e != cudaSuccess) return fail(nullptr, P3M_ECUDA, "p3m_pm_error", cudaGetErrorString(e));
+    for (int i = 0; i < count; ++i) {
+        const double *q = h.data() + (size_t)i * stride;
+        const int nb = pm_error_blocks(M[i]);
+        double sq = 0.0, sa = 0.0;
+        for (int b = 0; b < nb; ++b) {
+            sq += q[b];
+            sa += q[maxb + b];
+        }
+        const double V = box[i] * box[i] * box[i];
+        dF[i] = std::sqrt(std::max(sq, 0.0) * n[i] / (V * V));
+        if (a_pm) a_pm[i] = sa;
+    }
+    return P3M_OK;
 }

@@ -40,8 +40,9 @@ struct DevState {
     void *acc_pp = nullptr;      // V4<T> PP acceleration, cell-sorted order
     // brick sort
     int *brick_key = nullptr, *brick_count = nullptr, *brick_start = nullptr;
-    int *brick_cursor = nullptr, *brick_tmp = nullptr, *brick_perm = nullptr,
-        *brick_slot = nullptr;
+    int *brick_cursor = nullptr, *brick_perm = nullptr, *brick_slot = nullptr;
+    int *brick_hist = nullptr;   // [replica][chunk][brick] counts, then chunk offsets
+    int nchunk = 0, max_bricks = 0;
     // mesh
     void *tiles = nullptr;       // T assignment tiles [brick][TILE^3]
     void *spec = nullptr;        // C2<T> half spectrum rho_k / phi_k, [kx][z][y]
@@ -69,7 +70,7 @@ void launch_cell_keys(const DevState &s, cudaStream_t st);
 void launch_scan(const DevState &s, cudaStream_t st);
 void launch_scatter(const DevState &s, cudaStream_t st);
 template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st);
-void launch_fix_bricks(const DevState &s, cudaStream_t st);
+void launch_sort_bricks(const DevState &s, cudaStream_t st);  // 3 kernels
 template <typename T> void launch_quantize(const DevState &s, cudaStream_t st);
 template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st);
 template <typename T> void launch_pp(const DevState &s, cudaStream_t st);
@@ -129,6 +130,13 @@ int sqw_max_points();   // largest transform length
 int sqw_smem_points();  // largest transform length held in shared memory
 void launch_sqw(const SqwArgs &a, double2 *gscratch, cudaStream_t st);
 void launch_sqw_mean(const double *out_rep, int nrep, long long n, double *out, cudaStream_t st);
+// PPPM error estimates (p3m_tune.cu)
+double pp_error_estimate(double n_particles, double box, double kappa, double alpha, double rc);
+double pp_cutoff_for(double n_particles, double box, double kappa, double alpha, double tol,
+                     double rc_max);
+int pm_error_blocks(int M);
+void launch_pm_error(double kappa, double alpha, int p, int m_alias, int M, double L,
+                     double *q_part, double *a_part, cudaStream_t st);
 
 
 }  // namespace p3m

@@ -14,9 +14,13 @@
 // lists, and its rounding, do not depend on the other replicas of a batch. It is deterministic: counts and offsets
 // come from integer atomics and a scan; the order inside a cell is then
 // fixed by sorting each cell's particle indices ascending (rank sort), so
-// every rerun builds the same lists. The brick sort runs every step; each
-// brick's particles are then put in ascending index order the same way, so
-// the assignment adds them in a fixed order.
+// every rerun builds the same lists. The brick sort runs every step and puts
+// each brick's particles in ascending index order, so the assignment adds
+// them in a fixed order: a stable counting sort over chunks of SORT_CH
+// consecutive particles of one replica (per-chunk counts per brick, a scan of
+// each brick's counts over the chunks, then one warp per chunk placing its
+// particles in index order). Its work is linear in the particle count however
+// many particles share a brick.
 #include "p3m_kernels.h"
 
 namespace p3m {
@@ -117,20 +121,13 @@ __global__ void k_scan(const RepDev *__restrict__ reps, int nrep, int *cell_coun
 }
 
 __global__ void k_scatter(const int *__restrict__ cell_key, const int *__restrict__ cell_start,
-                          int *cell_cursor, int *__restrict__ cell_tmp,
-                          const int *__restrict__ brick_key, const int *__restrict__ brick_start,
-                          int *brick_cursor, int *__restrict__ brick_tmp,
-                          int ntot, int has_mesh,
+                          int *cell_cursor, int *__restrict__ cell_tmp, int ntot,
                           const int *__restrict__ prep, const int *__restrict__ rebuild)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
         if (rebuild[prep[i]]) {
             int c = cell_key[i];
             cell_tmp[cell_start[c] + atomicAdd(&cell_cursor[c], 1)] = i;
-        }
-        if (has_mesh) {
-            int b = brick_key[i];
-            brick_tmp[brick_start[b] + atomicAdd(&brick_cursor[b], 1)] = i;
         }
     }
 }
@@ -165,23 +162,84 @@ __global__ void k_fix_cells(const RepDev *__restrict__ reps, int nrep,
     }
 }
 
-// One warp per brick: order the brick's particles by index.
-__global__ void k_fix_bricks(const int *__restrict__ brick_start, const int *__restrict__ brick_tmp,
-                             int *__restrict__ brick_perm, int *__restrict__ brick_slot, int nbrick)
+// ---- brick sort ----------------------------------------------------------
+
+__device__ __forceinline__ int sort_chunks(const RepDev &R) { return (R.n + SORT_CH - 1) / SORT_CH; }
+
+// One block per chunk: hist[chunk][k] = particles of the chunk in the
+// replica's brick k (shared-memory integer counts).
+__global__ void __launch_bounds__(256)
+k_brick_hist(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_key,
+             int *__restrict__ hist, int nchunk)
 {
-    const int lane = threadIdx.x & 31;
-    const int wpb = blockDim.x >> 5;
-    for (int b = blockIdx.x * wpb + (threadIdx.x >> 5); b < nbrick; b += gridDim.x * wpb) {
-        const int start = brick_start[b], n = brick_start[b + 1] - start;
+    extern __shared__ int hcount[];
+    for (int c = blockIdx.x; c < nchunk; c += gridDim.x) {
+        const RepDev &R = reps[find_rep(c, nrep, [&](int k) { return reps[k].sc_off; })];
+        const int nbr = R.nb * R.nb * R.nb;
+        const int cl = c - R.sc_off;
+        const int p0 = R.p_off + cl * SORT_CH, n = min(SORT_CH, R.n - cl * SORT_CH);
+        for (int k = threadIdx.x; k < nbr; k += blockDim.x) hcount[k] = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            atomicAdd(&hcount[brick_key[p0 + i] - R.brick_off], 1);
+        __syncthreads();
+        int *row = hist + R.sh_off + (long long)cl * nbr;
+        for (int k = threadIdx.x; k < nbr; k += blockDim.x) row[k] = hcount[k];
+        __syncthreads();
+    }
+}
+
+// One thread per brick: its counts over the replica's chunks become the
+// chunks' first slots (exclusive scan from brick_start).
+__global__ void k_brick_colscan(const RepDev *__restrict__ reps, int nrep,
+                                const int *__restrict__ brick_start, int *__restrict__ hist,
+                                int nbrick)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbrick; b += gridDim.x * blockDim.x) {
+        const RepDev &R = reps[find_rep(b, nrep, [&](int k) { return reps[k].brick_off; })];
+        const int nbr = R.nb * R.nb * R.nb;
+        const int nch = sort_chunks(R);
+        int *col = hist + R.sh_off + (b - R.brick_off);
+        int s = brick_start[b];
+        for (int cl = 0; cl < nch; ++cl) {
+            const int t = col[(long long)cl * nbr];
+            col[(long long)cl * nbr] = s;
+            s += t;
+        }
+    }
+}
+
+// One warp per chunk, 32 particles at a time in index order: lanes with the
+// same brick take consecutive slots in lane order (__match_any_sync), then
+// the group's last lane advances the brick's next slot.
+__global__ void __launch_bounds__(32)
+k_brick_place(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_key,
+              const int *__restrict__ hist, int *__restrict__ brick_perm,
+              int *__restrict__ brick_slot, int nchunk)
+{
+    extern __shared__ int next_slot[];
+    const int lane = threadIdx.x;
+    for (int c = blockIdx.x; c < nchunk; c += gridDim.x) {
+        const RepDev &R = reps[find_rep(c, nrep, [&](int k) { return reps[k].sc_off; })];
+        const int nbr = R.nb * R.nb * R.nb;
+        const int cl = c - R.sc_off;
+        const int p0 = R.p_off + cl * SORT_CH, n = min(SORT_CH, R.n - cl * SORT_CH);
+        const int *row = hist + R.sh_off + (long long)cl * nbr;
+        for (int k = lane; k < nbr; k += 32) next_slot[k] = row[k];
+        __syncwarp();
         for (int e0 = 0; e0 < n; e0 += 32) {
             const int e = e0 + lane;
-            const int v = (e < n) ? brick_tmp[start + e] : 0x7fffffff;
-            int rank = 0;
-            for (int f = 0; f < n; ++f) rank += (brick_tmp[start + f] < v) ? 1 : 0;
-            if (e < n) {
-                brick_perm[start + rank] = v;
-                brick_slot[v] = start + rank;
+            const bool valid = e < n;
+            const int key = valid ? brick_key[p0 + e] - R.brick_off : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            if (valid) {
+                const int slot = next_slot[key] + __popc(peers & ((1u << lane) - 1u));
+                brick_perm[slot] = p0 + e;
+                brick_slot[p0 + e] = slot;
             }
+            __syncwarp();
+            if (valid && lane == 31 - __clz(peers)) next_slot[key] += __popc(peers);
+            __syncwarp();
         }
     }
 }
@@ -216,17 +274,19 @@ void launch_scan(const DevState &s, cudaStream_t st)
 void launch_scatter(const DevState &s, cudaStream_t st)
 {
     k_scatter<<<grid_for(s.ntot, 256), 256, 0, st>>>(s.cell_key, s.cell_start, s.cell_cursor,
-                                                      s.cell_tmp, s.brick_key, s.brick_start,
-                                                      s.brick_cursor, s.brick_tmp, s.ntot,
-                                                      s.has_mesh, s.prep, s.rebuild);
+                                                      s.cell_tmp, s.ntot, s.prep, s.rebuild);
 }
 
-void launch_fix_bricks(const DevState &s, cudaStream_t st)
+void launch_sort_bricks(const DevState &s, cudaStream_t st)
 {
-    const int wpb = 8;
-    k_fix_bricks<<<(s.nbrick + wpb - 1) / wpb, wpb * 32, 0, st>>>(s.brick_start, s.brick_tmp,
-                                                                 s.brick_perm, s.brick_slot,
-                                                                 s.nbrick);
+    const size_t smem = (size_t)s.max_bricks * sizeof(int);
+    k_brick_hist<<<grid_for(s.nchunk, 1), 256, smem, st>>>(s.reps, s.nrep, s.brick_key,
+                                                            s.brick_hist, s.nchunk);
+    k_brick_colscan<<<grid_for(s.nbrick, 128), 128, 0, st>>>(s.reps, s.nrep, s.brick_start,
+                                                              s.brick_hist, s.nbrick);
+    k_brick_place<<<grid_for(s.nchunk, 1), 32, smem, st>>>(s.reps, s.nrep, s.brick_key,
+                                                           s.brick_hist, s.brick_perm,
+                                                           s.brick_slot, s.nchunk);
 }
 
 template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st)

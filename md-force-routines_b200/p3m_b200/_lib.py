@@ -91,6 +91,9 @@ SIGNATURES = {
     "p3m_check": (_I, [_V]),
     "p3m_sqw": (_I, [_V, ctypes.c_double, _I, _I, _I, _I, _D, _D]),
     "p3m_sqw_series": (_I, [_I, _D, _I, ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]),
+    "p3m_pp_error": (_I, [ctypes.c_double] * 5 + [_D]),
+    "p3m_pp_cutoff": (_I, [ctypes.c_double] * 6 + [_D]),
+    "p3m_pm_error": (_I, [_I, _I, _D, _D, _D, _D, ctypes.POINTER(ctypes.c_int), _I, _I, _D, _D]),
     "p3m_sqw_runs": (_I, [_I, _D, _I, _I, _I, _I, _I, _I, ctypes.c_double, ctypes.c_double,
                           ctypes.c_double, _D]),
     "p3m_get_replica_stats": (_I, [_V, _I, _D]),

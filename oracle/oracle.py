@@ -29,6 +29,7 @@ the one place where parity is unpinned.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 
@@ -288,3 +289,107 @@ def sqw_avg(n_q_t_array, Nq, N, dt, T, stride=3):
         for i in range(Nq):
             out[j, i, :] = np.mean(sqw(n_q_t_array[j][:, i * stride, :], N, dt, T), axis=1)
     return out.mean(axis=0)
+
+
+# ---------------------------------------------------------------------------
+# PPPM error estimates (the reference sets alpha, r_c and M by hand,
+# yukawa_MD_p3m_ord6.py:52-68; its only error measure is A_pm,
+# yukawa_gf_opt.py:96). Restated from the published methods, for checking the
+# library's estimator.
+# ---------------------------------------------------------------------------
+
+_erfc_v = np.frompyfunc(math.erfc, 1, 1)
+
+
+def pair_force_sr(r, kappa, alpha):
+    """Radial short-range Yukawa-Ewald force -d phi/dr of
+    phi = (1/2r)[e^{kr} erfc(ar + b) + e^{-kr} erfc(ar - b)], b = k/(2a)
+    (yukawa_pp.py:115-124)."""
+    r = np.asarray(r, dtype=np.float64)
+    b = kappa / (2.0 * alpha)
+    ep = np.exp(kappa * r) * _erfc_v(alpha * r + b).astype(np.float64)
+    em = np.exp(-kappa * r) * _erfc_v(alpha * r - b).astype(np.float64)
+    phi = 0.5 * (ep + em) / r
+    return (phi / r - 0.5 * kappa * (ep - em) / r
+            + 2.0 * alpha / (r * np.sqrt(np.pi)) * np.exp(-alpha * alpha * r * r - b * b))
+
+
+def pp_error(N, L, kappa, alpha, rc, n_int=4000):
+    """RMS per-particle force error of cutting the short-range force at r_c
+    for N unit charges placed at random (Kolafa & Perram, Mol. Sim. 9 (1992)
+    351, with the Yukawa-Ewald force): sqrt(4 pi n int_rc^inf F(r)^2 r^2 dr),
+    n = N / L^3, by Simpson's rule on [r_c, sqrt(r_c^2 + 40/alpha^2)]."""
+    n = N / L ** 3
+    r_end = np.sqrt(rc * rc + 40.0 / (alpha * alpha))
+    r = np.linspace(rc, r_end, n_int + 1)
+    f = pair_force_sr(r, kappa, alpha) ** 2 * r * r
+    w = np.ones(n_int + 1)
+    w[1:-1:2] = 4.0
+    w[2:-1:2] = 2.0
+    integral = (r[1] - r[0]) / 3.0 * np.sum(w * f)
+    return float(np.sqrt(4.0 * np.pi * n * integral))
+
+
+def pm_error(N, L, kappa, alpha, M, p=6, m_max=3):
+    """RMS per-particle PM force error with the optimal influence function
+    (Hockney & Eastwood, Computer Simulation Using Particles, eq. 8-22):
+    sqrt(N / V^2 sum_k [sum_m k_m^2 G_m^2 - A(k)]), G_m the Yukawa-Ewald
+    long-range kernel 4 pi e^{-(kappa^2+k_m^2)/(4 alpha^2)}/(kappa^2+k_m^2),
+    A(k) the term yukawa_gf_opt.py:92-94 sums into A_pm. Returns
+    (dF_pm, A_pm)."""
+    h = L / M
+    s = np.arange(M) - M // 2
+    kx = (2 * np.pi * s / L).reshape((1, 1, M))
+    ky = (2 * np.pi * s / L).reshape((1, M, 1))
+    kz = (2 * np.pi * s / L).reshape((M, 1, 1))
+    ksq = kx * kx + ky * ky + kz * kz
+    UG = np.zeros((M, M, M))
+    Usq = np.zeros((M, M, M))
+    R2 = np.zeros((M, M, M))
+
+    def sinc(x):
+        return np.where(x != 0.0, np.sin(0.5 * x * h) / np.where(x != 0.0, 0.5 * x * h, 1.0), 1.0)
+
+    for mz in range(-m_max, m_max + 1):
+        kmz = kz + 2 * np.pi * mz * M / L
+        for my in range(-m_max, m_max + 1):
+            kmy = ky + 2 * np.pi * my * M / L
+            for mx in range(-m_max, m_max + 1):
+                kmx = kx + 2 * np.pi * mx * M / L
+                kmsq = kmx * kmx + kmy * kmy + kmz * kmz
+                u2 = (sinc(kmx) * sinc(kmy) * sinc(kmz)) ** (2 * p)
+                g = 4 * np.pi * np.exp(-0.25 * (kappa ** 2 + kmsq) / alpha ** 2) / (kappa ** 2 + kmsq)
+                UG += u2 * g * (kx * kmx + ky * kmy + kz * kmz)
+                Usq += u2
+                R2 += kmsq * g * g
+    nz = ksq != 0.0
+    A = np.where(nz, UG ** 2 / np.where(nz, Usq ** 2 * ksq, 1.0), 0.0)
+    Q = np.sum(np.where(nz, R2, 0.0)) - np.sum(A)
+    V = L ** 3
+    return float(np.sqrt(max(Q, 0.0) * N / (V * V))), float(np.sum(A))
+
+
+def ewald_lr_acc(pos, L, kappa, alpha, kcut_exp=40.0):
+    """Exact long-range field at each particle, E_i = -(1/V) sum_{k!=0}
+    i k G(k) e^{i k.r_i} sum_j e^{-i k.r_j}, over all k with
+    (k^2+kappa^2)/(4 alpha^2) < kcut_exp (the remainder is below e^-40)."""
+    V = L ** 3
+    kmax = 2.0 * alpha * np.sqrt(kcut_exp)
+    nmax = int(np.ceil(kmax * L / (2 * np.pi)))
+    n = np.arange(-nmax, nmax + 1)
+    g = np.stack(np.meshgrid(n, n, n, indexing="ij"), -1).reshape(-1, 3).astype(np.float64)
+    k = 2 * np.pi * g / L
+    ksq = np.sum(k * k, axis=1)
+    keep = (ksq > 0) & ((ksq + kappa ** 2) / (4 * alpha ** 2) < kcut_exp)
+    k, ksq = k[keep], ksq[keep]
+    G = 4 * np.pi * np.exp(-(ksq + kappa ** 2) / (4 * alpha ** 2)) / (ksq + kappa ** 2)
+    acc = np.zeros_like(pos)
+    for c0 in range(0, len(k), 2048):
+        kc, Gc = k[c0:c0 + 2048], G[c0:c0 + 2048]
+        ph = pos @ kc.T                       # (N, K)
+        cs, sn = np.cos(ph), np.sin(ph)
+        S_re, S_im = cs.sum(0), -sn.sum(0)    # S(k) = sum_j e^{-i k r_j}
+        # Re(-i e^{i k r_i} S) = sin(k r_i) S_re + cos(k r_i) S_im
+        w = (sn * S_re + cs * S_im) * Gc      # (N, K)
+        acc += w @ kc
+    return acc / V
