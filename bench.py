@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--equil", type=int, default=300,
                     help="untimed thermostat steps before the NVE warm-up")
     ap.add_argument("--no-tune", action="store_true", help="skip the PP autotuner")
+    ap.add_argument("--pp-config", default=None, metavar="TPI,SKIN",
+                    help="set threads per particle and Verlet skin instead of autotuning")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the FP64, e2e, roofline and CPU-baseline legs")
     return ap.parse_args()
@@ -278,7 +280,10 @@ def run_ours(args):
     # from the random initial state, then NVE warm-up (also builds the graph)
     ctx.run(args.equil, MODE_THERMOSTAT, it0=0, graph=True)
     tuned = None
-    if not args.no_tune:
+    if args.pp_config:
+        tpi, skin = args.pp_config.split(",")
+        ctx.set_pp_config(int(tpi), float(skin))
+    elif not args.no_tune:
         from p3m_b200.autotune import tune
 
         tuned = tune(ctx, use_cache=False)
@@ -419,41 +424,35 @@ def extras(args, line, ctx, reps, states, device):
                           "batched_fp32_over_fp64": line["value"] / line["n_gpus"] / fp64}
 
     # -- end to end through the C ABI with host buffers ----------------------------
-    # per step: H2D of every replica's (pos, vel, acc) from pinned host memory,
-    # one batched step, D2H of the state and of the step's energies
-    host = []
-    for i, r in enumerate(reps):
-        bufs = [torch.empty((r.N, 3), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
-        bufs[0][:] = states[i][0]
-        bufs[1][:] = states[i][1]
-        bufs[2][:] = 0.0
-        host.append(bufs)
+    # per step: H2D of the whole ensemble's (pos, vel, acc) from pinned host
+    # memory, one batched step, D2H of the state and of the step's energies
+    ntot = sum(r.N for r in reps)
+    host = [torch.empty((ntot, 3), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+    host[0][:] = np.concatenate([st[0] for st in states])
+    host[1][:] = np.concatenate([st[1] for st in states])
     with Context(reps, precision=FP32, device=device) as c:
-        for i, b in enumerate(host):
-            c.set_state(i, b[0], b[1])
+        c.set_state_all(host[0], host[1])
         c.init_forces()
-        for i, b in enumerate(host):
-            b[0][:], b[1][:], b[2][:] = c.get_state(i)
+        c.get_state_all(*host)
         c.run(2, MODE_NVE, graph=True)
-        n_e2e = min(args.steps, 50)
+        c.get_state_all(*host)
+        n_e2e = min(args.steps, 200)
         s = torch.cuda.ExternalStream(c.stream())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
         for _ in range(n_e2e):
-            for i, b in enumerate(host):
-                c.set_state(i, b[0], b[1], b[2])
+            c.set_state_all(*host, keep_lists=True)
             c.run(1, MODE_NVE, graph=True)
-            for i, b in enumerate(host):
-                b[0][:], b[1][:], b[2][:] = c.get_state(i)
+            c.get_state_all(*host)
             c.energies(max_steps=1)
         e1.record(s)
         e1.synchronize()
         t = e0.elapsed_time(e1) * 1e-3
-    nb = sum(r.N for r in reps) * 3 * 8
-    line["e2e"] = {"value": sum(r.N for r in reps) * n_e2e / t, "unit": UNIT,
+    nb = ntot * 3 * 8
+    line["e2e"] = {"value": ntot * n_e2e / t, "unit": UNIT,
                    "h2d_bytes_per_step": 3 * nb, "d2h_bytes_per_step": 3 * nb + 4 * 8 * len(reps),
-                   "how": "p3m_set_state x R (pinned host -> device), p3m_run(1), p3m_get_state x R "
-                          "and p3m_get_energies per step"}
+                   "how": "p3m_set_state_all (pinned host -> device, lists kept), p3m_run(1), "
+                          "p3m_get_state_all and p3m_get_energies per step"}
 
     # -- CPU baseline: the oracle port on one host core ------------------------------
     G, _ = gf_opt_device(r0.kappa, r0.alpha, 6, 3, r0.M, r0.L, device=device)

@@ -190,6 +190,17 @@ int p3m_set_state(p3m_ctx *ctx, int replica, const double *pos, const double *ve
                   const double *acc);
 int p3m_get_state(p3m_ctx *ctx, int replica, double *pos, double *vel, double *acc);
 
+/* The same for every replica at once: (sum of n, 3) arrays, replicas
+ * concatenated in order, one copy per array (host buffers may be pinned).
+ * p3m_set_state marks the replica's neighbour lists for a rebuild; with
+ * keep_lists != 0 p3m_set_state_all keeps them, and the next step rebuilds a
+ * replica's lists only if one of its particles has moved more than skin/2
+ * since they were built (what p3m_run does between its own steps) -- for a
+ * caller that continues a trajectory it read back. */
+int p3m_set_state_all(p3m_ctx *ctx, const double *pos, const double *vel, const double *acc,
+                      int keep_lists);
+int p3m_get_state_all(p3m_ctx *ctx, double *pos, double *vel, double *acc);
+
 /* Compute acc for the uploaded positions of all replicas (the driver's
  * initial force call, yukawa_MD_p3m_ord6.py:171). */
 int p3m_init_forces(p3m_ctx *ctx);

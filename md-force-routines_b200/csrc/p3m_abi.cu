@@ -287,6 +287,13 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     ctx->rh.resize(n_reps);
     long long mesh = 0, spec = 0, tile = 0, hist = 0;
     int nchunk = 0, max_bricks = 0;
+    // brick-sort chunks: about 4 per SM over the whole batch (one warp each
+    // places its particles), 256 to 4096 particles, a multiple of 32
+    long long ntot_all = 0;
+    for (int r = 0; r < n_reps; ++r) ntot_all += reps[r].n;
+    int sort_ch = (int)std::min<long long>(4096, std::max<long long>(256, (ntot_all + 591) / 592));
+    sort_ch = (sort_ch + 31) / 32 * 32;
+    s.sort_ch = sort_ch;
     int p = 0, cell = 0, brick = 0, wa = 0, wb = 0, wc = 0, wp = 0, blk = 0, maxm = 0, maxp = 0;
     for (int r = 0; r < n_reps; ++r) {
         const p3m_replica_desc &d = reps[r];
@@ -324,8 +331,8 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
             R.wp_off = wp;
             R.sc_off = nchunk;
             R.sh_off = hist;
-            nchunk += (d.n + SORT_CH - 1) / SORT_CH;
-            hist += (long long)((d.n + SORT_CH - 1) / SORT_CH) * R.nb * R.nb * R.nb;
+            nchunk += (d.n + sort_ch - 1) / sort_ch;
+            hist += (long long)((d.n + sort_ch - 1) / sort_ch) * R.nb * R.nb * R.nb;
             if (R.nb * R.nb * R.nb > max_bricks) max_bricks = R.nb * R.nb * R.nb;
             brick += R.nb * R.nb * R.nb;
             mesh += (long long)M * M * M;
@@ -966,6 +973,31 @@ extern "C" int p3m_get_state(p3m_ctx *ctx, int replica, double *pos, double *vel
     if (pos) RET(d2h(ctx, pos, ctx->s.pos + o, b));
     if (vel) RET(d2h(ctx, vel, ctx->s.vel + o, b));
     if (acc) RET(d2h(ctx, acc, ctx->s.acc + o, b));
+    return finish(ctx);
+}
+
+extern "C" int p3m_set_state_all(p3m_ctx *ctx, const double *pos, const double *vel,
+                                 const double *acc, int keep_lists)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    CK(cudaSetDevice(ctx->device));
+    const size_t b = sizeof(double) * 3 * (size_t)ctx->s.ntot;
+    if (pos) RET(h2d(ctx, ctx->s.pos, pos, b));
+    if (vel) RET(h2d(ctx, ctx->s.vel, vel, b));
+    if (acc) RET(h2d(ctx, ctx->s.acc, acc, b));
+    if (pos && !keep_lists) launch_set_flags(ctx->s.rebuild, ctx->s.nrep, 1, ctx->st);
+    ctx->state_set = true;
+    return finish(ctx);
+}
+
+extern "C" int p3m_get_state_all(p3m_ctx *ctx, double *pos, double *vel, double *acc)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    CK(cudaSetDevice(ctx->device));
+    const size_t b = sizeof(double) * 3 * (size_t)ctx->s.ntot;
+    if (pos) RET(d2h(ctx, pos, ctx->s.pos, b));
+    if (vel) RET(d2h(ctx, vel, ctx->s.vel, b));
+    if (acc) RET(d2h(ctx, acc, ctx->s.acc, b));
     return finish(ctx);
 }
 

@@ -20,7 +20,6 @@ constexpr int TILE3 = TILE * TILE * TILE;
 constexpr int PENCIL = 16;
 constexpr int MAX_LOGM = 8;  // M <= 256
 constexpr int PBLK = 256;      // particles per block in replica-aligned particle kernels
-constexpr int SORT_CH = 2048;  // particles per chunk of the brick sort
 
 // Device status bits (first error wins in the host's reading order).
 enum : int {
@@ -49,7 +48,7 @@ struct RepDev {
     int blk_off;           // offset of this replica's particle blocks (PBLK each)
     int pp_blk_off;        // offset of this replica's blocks in the PP force kernel
     int nq_blk_off;        // offset of this replica's blocks in the n(q,t) kernel
-    int sc_off;            // first brick-sort chunk (SORT_CH particles) of this replica
+    int sc_off;            // first brick-sort chunk (DevState::sort_ch particles) of this replica
     long long sh_off;      // offset into the brick-sort count table (chunks x nb^3)
     double L, kappa, alpha, rc, cellw, h, dt, t_desired, af, uf, kf;
     double skin, rcl;      // Verlet skin and list cutoff rc + skin

@@ -42,7 +42,7 @@ struct DevState {
     int *brick_key = nullptr, *brick_count = nullptr, *brick_start = nullptr;
     int *brick_cursor = nullptr, *brick_perm = nullptr, *brick_slot = nullptr;
     int *brick_hist = nullptr;   // [replica][chunk][brick] counts, then chunk offsets
-    int nchunk = 0, max_bricks = 0;
+    int nchunk = 0, max_bricks = 0, sort_ch = 2048;  // chunks, bricks of the largest mesh, chunk size
     // mesh
     void *tiles = nullptr;       // T assignment tiles [brick][TILE^3]
     void *spec = nullptr;        // C2<T> half spectrum rho_k / phi_k, [kx][z][y]

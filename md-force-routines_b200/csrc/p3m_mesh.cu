@@ -16,7 +16,7 @@
 // the half spectrum with weight 2 off the kx = 0 and kx = M/2 planes.
 //
 // Layouts (per replica, concatenated over replicas):
-//   tiles   int64 [brick][TILE^3]   fixed-point partial charge of each brick
+//   tiles   T     [brick][TILE^3]   partial charge of each brick's particles
 //   spec    C2<T> [kx][z][y]        kx in [0, M/2], y fastest
 //   ek      C2<T> [3][kx][z][y]     field spectra
 //   green   T     [kx][z][y]        G_k / V in the same layout
@@ -24,7 +24,9 @@
 //
 // Assignment is deterministic: each CTA owns one brick of BRICK^3 base
 // cells and adds its particles' 216-node stencils into a shared-memory tile
-// of TILE^3 nodes in a fixed particle order without atomics (see k_assign).
+// of TILE^3 nodes, in FP64 in a fixed particle order without atomics
+// (k_assign), or in FP32 with order-independent integer atomics
+// (k_assign_i32).
 // Overlapping tile halos are summed in a fixed order when the first FFT pass
 // reads the mesh.
 //
@@ -243,10 +245,12 @@ k_assign(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
 // every run. Each contribution q w is scaled by S = 2^k, the largest power of
 // two with 0.17 n |q|max S <= 2^22 for the brick's n particles (0.17 bounds a
 // product of three order-6 weights), so no node sum can exceed 2^22 in
-// magnitude. t = q w S is split exactly into an integer part and a 16-bit
+// magnitude. t = q w S is split exactly into an integer part and an fb-bit
 // fraction with the 1.5 * 2^23 rounding constant (exact for |t| < 2^22, no
 // float <-> int conversions) and the two parts go to two int32 tiles: the node
-// value is (hi + lo / 2^16) / S, resolved to 2^-16 / S.
+// value is (hi + lo / 2^fb) / S, resolved to 2^-fb / S. fb = 16, or fewer for
+// bricks of more than 2^14 particles, so that the n fractions of a node (each
+// at most 2^fb) cannot overflow: n 2^fb <= 2^30.
 constexpr int A32_THREADS = 256;
 constexpr float kRound = 12582912.0f;  // 1.5 * 2^23
 constexpr int kRoundBits = 0x4B400000;
@@ -270,6 +274,10 @@ k_assign_i32(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ 
         const double bound = 0.17 * (double)(n > 0 ? n : 1) * R.qmax;
         const int kexp = (int)floor(22.0 - log2(bound > 1e-300 ? bound : 1e-300));
         const float S = ldexpf(1.0f, max(-100, min(kexp, 100)));
+        int nbits = 0;
+        while ((1 << nbits) <= n && nbits < 30) ++nbits;  // n < 2^nbits
+        const int fb = max(0, min(16, 30 - nbits));
+        const float F = ldexpf(1.0f, fb);
         __syncthreads();
         for (int k = threadIdx.x; k < TILE3; k += A32_THREADS) {
             thi[k] = 0;
@@ -305,7 +313,7 @@ k_assign_i32(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ 
                         const float hb = (t - 0.5f) + kRound;       // floor(t), as a float
                         const int hi = __float_as_int(hb) - kRoundBits;
                         const float frac = t - (hb - kRound);         // in [0, 1], exact
-                        const int lo = __float_as_int(frac * 65536.0f + kRound) - kRoundBits;
+                        const int lo = __float_as_int(frac * F + kRound) - kRoundBits;
                         atomicAdd(thi + row + c, hi);
                         atomicAdd(tlo + row + c, lo);
                     }
@@ -315,8 +323,9 @@ k_assign_i32(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ 
         __syncthreads();
         float *dst = tiles + R.tile_off + (long long)local * TILE3;
         const double inv = 1.0 / (double)S;
+        const double invF = 1.0 / (double)F;  // exact: F is a power of two
         for (int k = threadIdx.x; k < TILE3; k += A32_THREADS)
-            dst[k] = (float)(((double)thi[k] + (double)tlo[k] * (1.0 / 65536.0)) * inv);
+            dst[k] = (float)(((double)thi[k] + (double)tlo[k] * invF) * inv);
     }
 }
 

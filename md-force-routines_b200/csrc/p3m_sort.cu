@@ -16,8 +16,9 @@
 // fixed by sorting each cell's particle indices ascending (rank sort), so
 // every rerun builds the same lists. The brick sort runs every step and puts
 // each brick's particles in ascending index order, so the assignment adds
-// them in a fixed order: a stable counting sort over chunks of SORT_CH
-// consecutive particles of one replica (per-chunk counts per brick, a scan of
+// them in a fixed order: a stable counting sort over chunks of `ch`
+// consecutive particles of one replica (ch sized at context creation so that
+// there are a few chunks per SM) (per-chunk counts per brick, a scan of
 // each brick's counts over the chunks, then one warp per chunk placing its
 // particles in index order). Its work is linear in the particle count however
 // many particles share a brick.
@@ -164,20 +165,20 @@ __global__ void k_fix_cells(const RepDev *__restrict__ reps, int nrep,
 
 // ---- brick sort ----------------------------------------------------------
 
-__device__ __forceinline__ int sort_chunks(const RepDev &R) { return (R.n + SORT_CH - 1) / SORT_CH; }
+__device__ __forceinline__ int sort_chunks(const RepDev &R, int ch) { return (R.n + ch - 1) / ch; }
 
 // One block per chunk: hist[chunk][k] = particles of the chunk in the
 // replica's brick k (shared-memory integer counts).
 __global__ void __launch_bounds__(256)
 k_brick_hist(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_key,
-             int *__restrict__ hist, int nchunk)
+             int *__restrict__ hist, int nchunk, int ch)
 {
     extern __shared__ int hcount[];
     for (int c = blockIdx.x; c < nchunk; c += gridDim.x) {
         const RepDev &R = reps[find_rep(c, nrep, [&](int k) { return reps[k].sc_off; })];
         const int nbr = R.nb * R.nb * R.nb;
         const int cl = c - R.sc_off;
-        const int p0 = R.p_off + cl * SORT_CH, n = min(SORT_CH, R.n - cl * SORT_CH);
+        const int p0 = R.p_off + cl * ch, n = min(ch, R.n - cl * ch);
         for (int k = threadIdx.x; k < nbr; k += blockDim.x) hcount[k] = 0;
         __syncthreads();
         for (int i = threadIdx.x; i < n; i += blockDim.x)
@@ -193,12 +194,12 @@ k_brick_hist(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ 
 // chunks' first slots (exclusive scan from brick_start).
 __global__ void k_brick_colscan(const RepDev *__restrict__ reps, int nrep,
                                 const int *__restrict__ brick_start, int *__restrict__ hist,
-                                int nbrick)
+                                int nbrick, int ch)
 {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbrick; b += gridDim.x * blockDim.x) {
         const RepDev &R = reps[find_rep(b, nrep, [&](int k) { return reps[k].brick_off; })];
         const int nbr = R.nb * R.nb * R.nb;
-        const int nch = sort_chunks(R);
+        const int nch = sort_chunks(R, ch);
         int *col = hist + R.sh_off + (b - R.brick_off);
         int s = brick_start[b];
         for (int cl = 0; cl < nch; ++cl) {
@@ -215,7 +216,7 @@ __global__ void k_brick_colscan(const RepDev *__restrict__ reps, int nrep,
 __global__ void __launch_bounds__(32)
 k_brick_place(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_key,
               const int *__restrict__ hist, int *__restrict__ brick_perm,
-              int *__restrict__ brick_slot, int nchunk)
+              int *__restrict__ brick_slot, int nchunk, int ch)
 {
     extern __shared__ int next_slot[];
     const int lane = threadIdx.x;
@@ -223,7 +224,7 @@ k_brick_place(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
         const RepDev &R = reps[find_rep(c, nrep, [&](int k) { return reps[k].sc_off; })];
         const int nbr = R.nb * R.nb * R.nb;
         const int cl = c - R.sc_off;
-        const int p0 = R.p_off + cl * SORT_CH, n = min(SORT_CH, R.n - cl * SORT_CH);
+        const int p0 = R.p_off + cl * ch, n = min(ch, R.n - cl * ch);
         const int *row = hist + R.sh_off + (long long)cl * nbr;
         for (int k = lane; k < nbr; k += 32) next_slot[k] = row[k];
         __syncwarp();
@@ -281,12 +282,12 @@ void launch_sort_bricks(const DevState &s, cudaStream_t st)
 {
     const size_t smem = (size_t)s.max_bricks * sizeof(int);
     k_brick_hist<<<grid_for(s.nchunk, 1), 256, smem, st>>>(s.reps, s.nrep, s.brick_key,
-                                                            s.brick_hist, s.nchunk);
+                                                            s.brick_hist, s.nchunk, s.sort_ch);
     k_brick_colscan<<<grid_for(s.nbrick, 128), 128, 0, st>>>(s.reps, s.nrep, s.brick_start,
-                                                              s.brick_hist, s.nbrick);
+                                                              s.brick_hist, s.nbrick, s.sort_ch);
     k_brick_place<<<grid_for(s.nchunk, 1), 32, smem, st>>>(s.reps, s.nrep, s.brick_key,
                                                            s.brick_hist, s.brick_perm,
-                                                           s.brick_slot, s.nchunk);
+                                                           s.brick_slot, s.nchunk, s.sort_ch);
 }
 
 template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st)

@@ -38,6 +38,16 @@ class Replica:
                            float(self.uf), float(self.kf), float(self.skin))
 
 
+def _out(a, shape):
+    """An output array: a new one, or the caller's if it is FP64, C-order and
+    of the right shape."""
+    if a is None:
+        return np.empty(shape)
+    if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape != tuple(shape):
+        raise ValueError(f"output array must be float64, C-contiguous, shape {tuple(shape)}")
+    return a
+
+
 def _f64(a, shape=None):
     a = np.ascontiguousarray(a, dtype=np.float64)
     if shape is not None and a.shape != shape:
@@ -188,10 +198,29 @@ class Context:
                                      dptr(None if vel is None else _f64(vel)),
                                      dptr(None if acc is None else _f64(acc))))
 
-    def get_state(self, replica):
+    def get_state(self, replica, pos=None, vel=None, acc=None):
+        """-> (pos, vel, acc) of one replica, into the given (n,3) FP64
+        C-order arrays where passed (e.g. pinned buffers)."""
         n = self.replicas[replica].N
-        pos, vel, acc = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
+        pos, vel, acc = (_out(a, (n, 3)) for a in (pos, vel, acc))
         self._ck(lib().p3m_get_state(self.handle, replica, dptr(pos), dptr(vel), dptr(acc)))
+        return pos, vel, acc
+
+    def set_state_all(self, pos=None, vel=None, acc=None, keep_lists=False):
+        """State of every replica from (sum N, 3) arrays in replica order.
+        keep_lists: keep the neighbour lists (continuing a trajectory)."""
+        n = sum(r.N for r in self.replicas)
+        self._ck(lib().p3m_set_state_all(self.handle,
+                                         dptr(None if pos is None else _f64(pos, (n, 3))),
+                                         dptr(None if vel is None else _f64(vel, (n, 3))),
+                                         dptr(None if acc is None else _f64(acc, (n, 3))),
+                                         int(bool(keep_lists))))
+
+    def get_state_all(self, pos=None, vel=None, acc=None):
+        """-> (pos, vel, acc) of every replica, (sum N, 3) in replica order."""
+        n = sum(r.N for r in self.replicas)
+        pos, vel, acc = (_out(a, (n, 3)) for a in (pos, vel, acc))
+        self._ck(lib().p3m_get_state_all(self.handle, dptr(pos), dptr(vel), dptr(acc)))
         return pos, vel, acc
 
     def init_forces(self):
