@@ -237,6 +237,19 @@ int p3m_get_energies(p3m_ctx *ctx, double *out, int max_steps, int *n_out);
  * interleaved (re,im) doubles. */
 int p3m_get_nqt(p3m_ctx *ctx, int replica, double *out, int max_steps, int *n_out);
 
+/* State snapshots for the output files of yukawa_MD_p3m_ord6.py:189-231
+ * (pos_vel_acc.out, .xyz): with interval > 0, every step `it` of p3m_run
+ * with (it + 1) % interval == 0 copies [pos | vel | acc] (n rows of 9) of
+ * every replica into a device ring of `capacity` snapshots, inside the step
+ * (no host round trip). interval 0 turns them off. Resets the ring. */
+int p3m_set_snapshots(p3m_ctx *ctx, int interval, int capacity);
+
+/* The snapshots taken since the last call, oldest first, at most max_snaps:
+ * out (n_out, sum of n, 9), replicas concatenated; steps (may be NULL)
+ * receives each one's step index. P3M_ESTATE if more than `capacity` were
+ * taken since the last call (the oldest were overwritten). */
+int p3m_get_snapshots(p3m_ctx *ctx, double *out, int *steps, int max_snaps, int *n_out);
+
 /* Last values of one replica (8 doubles): U_short, U_fft, U_self, U, K, T,
  * thermostat factor, and the number of neighbour-list rebuilds so far. */
 int p3m_get_replica_stats(p3m_ctx *ctx, int replica, double *out);

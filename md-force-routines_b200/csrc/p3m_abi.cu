@@ -20,7 +20,12 @@ struct p3m_ctx {
     std::vector<char> green_ready;
     DevState s;
     cudaStream_t st = nullptr;
-    int *counters = nullptr;      // [0] run step, [1] ring position, [2] it0
+    int *counters = nullptr;      // [0] run step, [1] ring position, [2] it0, [3] n(q,t) rows,
+                                  // [4] snapshots taken, [5] this step's snapshot slot
+    int snap_interval = 0, snap_cap = 0;
+    double *snap = nullptr;       // [cap][ntot][9] state snapshots
+    int *snap_steps = nullptr;    // [cap] step index of each snapshot
+    long long snap_read = 0;      // snapshots handed to the caller
     double *ring = nullptr;       // energies [cap][nrep][4]
     int ring_cap = 0;
     int ring_rows = 0;            // rows written (host-side tally)
@@ -198,7 +203,8 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
                     s.acc_pp, s.brick_key, s.brick_count, s.brick_start, s.brick_cursor,
                     s.brick_perm, s.brick_slot, s.brick_hist, s.tiles, s.spec, s.ek, s.green, s.efield,
                     s.acc_pm, s.twiddle, s.u_pp_part, s.u_pm_part, s.kin_part, s.rep_out,
-                    s.status, ctx->counters, ctx->ring, ctx->qmult, ctx->nqt_part,
+                    s.status, ctx->counters, ctx->ring, ctx->qmult, ctx->nqt_part, ctx->snap,
+                    ctx->snap_steps,
                     ctx->nqt_ring, ctx->scratch, ctx->ep, ctx->tmp_nq};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -453,7 +459,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(dalloc(&s.kin_part, (size_t)blk));
     CKC(dalloc(&s.rep_out, (size_t)8 * n_reps));
     CKC(dalloc(&s.status, 1));
-    CKC(dalloc(&ctx->counters, 4));
+    CKC(dalloc(&ctx->counters, 8));
     ctx->ring_cap = 8192;
     CKC(dalloc(&ctx->ring, (size_t)ctx->ring_cap * n_reps * 4));
     {
@@ -569,10 +575,15 @@ template <typename T> static void seq_step(p3m_ctx *ctx, int mode, int record_nq
                       ctx->nqt_ring, ctx->counters, ctx->nqt_cap, ctx->st);
         ctx->launches += 2;
     }
-    launch_step_reduce(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, ctx->st, rec);
+    launch_step_reduce(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, ctx->st, rec,
+                       ctx->snap_interval, ctx->snap_cap);
     ctx->launches++;
     if (mode == P3M_MODE_THERMOSTAT) {
         launch_scale_vel(s, ctx->st);
+        ctx->launches++;
+    }
+    if (ctx->snap_interval > 0) {  // after the thermostat's rescale: the step's final state
+        launch_snapshot(s, ctx->counters, ctx->snap, ctx->snap_steps, ctx->st);
         ctx->launches++;
     }
 }
@@ -1073,7 +1084,8 @@ template <typename T> static int do_run(p3m_ctx *ctx, int n_steps, int mode, int
             CK(cudaGraphLaunch(ctx->graph[gi][gr], ctx->st));
             // count the kernels the graph holds (same sequence as seq_step)
             ctx->launches = before + (long long)(11 + (s.has_mesh ? 4 + fft_kernel_count(s) : 0) + (gi ? 1 : 0) +
-                                                 ((gr && ctx->nq > 0) ? 2 : 0));
+                                                 ((gr && ctx->nq > 0) ? 2 : 0) +
+                                                 (ctx->snap_interval > 0 ? 1 : 0));
         } else {
             seq_step<T>(ctx, mode, rec);
         }
@@ -1107,10 +1119,13 @@ extern "C" int p3m_get_energies(p3m_ctx *ctx, double *out, int max_steps, int *n
     int n = total < ctx->ring_cap ? total : ctx->ring_cap;
     if (n > max_steps) n = max_steps;
     const size_t row = (size_t)ctx->nrep * 4;
-    for (int k = 0; k < n; ++k) {
-        const int step = total - n + k;
-        CK(cudaMemcpy(out + (size_t)k * row, ctx->ring + (size_t)(step % ctx->ring_cap) * row,
-                      sizeof(double) * row, cudaMemcpyDeviceToHost));
+    // rows total-n .. total-1 of the ring: at most two contiguous pieces
+    for (int k = 0; k < n;) {
+        const int slot = (total - n + k) % ctx->ring_cap;
+        const int len = std::min(n - k, ctx->ring_cap - slot);
+        CK(cudaMemcpy(out + (size_t)k * row, ctx->ring + (size_t)slot * row,
+                      sizeof(double) * row * len, cudaMemcpyDeviceToHost));
+        k += len;
     }
     *n_out = n;
     return P3M_OK;
@@ -1129,11 +1144,85 @@ extern "C" int p3m_get_nqt(p3m_ctx *ctx, int replica, double *out, int max_steps
     int n = total < ctx->nqt_cap ? total : ctx->nqt_cap;
     if (n > max_steps) n = max_steps;
     const size_t rowlen = (size_t)ctx->nq * 6;
-    for (int k = 0; k < n; ++k) {
-        const int step = total - n + k;
-        const double *src = ctx->nqt_ring + ((size_t)(step % ctx->nqt_cap) * ctx->nrep + replica) * rowlen;
-        CK(cudaMemcpy(out + (size_t)k * rowlen, src, sizeof(double) * rowlen, cudaMemcpyDeviceToHost));
+    // the replica's rows, strided by the ring's row of all replicas: at most
+    // two 2-D copies (the ring wraps once)
+    for (int k = 0; k < n;) {
+        const int slot = (total - n + k) % ctx->nqt_cap;
+        const int len = std::min(n - k, ctx->nqt_cap - slot);
+        const double *src = ctx->nqt_ring + ((size_t)slot * ctx->nrep + replica) * rowlen;
+        CK(cudaMemcpy2D(out + (size_t)k * rowlen, sizeof(double) * rowlen, src,
+                        sizeof(double) * rowlen * ctx->nrep, sizeof(double) * rowlen, len,
+                        cudaMemcpyDeviceToHost));
+        k += len;
     }
+    *n_out = n;
+    return P3M_OK;
+}
+
+extern "C" int p3m_set_snapshots(p3m_ctx *ctx, int interval, int capacity)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (interval < 0 || (interval > 0 && capacity < 1))
+        return fail(ctx, P3M_EARG, "p3m_set_snapshots", "interval must be >= 0 and capacity >= 1");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    // the step sequence changes: drop the captured graphs
+    for (auto &row : ctx->graph)
+        for (auto &g : row)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    if (capacity != ctx->snap_cap || interval == 0) {
+        cudaFree(ctx->snap);
+        cudaFree(ctx->snap_steps);
+        ctx->snap = nullptr;
+        ctx->snap_steps = nullptr;
+        ctx->snap_cap = 0;
+    }
+    ctx->snap_interval = 0;
+    if (interval > 0) {
+        if (!ctx->snap) {
+            CK(dalloc(&ctx->snap, (size_t)capacity * ctx->s.ntot * 9));
+            CK(dalloc(&ctx->snap_steps, (size_t)capacity));
+        }
+        ctx->snap_cap = capacity;
+        ctx->snap_interval = interval;
+    }
+    CK(cudaMemsetAsync(ctx->counters + 4, 0, 2 * sizeof(int), ctx->st));
+    ctx->snap_read = 0;
+    return finish(ctx);
+}
+
+extern "C" int p3m_get_snapshots(p3m_ctx *ctx, double *out, int *steps, int max_snaps, int *n_out)
+{
+    if (!ctx || !out || !n_out || max_snaps < 0)
+        return fail(ctx, P3M_EARG, "p3m_get_snapshots", "NULL argument");
+    *n_out = 0;
+    if (ctx->snap_cap == 0) return fail(ctx, P3M_EARG, "p3m_get_snapshots", "snapshots not configured");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    int taken = 0;
+    CK(cudaMemcpy(&taken, ctx->counters + 4, sizeof(int), cudaMemcpyDeviceToHost));
+    const long long avail = taken - ctx->snap_read;
+    if (avail > ctx->snap_cap) {
+        ctx->snap_read = taken;
+        return fail(ctx, P3M_ESTATE, "p3m_get_snapshots",
+                    "the snapshot ring overflowed: read it at least every capacity x interval steps");
+    }
+    const int n = (int)std::min<long long>(avail, max_snaps);
+    const size_t per = (size_t)ctx->s.ntot * 9;
+    for (int k = 0; k < n;) {
+        const int slot = (int)((ctx->snap_read + k) % ctx->snap_cap);
+        const int len = std::min(n - k, ctx->snap_cap - slot);
+        CK(cudaMemcpy(out + (size_t)k * per, ctx->snap + (size_t)slot * per,
+                      sizeof(double) * per * len, cudaMemcpyDeviceToHost));
+        if (steps)
+            CK(cudaMemcpy(steps + k, ctx->snap_steps + slot, sizeof(int) * len,
+                          cudaMemcpyDeviceToHost));
+        k += len;
+    }
+    ctx->snap_read += n;
     *n_out = n;
     return P3M_OK;
 }

@@ -126,11 +126,13 @@ k_kick_finish(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
 __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nblk,
                               const double *__restrict__ kin_part, double *__restrict__ rep_out,
                               int mode, int *__restrict__ counters, double *__restrict__ ring,
-                              int ring_cap, int recorded, int *rebuild, int *status)
+                              int ring_cap, int recorded, int snap_interval, int snap_cap,
+                              int *rebuild, int *status)
 {
     // counters: [0] steps since the run started, [1] energy-ring position,
     // [2] step index of the run's first step (thermostat_p3m_ord6.py:15 tests
-    // it <= 1999), [3] n(q,t) rows recorded
+    // it <= 1999), [3] n(q,t) rows recorded, [4] snapshots taken, [5] the
+    // snapshot slot this step writes (-1: none)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int it = counters[2] + counters[0];
     const int step = counters[1];
@@ -173,6 +175,14 @@ __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nbl
             counters[0] += 1;
             counters[1] = step + 1;
             if (recorded) counters[3] += 1;
+            // a snapshot after step `it` when (it + 1) % interval == 0, as the
+            // reference writes its files (yukawa_MD_p3m_ord6.py:222)
+            if (snap_interval > 0 && (it + 1) % snap_interval == 0) {
+                counters[5] = counters[4] % snap_cap;
+                counters[4] += 1;
+            } else {
+                counters[5] = -1;
+            }
         }
     }
     // this step's lists are built (count them); the next drift decides again
@@ -180,6 +190,28 @@ __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nbl
         if (rebuild[r] && mode != 2) rep_out[8 * r + RO_REBUILDS] += 1.0;
         rebuild[r] = 0;
     }
+}
+
+// The state after this step, [slot][particle][pos, vel, acc] (the rows of
+// yukawa_MD_p3m_ord6.py:223), into the slot k_step_reduce chose; steps[slot]
+// = the step index.
+__global__ void k_snapshot(const double *__restrict__ pos, const double *__restrict__ vel,
+                           const double *__restrict__ acc, int ntot,
+                           const int *__restrict__ counters, double *__restrict__ snap,
+                           int *__restrict__ steps)
+{
+    const int slot = counters[5];
+    if (slot < 0) return;
+    double *dst = snap + (long long)slot * ntot * 9;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            dst[9 * (long long)i + c] = pos[3 * (long long)i + c];
+            dst[9 * (long long)i + 3 + c] = vel[3 * (long long)i + c];
+            dst[9 * (long long)i + 6 + c] = acc[3 * (long long)i + c];
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) steps[slot] = counters[2] + counters[0] - 1;
 }
 
 __global__ void k_set_flags(int *flag, int n, int value)
@@ -461,10 +493,17 @@ void launch_kick_finish(const DevState &s, int do_kick, double *ep_out, cudaStre
 }
 
 void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring, int ring_cap,
-                        cudaStream_t st, int recorded)
+                        cudaStream_t st, int recorded, int snap_interval, int snap_cap)
 {
     k_step_reduce<<<1, 1024, 0, st>>>(s.reps, s.nrep, s.nblk, s.kin_part, s.rep_out, mode,
-                                      counters, ring, ring_cap, recorded, s.rebuild, s.status);
+                                      counters, ring, ring_cap, recorded, snap_interval, snap_cap,
+                                      s.rebuild, s.status);
+}
+
+void launch_snapshot(const DevState &s, const int *counters, double *snap, int *steps,
+                     cudaStream_t st)
+{
+    k_snapshot<<<pgrid(s.ntot), 256, 0, st>>>(s.pos, s.vel, s.acc, s.ntot, counters, snap, steps);
 }
 
 void launch_set_counters(int *counters, int run_step, int ring_pos, int it0, cudaStream_t st)

@@ -100,7 +100,10 @@ void launch_kick_drift(const DevState &s, cudaStream_t st);
 template <typename T> void launch_kick_finish(const DevState &s, int do_kick, double *ep_out,
                                               cudaStream_t st);
 void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring, int ring_cap,
-                        cudaStream_t st, int recorded = 0);
+                        cudaStream_t st, int recorded = 0, int snap_interval = 0,
+                        int snap_cap = 0);
+void launch_snapshot(const DevState &s, const int *counters, double *snap, int *steps,
+                     cudaStream_t st);
 void launch_set_counters(int *counters, int run_step, int ring_pos, int it0, cudaStream_t st);
 void launch_set_flags(int *flag, int n, int value, cudaStream_t st);
 void launch_scale_vel(const DevState &s, cudaStream_t st);

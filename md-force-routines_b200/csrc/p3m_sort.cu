@@ -190,22 +190,30 @@ k_brick_hist(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ 
     }
 }
 
-// One thread per brick: its counts over the replica's chunks become the
-// chunks' first slots (exclusive scan from brick_start).
+// One warp per brick: its counts over the replica's chunks become the
+// chunks' first slots (exclusive scan from brick_start), 32 chunks a pass.
 __global__ void k_brick_colscan(const RepDev *__restrict__ reps, int nrep,
                                 const int *__restrict__ brick_start, int *__restrict__ hist,
                                 int nbrick, int ch)
 {
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbrick; b += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int b = blockIdx.x * wpb + (threadIdx.x >> 5); b < nbrick; b += gridDim.x * wpb) {
         const RepDev &R = reps[find_rep(b, nrep, [&](int k) { return reps[k].brick_off; })];
         const int nbr = R.nb * R.nb * R.nb;
         const int nch = sort_chunks(R, ch);
         int *col = hist + R.sh_off + (b - R.brick_off);
-        int s = brick_start[b];
-        for (int cl = 0; cl < nch; ++cl) {
-            const int t = col[(long long)cl * nbr];
-            col[(long long)cl * nbr] = s;
-            s += t;
+        int carry = brick_start[b];
+        for (int c0 = 0; c0 < nch; c0 += 32) {
+            const int cl = c0 + lane;
+            const int t = cl < nch ? col[(long long)cl * nbr] : 0;
+            int x = t;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (cl < nch) col[(long long)cl * nbr] = carry + x - t;
+            carry += __shfl_sync(0xffffffffu, x, 31);
         }
     }
 }
@@ -283,7 +291,7 @@ void launch_sort_bricks(const DevState &s, cudaStream_t st)
     const size_t smem = (size_t)s.max_bricks * sizeof(int);
     k_brick_hist<<<grid_for(s.nchunk, 1), 256, smem, st>>>(s.reps, s.nrep, s.brick_key,
                                                             s.brick_hist, s.nchunk, s.sort_ch);
-    k_brick_colscan<<<grid_for(s.nbrick, 128), 128, 0, st>>>(s.reps, s.nrep, s.brick_start,
+    k_brick_colscan<<<grid_for(s.nbrick, 8), 256, 0, st>>>(s.reps, s.nrep, s.brick_start,
                                                               s.brick_hist, s.nbrick, s.sort_ch);
     k_brick_place<<<grid_for(s.nchunk, 1), 32, smem, st>>>(s.reps, s.nrep, s.brick_key,
                                                            s.brick_hist, s.brick_perm,

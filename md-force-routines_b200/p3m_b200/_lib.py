@@ -90,6 +90,8 @@ SIGNATURES = {
     "p3m_run": (_I, [_V, _I, _I, _I, _I, _I, _I]),
     "p3m_get_energies": (_I, [_V, _D, _I, ctypes.POINTER(_I)]),
     "p3m_get_nqt": (_I, [_V, _I, _D, _I, ctypes.POINTER(_I)]),
+    "p3m_set_snapshots": (_I, [_V, _I, _I]),
+    "p3m_get_snapshots": (_I, [_V, _D, ctypes.POINTER(ctypes.c_int), _I, ctypes.POINTER(ctypes.c_int)]),
     "p3m_check": (_I, [_V]),
     "p3m_sqw": (_I, [_V, ctypes.c_double, _I, _I, _I, _I, _D, _D]),
     "p3m_sqw_series": (_I, [_I, _D, _I, ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]),

@@ -72,6 +72,8 @@ class Context:
         self._h = h
         self._green_key = [None] * R
         self._nq = 0
+        self._nqt_cap = 0
+        self._snap_cap = 0
 
     # -- lifetime -------------------------------------------------------------
     @property
@@ -229,6 +231,7 @@ class Context:
     def set_nqt(self, qmult, capacity):
         qm = None if qmult is None or len(qmult) == 0 else _f64(qmult)
         self._nq = 0 if qm is None else len(qm)
+        self._nqt_cap = int(capacity)
         self._ck(lib().p3m_set_nqt(self.handle, dptr(qm), 0 if qm is None else len(qm),
                                    int(capacity)))
 
@@ -248,12 +251,35 @@ class Context:
         self._ck(lib().p3m_get_energies(self.handle, dptr(out), cap, ctypes.byref(n)))
         return out[: n.value]
 
-    def get_nqt(self, replica, nq, max_steps=1 << 16):
+    def get_nqt(self, replica, nq, max_steps=None):
+        """The recorded n(q,t) rows of one replica, oldest first: (steps, nq, 3)
+        complex."""
+        if max_steps is None:
+            max_steps = max(1, self._nqt_cap)
         out = np.empty((max_steps, nq, 3, 2))
         n = ctypes.c_int()
         self._ck(lib().p3m_get_nqt(self.handle, replica, dptr(out), max_steps, ctypes.byref(n)))
         o = out[: n.value]
         return o[..., 0] + 1j * o[..., 1]
+
+    def set_snapshots(self, interval, capacity=64):
+        """Copy [pos | vel | acc] of every replica into a device ring after
+        each step it of run() with (it + 1) % interval == 0 (0: off)."""
+        self._ck(lib().p3m_set_snapshots(self.handle, int(interval), int(capacity)))
+        self._snap_cap = int(capacity) if interval > 0 else 0
+
+    def get_snapshots(self, max_snaps=None):
+        """The snapshots taken since the last call, oldest first ->
+        (array (n, sum N, 9), step indices (n,))."""
+        ntot = sum(r.N for r in self.replicas)
+        m = self._snap_cap if max_snaps is None else int(max_snaps)
+        out = np.empty((max(m, 1), ntot, 9))
+        steps = np.empty(max(m, 1), dtype=np.int32)
+        n = ctypes.c_int()
+        self._ck(lib().p3m_get_snapshots(self.handle, dptr(out),
+                                         steps.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), m,
+                                         ctypes.byref(n)))
+        return out[: n.value], steps[: n.value]
 
     def sqw(self, dt, nt, col0=0, col_stride=1, ncols=None, per_replica=False):
         """S(q,w) of the last nt recorded n(q,t) rows, averaged over axes and
