@@ -128,7 +128,7 @@ static void pair_g_psi(double r, double kappa, double a, double *g, double *psi)
 }
 
 // Cubic per interval through the samples at u = 0, 1/3, 2/3, 1 (monomial
-// coefficients in u), for g and psi: 2 float4 per interval.
+// coefficients in u): PP_TABLE_N float4 for g, then PP_TABLE_N for psi.
 static void build_pp_table(const p3m_replica_desc &d, float4 *out)
 {
     const double h = d.rc / PP_TABLE_N;
@@ -141,8 +141,8 @@ static void build_pp_table(const p3m_replica_desc &d, float4 *out)
             c.z = (float)((18.0 * f[0] - 45.0 * f[1] + 36.0 * f[2] - 9.0 * f[3]) / 2.0);
             c.w = (float)((-9.0 * f[0] + 27.0 * f[1] - 27.0 * f[2] + 9.0 * f[3]) / 2.0);
         };
-        coef(fg, out[2 * i]);
-        coef(fp, out[2 * i + 1]);
+        coef(fg, out[i]);
+        coef(fp, out[PP_TABLE_N + i]);
     }
 }
 

@@ -217,8 +217,10 @@ __device__ __forceinline__ void pair_direct(double r2, const RepDev &R, double &
     f_over_r = fr * rinv;
 }
 
-// FP32: tabulated g and psi; tab holds 2 float4 (cubic coefficients in the
-// interval coordinate u in [0,1)) per interval.
+// FP32: tabulated g and psi; tab holds the cubic coefficients (in the
+// interval coordinate u in [0,1)) of g for every interval, then those of psi:
+// float4 slots i and PP_TABLE_N + i. (Interleaving them would put every g
+// read on an even slot, half of shared memory's eight 16-byte bank groups.)
 __device__ __forceinline__ void pair_table(float r2, const float4 *__restrict__ tab, float inv_h,
                                            float &f_over_r, float &phi)
 {
@@ -230,7 +232,7 @@ __device__ __forceinline__ void pair_table(float r2, const float4 *__restrict__ 
     const float tb = (t - 0.5f) + 12582912.0f;
     const int i = min(__float_as_int(tb) - 0x4B400000, PP_TABLE_N - 1);
     const float u = t - (tb - 12582912.0f);
-    const float4 cg = tab[2 * i], cp = tab[2 * i + 1];
+    const float4 cg = tab[i], cp = tab[PP_TABLE_N + i];
     const float g = fmaf(fmaf(fmaf(cg.w, u, cg.z), u, cg.y), u, cg.x);
     const float ps = fmaf(fmaf(fmaf(cp.w, u, cp.z), u, cp.y), u, cp.x);
     const float rinv2 = rinv * rinv;
