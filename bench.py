@@ -146,6 +146,29 @@ def working_set_mb(reps):
     return b / 1e6
 
 
+def rank_first_seed(rank, n_replicas):
+    """Seeds of rank r's ensemble: 1 + r R .. (r + 1) R (disjoint over ranks)."""
+    return 1 + rank * n_replicas
+
+
+def max_over_ranks(x, world, device):
+    """The largest x over all ranks (every rank calls it, in the same order)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(n_part_per_rank, steps, world, ms_max):
+    """Whole-job particle-steps/s: every rank's particles over the slowest
+    rank's time (weak scaling: each rank has the same work)."""
+    return n_part_per_rank * steps * world / (ms_max * 1e-3)
+
+
 def dist_setup(backend):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -267,7 +290,7 @@ def run_ours(args):
     from p3m_b200 import FP32, MODE_NVE, MODE_THERMOSTAT, Context
     from p3m_b200.configs import CFG3_QMULT, cfg3
 
-    reps = cfg3(args.replicas, first_seed=1 + rank * args.replicas)
+    reps = cfg3(args.replicas, first_seed=rank_first_seed(rank, args.replicas))
     states = initial_states(reps)
     ctx = Context(reps, precision=FP32, device=local)
     for i, (p, v) in enumerate(states):
@@ -315,14 +338,9 @@ def run_ours(args):
     barrier()
     clocks = sampler.stop()
     ctx.check()
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, "cuda")
     n_part = sum(r.N for r in reps)
-    value = n_part * args.steps * world / (ms * 1e-3)
+    value = job_value(n_part, args.steps, world, ms)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
