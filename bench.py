@@ -43,6 +43,14 @@ METRIC = "particle-steps/s on 1 B200: batched FP32 vs plain FP64 P3M at force er
 UNIT = "particle-steps/s"
 WORKLOAD = ("cfg3 ensemble: 20 replicas x N=1e4, Gamma=100, kappa=2, 64^3 mesh, p=6, "
             "alpha=0.6, rc=6, dt=0.1, NVE steps with n(q,t) (32 q x 3 axes)")
+WORKLOADS_TEXT = {
+    "cfg1": "cfg1: 1 replica N=1e4, Gamma=100, kappa=2, 64^3 mesh, p=6, alpha=0.6, rc=6, dt=0.1",
+    "cfg2": "cfg2: 1 replica N=1e5, Gamma=50, kappa=1, 128^3 mesh, p=6, alpha=0.5, rc=7, dt=0.1",
+    "cfg3": WORKLOAD,
+    "cfg4": ("cfg4: 64 uneven replicas (seeds 100-163; N 2031-48336, Gamma 10-198, kappa 0.50-2.92; "
+             "M in {32,64,128}, alpha, rc picked for 1e-6 RMS force error), dt=0.1"),
+    "cfg5": "cfg5: 1 replica N=1e6, Gamma=100, kappa=2, 256^3 mesh, p=6, alpha=0.6, rc=6, dt=0.1",
+}
 FLOP_PER_PAIR = 48  # fixed convention for the PP roofline (unique pairs)
 
 
@@ -52,9 +60,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--replicas", type=int, default=20)
+    ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS_TEXT),
+                    help="the configuration to time (default: the 20-replica ensemble)")
+    ap.add_argument("--replicas", type=int, default=20, help="cfg3's ensemble size")
     ap.add_argument("--equil", type=int, default=300,
                     help="untimed thermostat steps before the NVE warm-up")
+    ap.add_argument("--quench", type=int, default=200,
+                    help="thermostat steps at T_desired/100 before --equil (damps the runaway "
+                         "particles that random initial positions launch)")
     ap.add_argument("--no-tune", action="store_true", help="skip the PP autotuner")
     ap.add_argument("--pp-config", default=None, metavar="TPI,SKIN",
                     help="set threads per particle and Verlet skin instead of autotuning")
@@ -163,6 +176,19 @@ def max_over_ranks(x, world, device):
     return float(t.item())
 
 
+def workload_replicas(name, n_replicas, rank):
+    """The replicas rank `rank` runs: cfg3's ensemble with the rank's seeds,
+    or the named configuration with its seeds shifted by 1000 per rank."""
+    import dataclasses
+
+    from p3m_b200.configs import WORKLOADS, cfg3
+
+    if name == "cfg3":
+        return cfg3(n_replicas, first_seed=rank_first_seed(rank, n_replicas))
+    reps = WORKLOADS[name]()
+    return [dataclasses.replace(r, seed=r.seed + 1000 * rank) for r in reps]
+
+
 def job_value(n_part_per_rank, steps, world, ms_max):
     """Whole-job particle-steps/s: every rank's particles over the slowest
     rank's time (weak scaling: each rank has the same work)."""
@@ -196,6 +222,9 @@ def _ref_worker(args):
     if idx not in _REF_STATE:
         N, L, kappa, alpha, rc, M, dt, Gamma, seed = params
         P = O.Params(N, kappa, alpha, rc, M, L=L, Gamma=Gamma, dt=dt)
+        if G is None:
+            h = L / M
+            G = O.gf_opt(kappa, alpha, 6, 3, 3, 3, M, M, M, h, h, h, L, L, L)[0]
         mid = M // 2
         kv = 2 * np.pi * (np.arange(M) - mid) / L
         P._gk = (G, kv.reshape(1, M), kv.reshape(M, 1), kv.reshape(M, 1, 1), 0.0)
@@ -219,21 +248,23 @@ def run_reference(args):
     import multiprocessing as mp
 
     from oracle import oracle as O
-    from p3m_b200.configs import cfg3
 
     O.build()
-    reps = cfg3(args.replicas)
+    reps = workload_replicas(args.workload, args.replicas, 0)
     r0 = reps[0]
-    h = r0.L / r0.M
-    G, _, _, _, _ = O.gf_opt(r0.kappa, r0.alpha, 6, 3, 3, 3, r0.M, r0.M, r0.M, h, h, h,
-                             r0.L, r0.L, r0.L)
+    G = None  # each worker computes its replica's influence function ...
+    if all((r.kappa, r.alpha, r.M, r.L) == (r0.kappa, r0.alpha, r0.M, r0.L) for r in reps):
+        h = r0.L / r0.M  # ... unless all replicas share one
+        G, _, _, _, _ = O.gf_opt(r0.kappa, r0.alpha, 6, 3, 3, 3, r0.M, r0.M, r0.M, h, h, h,
+                                 r0.L, r0.L, r0.L)
     cores = os.cpu_count() or 1
     nproc = min(len(reps), cores)
     params = [(r.N, r.L, r.kappa, r.alpha, r.rc, r.M, r.dt, 1.0 / r.T_desired, r.seed) for r in reps]
     # bounded sample: each step of this arm is one NVE step of every replica;
     # cap the steps so the arm ends within a few minutes
-    steps = max(1, min(args.steps, 10))
-    warm = max(1, min(args.warmup, 2))
+    big = max(r.N for r in reps) > 2 * 10 ** 5
+    steps = max(1, min(args.steps, 1 if big else 10))
+    warm = max(1, min(args.warmup, 1 if big else 2))
     ctx = mp.get_context("spawn")
     with ctx.Pool(nproc) as pool:
         # pin replicas to workers: one task per replica per phase
@@ -243,13 +274,14 @@ def run_reference(args):
         wall = time.perf_counter() - t0
     total = sum(r.N for r in reps) * steps
     value = total / wall
-    sample = (f"{len(reps)} replicas x N=1e4 (64^3) advanced {steps} NVE steps each by the oracle "
-              f"port (C PP + numpy FFT/PM) in {nproc} spawned processes; wall {wall:.2f} s")
+    sample = (f"{len(reps)} replicas ({args.workload}) advanced {steps} NVE steps each by the "
+              f"oracle port (C PP + numpy FFT/PM) in {nproc} spawned processes; wall {wall:.2f} s")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
             "steps": steps, "warmup": warm, "ms_per_step": 1e3 * wall / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded initialize_pos_vel states)",
-            "config": {"workload": WORKLOAD, "replicas": len(reps), "parallelism": "replicas"},
+            "config": {"workload": WORKLOADS_TEXT[args.workload], "replicas": len(reps),
+                       "parallelism": "replicas"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -260,9 +292,12 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def cpu_baseline_port(rep, G, n_steps=4):
+def cpu_baseline_port(rep, G, n_steps=None):
     """The oracle port on one core for replica `rep` (bounded sample)."""
     from oracle import oracle as O
+
+    if n_steps is None:
+        n_steps = 1 if rep.N > 2 * 10 ** 5 else 4
 
     M = rep.M
     P = O.Params(rep.N, rep.kappa, rep.alpha, rep.rc, M, L=rep.L, Gamma=1.0 / rep.T_desired,
@@ -288,9 +323,9 @@ def run_ours(args):
     world, rank, local = dist_setup("nccl")
     torch.cuda.set_device(local)
     from p3m_b200 import FP32, MODE_NVE, MODE_THERMOSTAT, Context
-    from p3m_b200.configs import CFG3_QMULT, cfg3
+    from p3m_b200.configs import CFG3_QMULT
 
-    reps = cfg3(args.replicas, first_seed=rank_first_seed(rank, args.replicas))
+    reps = workload_replicas(args.workload, args.replicas, rank)
     states = initial_states(reps)
     ctx = Context(reps, precision=FP32, device=local)
     for i, (p, v) in enumerate(states):
@@ -301,7 +336,7 @@ def run_ours(args):
 
     # equilibration with the reference's thermostat (thermostat_p3m_ord6.vscale)
     # from the random initial state, then NVE warm-up (also builds the graph)
-    ctx.run(args.equil, MODE_THERMOSTAT, it0=0, graph=True)
+    ctx.equilibrate(args.equil, quench_steps=args.quench)
     tuned = None
     if args.pp_config:
         tpi, skin = args.pp_config.split(",")
@@ -346,8 +381,9 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded initialize_pos_vel: uniform positions, Maxwell-Boltzmann "
                     "velocities)",
-            "config": {"workload": WORKLOAD, "replicas": len(reps), "N_per_replica": reps[0].N,
-                       "mesh": reps[0].M, "parallelism": f"replicas x{world}" if world > 1 else "replicas",
+            "config": {"workload": WORKLOADS_TEXT[args.workload], "replicas": len(reps),
+                       "N_per_replica": reps[0].N if len({r.N for r in reps}) == 1 else "varies",
+                       "mesh": reps[0].M if len({r.M for r in reps}) == 1 else "varies", "parallelism": f"replicas x{world}" if world > 1 else "replicas",
                        "l2": (f"inputs larger than L2 (working set {working_set_mb(reps):.0f} MB > 126 MB)"
                               if working_set_mb(reps) > 126 else
                               f"working set {working_set_mb(reps):.0f} MB fits L2; no flush"),
@@ -393,7 +429,8 @@ def extras(args, line, ctx, reps, states, device):
     tpath = os.path.join(ROOT, "profiles", "pp_traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get("cfg3_bytes_per_launch")
+            traffic = (json.load(open(tpath)).get("cfg3_bytes_per_launch")
+                       if args.workload == "cfg3" else None)
         except Exception:
             traffic = None
     achieved = flop / (pp_ms * 1e-3) / 1e12 if pp_ms > 0 else None

@@ -190,6 +190,10 @@ int p3m_set_state(p3m_ctx *ctx, int replica, const double *pos, const double *ve
                   const double *acc);
 int p3m_get_state(p3m_ctx *ctx, int replica, double *pos, double *vel, double *acc);
 
+/* New thermostat targets T_desired (one per replica, > 0) for the following
+ * p3m_run calls in thermostat mode (thermostat_p3m_ord6.py:5 T_desired). */
+int p3m_set_t_desired(p3m_ctx *ctx, const double *t_desired);
+
 /* The same for every replica at once: (sum of n, 3) arrays, replicas
  * concatenated in order, one copy per array (host buffers may be pinned).
  * p3m_set_state marks the replica's neighbour lists for a rebuild; with

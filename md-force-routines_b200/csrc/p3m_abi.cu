@@ -1731,3 +1731,20 @@ extern "C" int p3m_pm_error(int device, int count, const double *n, const double
     }
     return P3M_OK;
 }
+
+extern "C" int p3m_set_t_desired(p3m_ctx *ctx, const double *t_desired)
+{
+    if (!ctx || !t_desired) return fail(ctx, P3M_EARG, "p3m_set_t_desired", "NULL argument");
+    for (int r = 0; r < ctx->nrep; ++r)
+        if (!(t_desired[r] > 0.0) || !(t_desired[r] < 1e300))
+            return fail(ctx, P3M_EARG, "p3m_set_t_desired", "temperatures must be finite and > 0");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int r = 0; r < ctx->nrep; ++r) {
+        ctx->desc[r].t_desired = t_desired[r];
+        ctx->rh[r].t_desired = t_desired[r];
+    }
+    // the step graphs read the replica table from device memory: no recapture
+    CK(cudaMemcpy(ctx->s.reps, ctx->rh.data(), sizeof(RepDev) * ctx->nrep, cudaMemcpyHostToDevice));
+    return P3M_OK;
+}

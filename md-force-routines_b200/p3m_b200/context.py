@@ -225,6 +225,31 @@ class Context:
         self._ck(lib().p3m_get_state_all(self.handle, dptr(pos), dptr(vel), dptr(acc)))
         return pos, vel, acc
 
+    def set_t_desired(self, t_desired):
+        """Thermostat targets for the following thermostat-mode runs: one
+        value per replica, or one for all."""
+        t = np.broadcast_to(np.asarray(t_desired, dtype=np.float64), (len(self.replicas),)).copy()
+        self._ck(lib().p3m_set_t_desired(self.handle, dptr(t)))
+
+    def equilibrate(self, steps, quench_steps=200, quench_factor=0.01):
+        """Thermostat phase from seeded random positions: `quench_steps` of
+        the reference's thermostat at quench_factor * T_desired, then `steps`
+        at T_desired. Uniformly random initial positions leave close pairs
+        whose repulsion launches a few particles at tens of times the thermal
+        speed; in weakly coupled, strongly screened replicas the reference's
+        rescaling alone does not slow them within thousands of steps (their
+        collisions weaken as the speed grows), and at dt = 0.1 they heat the
+        system. The quench damps them with everything else."""
+        td = np.array([r.T_desired for r in self.replicas])
+        if quench_steps > 0:
+            self.set_t_desired(td * quench_factor)
+            try:
+                self.run(quench_steps, MODE_THERMOSTAT, it0=0)
+            finally:
+                self.set_t_desired(td)
+        if steps > 0:
+            self.run(steps, MODE_THERMOSTAT, it0=0)
+
     def init_forces(self):
         self._ck(lib().p3m_init_forces(self.handle))
 

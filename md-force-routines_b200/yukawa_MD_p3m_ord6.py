@@ -58,6 +58,9 @@ def parse(argv):
     ap.add_argument("--mesh", type=int, default=MESH)
     ap.add_argument("--tol", type=float, default=None,
                     help="choose alpha, r_c and the mesh for this RMS force error instead")
+    ap.add_argument("--quench", type=int, default=0,
+                    help="thermostat steps at T_desired/100 before the equilibration (not in the "
+                         "reference; damps runaway particles of random starts)")
     ap.add_argument("--chunk", type=int, default=1000, help="steps per launch batch")
     ap.add_argument("--quiet", action="store_true", help="no per-step lines on stdout")
     return ap.parse_args(argv)
@@ -124,6 +127,8 @@ def run(argv=None):
         say("\n------------- Equilibration -------------")
         say("time - temperature")
         chunk = max(1, min(a.chunk, 8192))
+        if a.quench > 0:
+            ctx.equilibrate(0, quench_steps=a.quench)
         for k0 in range(0, Neq, chunk):
             k = min(chunk, Neq - k0)
             ctx.run(k, MODE_THERMOSTAT, it0=k0)

@@ -283,3 +283,34 @@ def test_state_all_round_trip_and_kept_lists():
         b.run(5, MODE_NVE)
         for x, y in zip(a.get_state_all(), b.get_state_all()):
             assert np.array_equal(x, y)
+
+
+def test_set_t_desired_and_quench():
+    """The thermostat follows p3m_set_t_desired; the quench + thermostat
+    equilibration leaves a hot, strongly screened replica of the uneven
+    ensemble (the cfg4 draw of seed 163) with a thermal velocity tail and a
+    conserved energy, where the reference's thermostat alone leaves runaway
+    particles from the random start."""
+    from p3m_b200 import FP32, MODE_NVE, MODE_THERMOSTAT, Context, Replica
+    from p3m_b200.configs import box, cfg4_system
+
+    N, Gamma, kappa = cfg4_system(163)
+    r = Replica(N=N, L=box(N), kappa=kappa, alpha=0.54, rc=5.96, M=64, dt=0.1,
+                T_desired=1.0 / Gamma, seed=163)
+    pos, vel = _init_state(r, 163)
+    with Context(r, precision=FP32) as c:
+        c.set_state(0, pos, vel)
+        c.init_forces()
+        c.set_t_desired(2.0 * r.T_desired)
+        c.run(20, MODE_THERMOSTAT)
+        v = c.get_state(0)[1]
+        assert abs(np.sum(v ** 2) / N / (2.0 * r.T_desired) - 1.0) < 1e-9  # rescaled to 2 T_d
+        c.set_t_desired(r.T_desired)
+        c.equilibrate(300)
+        v = c.get_state(0)[1]
+        vm = np.sqrt(np.sum(v ** 2, axis=1))
+        assert vm.max() / np.sqrt(np.mean(vm ** 2)) < 6.0
+        c.run(300, MODE_NVE)
+        e = c.energies(max_steps=300)
+        E = e[:, 0, 0] + e[:, 0, 1]
+        assert np.max(np.abs(E - E[0])) / e[-1, 0, 1] < 1e-3
