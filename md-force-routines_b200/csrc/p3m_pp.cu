@@ -98,14 +98,18 @@ __device__ __forceinline__ long long list_index(int s, int k, int maxnb)
 // list build (rebuild steps only)
 // ---------------------------------------------------------------------------
 constexpr int LB_THREADS = 256;
-constexpr int LB_TPI = 2;  // threads per particle: they scan alternate candidates
+constexpr int LB_TPI = 8;                     // lanes per particle
+constexpr int LB_PPB = LB_THREADS / LB_TPI;   // particles per pass
+constexpr int LB_ITEMS = 4;                   // work items per cell
 template <typename T> __host__ __device__ constexpr int lb_scap() { return sizeof(T) == 4 ? 3072 : 1536; }
 
-// One CTA per cell. The 27 neighbour cells' coordinates are staged in shared
-// memory; thread `sub` of a particle's pair keeps the in-range candidates
-// with index = sub (mod 2) and writes its t-th one to list slot 2t + sub.
-// The shorter half is padded with the particle's own index, which the force
-// kernel skips (r = 0), so the list order is fixed and needs no merge.
+// Work item (cell, c): the cell's home particles c*32 + 128 k + [0, 32), so a
+// cell's particles spread over four CTAs (a rebuild of a few replicas keeps
+// the GPU busy). The 27 neighbour cells' coordinates are staged in shared
+// memory in the fixed stencil order; the 8 lanes of a particle test 8
+// consecutive candidates per round, and a warp ballot gives each candidate
+// in range its place: the list holds the in-range candidates in stencil
+// order, as a scan by one thread would, with no padding.
 template <typename T>
 __global__ void __launch_bounds__(LB_THREADS)
 k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
@@ -119,16 +123,19 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
     Q *stage = reinterpret_cast<Q *>(lb_smem);
     __shared__ int pre[28];
     __shared__ int nstart[27];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int sub = tid % LB_TPI;
-    const int half_cap = maxnb / LB_TPI;
-    for (int hc = blockIdx.x; hc < ncell; hc += gridDim.x) {
+    const int gshift = lane & ~(LB_TPI - 1);            // first lane of this particle's group
+    const unsigned below = (1u << (lane & (LB_TPI - 1))) - 1u;
+    for (int item = blockIdx.x; item < ncell * LB_ITEMS; item += gridDim.x) {
+        const int hc = item / LB_ITEMS, part = item % LB_ITEMS;
         const int r = find_rep(hc, nrep, [&](int k) { return reps[k].cell_off; });
         if (!rebuild[r]) continue;  // uniform over the block
+        const int hstart = cell_start[hc], nhome = cell_start[hc + 1] - hstart;
+        if (part * LB_PPB >= nhome) continue;
         const RepDev &R = reps[r];
         const int nc = R.nc, local = hc - R.cell_off;
         const int cx = local % nc, cy = (local / nc) % nc, cz = local / (nc * nc);
-        const int hstart = cell_start[hc], nhome = cell_start[hc + 1] - hstart;
         const float sc = (float)(R.L / Coord<T>::scale);
         const float rl2 = (float)(R.rcl * R.rcl);
         __syncthreads();
@@ -146,7 +153,7 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
         }
         __syncthreads();
         const int total = pre[27];
-        for (int i0 = 0; i0 < nhome; i0 += LB_THREADS / LB_TPI) {
+        for (int i0 = part * LB_PPB; i0 < nhome; i0 += LB_ITEMS * LB_PPB) {
             const int i = i0 + tid / LB_TPI;
             const bool have = i < nhome;
             const int s = hstart + i;
@@ -166,31 +173,29 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                     stage[k] = q;
                 }
                 __syncthreads();
-                if (have) {
-                    for (int k = sub; k < wlen; k += LB_TPI) {
+                for (int kb = 0; kb < wlen; kb += LB_TPI) {  // uniform over the block
+                    const int k = kb + sub;
+                    bool in = false;
+                    int j = 0;
+                    if (have && k < wlen) {
                         const Q q = stage[k];
                         const float dx = (float)qdiff<T>(xi.x, q.x) * sc;
                         const float dy = (float)qdiff<T>(xi.y, q.y) * sc;
                         const float dz = (float)qdiff<T>(xi.z, q.z) * sc;
-                        const float r2 = dx * dx + dy * dy + dz * dz;
-                        if (r2 < rl2 && (int)q.w != s) {
-                            if (cnt < half_cap)
-                                nlist[list_index(s, LB_TPI * cnt + sub, maxnb)] = (int)q.w;
-                            ++cnt;
-                        }
+                        j = (int)q.w;
+                        in = (dx * dx + dy * dy + dz * dz < rl2) && j != s;
                     }
+                    const unsigned grp = (__ballot_sync(0xffffffffu, in) >> gshift) & 0xffu;
+                    if (in) {
+                        const int pos = cnt + __popc(grp & below);
+                        if (pos < maxnb) nlist[list_index(s, pos, maxnb)] = j;
+                    }
+                    cnt += __popc(grp);
                 }
             }
-            // pad the shorter half with the particle itself (skipped as r = 0)
-            const int other = __shfl_xor_sync(0xffffffffu, cnt, 1);
-            int m = max(cnt, other);
-            if (m > half_cap) {
-                if (have && sub == 0) raise_status(status, ST_NBOVF);
-                m = half_cap;
-            }
-            if (have) {
-                for (int t = cnt; t < m; ++t) nlist[list_index(s, LB_TPI * t + sub, maxnb)] = s;
-                if (sub == 0) nnb[s] = LB_TPI * m;
+            if (have && sub == 0) {
+                if (cnt > maxnb) raise_status(status, ST_NBOVF);
+                nnb[s] = min(cnt, maxnb);
             }
         }
     }
@@ -391,7 +396,8 @@ template <typename T> void launch_quantize(const DevState &s, cudaStream_t st)
 template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st)
 {
     using Q = typename Coord<T>::Q;
-    const int grid = s.ncell < 148 * 16 ? s.ncell : 148 * 16;
+    const int items = s.ncell * LB_ITEMS;
+    const int grid = items < 148 * 8 ? items : 148 * 8;
     k_build_lists<T><<<grid, LB_THREADS, lb_scap<T>() * sizeof(Q), st>>>(
         s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.ncell,
         s.rebuild, s.status);
