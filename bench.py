@@ -480,34 +480,57 @@ def extras(args, line, ctx, reps, states, device):
 
     # -- end to end through the C ABI with host buffers ----------------------------
     # per step: H2D of the whole ensemble's (pos, vel, acc) from pinned host
-    # memory, one batched step, D2H of the state and of the step's energies
+    # memory, one step, D2H of the state and of the step's energies. An
+    # ensemble of several replicas is held as up to four contexts on their
+    # own streams with asynchronous copies, so one part's copies overlap the
+    # others' steps (the copy engines and the SMs work at the same time).
     ntot = sum(r.N for r in reps)
-    host = [torch.empty((ntot, 3), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
-    host[0][:] = np.concatenate([st[0] for st in states])
-    host[1][:] = np.concatenate([st[1] for st in states])
-    with Context(reps, precision=FP32, device=device) as c:
-        c.set_state_all(host[0], host[1])
-        c.init_forces()
-        c.get_state_all(*host)
-        c.run(2, MODE_NVE, graph=True)
-        c.get_state_all(*host)
+    nparts = min(4, len(reps))
+    cuts = [round(k * len(reps) / nparts) for k in range(nparts + 1)]
+    halves = [reps[cuts[k]:cuts[k + 1]] for k in range(nparts)]
+    offs = np.cumsum([0] + [sum(r.N for r in h) for h in halves])
+    pos_all = np.concatenate([st[0] for st in states])
+    vel_all = np.concatenate([st[1] for st in states])
+    host = []
+    for k in range(len(halves)):
+        n = int(offs[k + 1] - offs[k])
+        hb = [torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+        hb[0][:] = pos_all[offs[k]:offs[k + 1]]
+        hb[1][:] = vel_all[offs[k]:offs[k + 1]]
+        host.append(hb)
+    ctxs = [Context(h, precision=FP32, device=device) for h in halves]
+    try:
+        for c, hb in zip(ctxs, host):
+            c.set_state_all(hb[0], hb[1])
+            c.init_forces()
+            c.get_state_all(*hb)
+            c.run(2, MODE_NVE, graph=True)
+            c.get_state_all(*hb)
         n_e2e = min(args.steps, 200)
-        s = torch.cuda.ExternalStream(c.stream())
+        s = torch.cuda.ExternalStream(ctxs[0].stream())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
         for _ in range(n_e2e):
-            c.set_state_all(*host, keep_lists=True)
-            c.run(1, MODE_NVE, graph=True)
-            c.get_state_all(*host)
-            c.energies(max_steps=1)
-        e1.record(s)
+            for c, hb in zip(ctxs, host):
+                c.set_state_all(*hb, keep_lists=True, sync=False)
+                c.run(1, MODE_NVE, graph=True, sync=False)
+                c.get_state_all(*hb, sync=False)
+            for c in ctxs:
+                c.sync()
+                c.energies(max_steps=1)
+        e1.record(s)  # after both contexts' work: the host synchronised on both
         e1.synchronize()
         t = e0.elapsed_time(e1) * 1e-3
+    finally:
+        for c in ctxs:
+            c.close()
     nb = ntot * 3 * 8
     line["e2e"] = {"value": ntot * n_e2e / t, "unit": UNIT,
                    "h2d_bytes_per_step": 3 * nb, "d2h_bytes_per_step": 3 * nb + 4 * 8 * len(reps),
-                   "how": "p3m_set_state_all (pinned host -> device, lists kept), p3m_run(1), "
-                          "p3m_get_state_all and p3m_get_energies per step"}
+                   "how": ("p3m_set_state_all_async (pinned host -> device, lists kept), "
+                           "p3m_run(1, sync=0), p3m_get_state_all_async per step on each of "
+                           f"{len(halves)} contexts (its own stream), then p3m_sync and "
+                           "p3m_get_energies")}
 
     # -- CPU baseline: the oracle port on one host core ------------------------------
     G, _ = gf_opt_device(r0.kappa, r0.alpha, 6, 3, r0.M, r0.L, device=device)

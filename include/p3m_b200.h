@@ -205,6 +205,16 @@ int p3m_set_state_all(p3m_ctx *ctx, const double *pos, const double *vel, const 
                       int keep_lists);
 int p3m_get_state_all(p3m_ctx *ctx, double *pos, double *vel, double *acc);
 
+/* The same copies queued on the context's stream without waiting for them
+ * (with p3m_run(..., sync = 0) they let a caller keep one context's copies
+ * in flight while another context computes). The host arrays must stay
+ * valid, and unread or unchanged, until p3m_sync(ctx) returns; the copy
+ * engines reach full speed only from pinned host memory. Errors surface at
+ * p3m_sync / p3m_check. */
+int p3m_set_state_all_async(p3m_ctx *ctx, const double *pos, const double *vel, const double *acc,
+                            int keep_lists);
+int p3m_get_state_all_async(p3m_ctx *ctx, double *pos, double *vel, double *acc);
+
 /* Compute acc for the uploaded positions of all replicas (the driver's
  * initial force call, yukawa_MD_p3m_ord6.py:171). */
 int p3m_init_forces(p3m_ctx *ctx);
@@ -262,7 +272,9 @@ int p3m_get_replica_stats(p3m_ctx *ctx, int replica, double *out);
  * error seen by a kernel), then cleared. Synchronises the stream. */
 int p3m_check(p3m_ctx *ctx);
 
-/* Wait for all work on the context's stream. */
+/* Wait for all work on the context's stream; then, like p3m_check, report
+ * a device status (out-of-box particle, non-finite force, list overflow)
+ * raised by that work. */
 int p3m_sync(p3m_ctx *ctx);
 
 /* PP configuration: threads per particle in the force kernel (1, 2, 4, 8)

@@ -987,8 +987,8 @@ extern "C" int p3m_get_state(p3m_ctx *ctx, int replica, double *pos, double *vel
     return finish(ctx);
 }
 
-extern "C" int p3m_set_state_all(p3m_ctx *ctx, const double *pos, const double *vel,
-                                 const double *acc, int keep_lists)
+static int set_state_all(p3m_ctx *ctx, const double *pos, const double *vel, const double *acc,
+                         int keep_lists, bool sync)
 {
     if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
     CK(cudaSetDevice(ctx->device));
@@ -998,10 +998,14 @@ extern "C" int p3m_set_state_all(p3m_ctx *ctx, const double *pos, const double *
     if (acc) RET(h2d(ctx, ctx->s.acc, acc, b));
     if (pos && !keep_lists) launch_set_flags(ctx->s.rebuild, ctx->s.nrep, 1, ctx->st);
     ctx->state_set = true;
+    if (!sync) {
+        CK(cudaGetLastError());
+        return P3M_OK;
+    }
     return finish(ctx);
 }
 
-extern "C" int p3m_get_state_all(p3m_ctx *ctx, double *pos, double *vel, double *acc)
+static int get_state_all(p3m_ctx *ctx, double *pos, double *vel, double *acc, bool sync)
 {
     if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
     CK(cudaSetDevice(ctx->device));
@@ -1009,7 +1013,33 @@ extern "C" int p3m_get_state_all(p3m_ctx *ctx, double *pos, double *vel, double 
     if (pos) RET(d2h(ctx, pos, ctx->s.pos, b));
     if (vel) RET(d2h(ctx, vel, ctx->s.vel, b));
     if (acc) RET(d2h(ctx, acc, ctx->s.acc, b));
+    if (!sync) {
+        CK(cudaGetLastError());
+        return P3M_OK;
+    }
     return finish(ctx);
+}
+
+extern "C" int p3m_set_state_all(p3m_ctx *ctx, const double *pos, const double *vel,
+                                 const double *acc, int keep_lists)
+{
+    return set_state_all(ctx, pos, vel, acc, keep_lists, true);
+}
+
+extern "C" int p3m_get_state_all(p3m_ctx *ctx, double *pos, double *vel, double *acc)
+{
+    return get_state_all(ctx, pos, vel, acc, true);
+}
+
+extern "C" int p3m_set_state_all_async(p3m_ctx *ctx, const double *pos, const double *vel,
+                                       const double *acc, int keep_lists)
+{
+    return set_state_all(ctx, pos, vel, acc, keep_lists, false);
+}
+
+extern "C" int p3m_get_state_all_async(p3m_ctx *ctx, double *pos, double *vel, double *acc)
+{
+    return get_state_all(ctx, pos, vel, acc, false);
 }
 
 template <typename T> static int do_init_forces(p3m_ctx *ctx)
@@ -1248,8 +1278,7 @@ extern "C" int p3m_sync(p3m_ctx *ctx)
 {
     if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
     CK(cudaSetDevice(ctx->device));
-    CK(cudaStreamSynchronize(ctx->st));
-    return P3M_OK;
+    return finish(ctx);  // waits, then reports a device status raised meanwhile
 }
 
 extern "C" int p3m_set_pp_config(p3m_ctx *ctx, int tpi, double skin)

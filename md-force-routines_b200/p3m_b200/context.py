@@ -208,21 +208,36 @@ class Context:
         self._ck(lib().p3m_get_state(self.handle, replica, dptr(pos), dptr(vel), dptr(acc)))
         return pos, vel, acc
 
-    def set_state_all(self, pos=None, vel=None, acc=None, keep_lists=False):
+    def set_state_all(self, pos=None, vel=None, acc=None, keep_lists=False, sync=True):
         """State of every replica from (sum N, 3) arrays in replica order.
-        keep_lists: keep the neighbour lists (continuing a trajectory)."""
+        keep_lists: keep the neighbour lists (continuing a trajectory).
+        sync=False: only queue the copies (the arrays must be FP64 C-order,
+        ideally pinned, and untouched until sync())."""
         n = sum(r.N for r in self.replicas)
+        if not sync:
+            for x in (pos, vel, acc):
+                if x is not None and (x.dtype != np.float64 or not x.flags.c_contiguous
+                                      or x.shape != (n, 3)):
+                    raise ValueError("asynchronous copies need (sum N, 3) float64 C-order arrays")
+            self._ck(lib().p3m_set_state_all_async(self.handle, dptr(pos), dptr(vel), dptr(acc),
+                                                   int(bool(keep_lists))))
+            return
         self._ck(lib().p3m_set_state_all(self.handle,
                                          dptr(None if pos is None else _f64(pos, (n, 3))),
                                          dptr(None if vel is None else _f64(vel, (n, 3))),
                                          dptr(None if acc is None else _f64(acc, (n, 3))),
                                          int(bool(keep_lists))))
 
-    def get_state_all(self, pos=None, vel=None, acc=None):
-        """-> (pos, vel, acc) of every replica, (sum N, 3) in replica order."""
+    def get_state_all(self, pos=None, vel=None, acc=None, sync=True):
+        """-> (pos, vel, acc) of every replica, (sum N, 3) in replica order.
+        sync=False: only queue the copies into the given arrays (valid after
+        sync())."""
         n = sum(r.N for r in self.replicas)
+        if not sync and any(a is None for a in (pos, vel, acc)):
+            raise ValueError("asynchronous reads need the three output arrays")
         pos, vel, acc = (_out(a, (n, 3)) for a in (pos, vel, acc))
-        self._ck(lib().p3m_get_state_all(self.handle, dptr(pos), dptr(vel), dptr(acc)))
+        fn = lib().p3m_get_state_all if sync else lib().p3m_get_state_all_async
+        self._ck(fn(self.handle, dptr(pos), dptr(vel), dptr(acc)))
         return pos, vel, acc
 
     def set_t_desired(self, t_desired):

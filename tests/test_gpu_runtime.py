@@ -314,3 +314,49 @@ def test_set_t_desired_and_quench():
         e = c.energies(max_steps=300)
         E = e[:, 0, 0] + e[:, 0, 1]
         assert np.max(np.abs(E - E[0])) / e[-1, 0, 1] < 1e-3
+
+
+def test_async_state_copies_on_two_contexts():
+    """Two contexts on their own streams, driven with queued copies and
+    asynchronous runs, produce what the synchronous calls produce."""
+    from p3m_b200 import FP32, MODE_NVE, Context, Replica
+
+    def reps_of(seeds):
+        L = (4 * np.pi * 1500 / 3) ** (1 / 3)
+        return [Replica(N=1500, L=L, kappa=1.0, alpha=0.7, rc=4.0, M=32, seed=s) for s in seeds]
+
+    halves = [reps_of([31, 32]), reps_of([33, 34])]
+    states = []
+    for h in halves:
+        st = [_init_state(r, r.seed) for r in h]
+        states.append((np.concatenate([x[0] for x in st]), np.concatenate([x[1] for x in st])))
+    ref = []
+    for h, (p, v) in zip(halves, states):
+        with Context(h, precision=FP32) as c:
+            c.set_state_all(p, v)
+            c.init_forces()
+            for _ in range(3):
+                out = c.get_state_all()
+                c.set_state_all(*out, keep_lists=True)
+                c.run(1, MODE_NVE)
+            ref.append(c.get_state_all())
+    ctxs = [Context(h, precision=FP32) for h in halves]
+    try:
+        bufs = []
+        for c, (p, v) in zip(ctxs, states):
+            c.set_state_all(p, v)
+            c.init_forces()
+            bufs.append(list(c.get_state_all()))
+        for _ in range(3):
+            for c, b in zip(ctxs, bufs):
+                c.set_state_all(*b, keep_lists=True, sync=False)
+                c.run(1, MODE_NVE, sync=False)
+                c.get_state_all(*b, sync=False)
+            for c in ctxs:
+                c.sync()
+        for b, r in zip(bufs, ref):
+            for x, y in zip(b, r):
+                assert np.array_equal(x, y)
+    finally:
+        for c in ctxs:
+            c.close()
