@@ -199,6 +199,7 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
     DevState &s = ctx->s;
     void *ptrs[] = {s.reps, s.pos, s.vel, s.acc, s.charge, s.prep, s.cell_key, s.cell_count,
                     s.cell_start, s.cell_cursor, s.cell_tmp, s.cell_perm, s.cell_slot, s.xq, s.nnb,
+                    s.cell_sub,
                     s.nlist, s.rebuild, s.pos_ref, s.pp_tables,
                     s.acc_pp, s.brick_key, s.brick_count, s.brick_start, s.brick_cursor,
                     s.brick_perm, s.brick_slot, s.brick_hist, s.tiles, s.spec, s.ek, s.green, s.efield,
@@ -431,6 +432,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(dalloc(&s.cell_start, (size_t)ctx->ncell_cap + 1));
     CKC(dalloc(&s.cell_cursor, (size_t)ctx->ncell_cap));
     CKC(dalloc(&s.nnb, (size_t)p));
+    CKC(dalloc(&s.cell_sub, (size_t)p));
     ctx->nlist_cap = (long long)((p + 31) / 32) * 32 * s.maxnb;
     CKC(dalloc(&s.nlist, (size_t)ctx->nlist_cap));
     CKC(dalloc(&s.rebuild, (size_t)n_reps));

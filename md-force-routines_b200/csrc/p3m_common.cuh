@@ -156,11 +156,21 @@ __device__ __forceinline__ int fold_index(int i, int M)
     return i;
 }
 
+// 4-bit sub-cell coordinates interleaved into a 12-bit Morton code (z-order
+// of the 16^3 sub-cells of a PP cell).
+__device__ __forceinline__ int morton12(int x, int y, int z)
+{
+    auto spread = [](int b) { return (b & 1) | ((b & 2) << 2) | ((b & 4) << 4) | ((b & 8) << 6); };
+    return spread(x) | (spread(y) << 1) | (spread(z) << 2);
+}
+
 // PP cell and mesh brick of a particle (see p3m_sort.cu). Raises ST_BOX and
 // files the particle under cell 0 when it is outside [-L, 2L) or not finite.
-// cell == nullptr skips the cell key.
+// cell == nullptr skips the cell key; sub (may be NULL) receives the Morton
+// code of the particle's sub-cell within its cell.
 __device__ __forceinline__ void particle_keys(const RepDev &R, double x, double y, double z,
-                                              int has_mesh, int *cell, int *brick, int *status)
+                                              int has_mesh, int *cell, int *brick, int *status,
+                                              int *sub = nullptr)
 {
     const double L = R.L;
     const bool ok = (x >= -L && x < 2.0 * L) && (y >= -L && y < 2.0 * L) && (z >= -L && z < 2.0 * L);
@@ -174,6 +184,10 @@ __device__ __forceinline__ void particle_keys(const RepDev &R, double x, double 
         const int cy = min((int)floor(yw / R.cellw), R.nc - 1);
         const int cz = min((int)floor(zw / R.cellw), R.nc - 1);
         *cell = R.cell_off + cx + R.nc * (cy + R.nc * cz);
+        if (sub) {
+            auto q4 = [](double t, int c) { return max(0, min(15, (int)((t - c) * 16.0))); };
+            *sub = morton12(q4(xw / R.cellw, cx), q4(yw / R.cellw, cy), q4(zw / R.cellw, cz));
+        }
     }
     *brick = -1;
     if (has_mesh && R.M > 0) {

@@ -33,6 +33,7 @@ struct DevState {
     int *cell_cursor = nullptr, *cell_tmp = nullptr, *cell_perm = nullptr, *cell_slot = nullptr;
     void *xq = nullptr;          // integer coordinates in sorted order (uint4 / ulonglong4)
     int *nnb = nullptr;          // list length per sorted particle
+    int *cell_sub = nullptr;     // [particle] sub-cell Morton code (rebuild steps)
     int *nlist = nullptr;        // neighbour lists (sorted indices), warp-interleaved
     int *rebuild = nullptr;      // per-replica flags: rebuild cells and lists this step
     double *pos_ref = nullptr;   // positions at the last rebuild (ntot,3)

@@ -29,14 +29,17 @@ namespace p3m {
 template <typename T>
 __global__ void k_keys(const RepDev *__restrict__ reps, const int *__restrict__ prep,
                        const double *__restrict__ pos, int ntot, int *__restrict__ cell_key,
-                       int *__restrict__ cell_count, int *__restrict__ brick_key,
-                       int *__restrict__ brick_count, int has_mesh, int *status)
+                       int *__restrict__ cell_sub, int *__restrict__ cell_count,
+                       int *__restrict__ brick_key, int *__restrict__ brick_count, int has_mesh,
+                       int *status)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
         const RepDev &R = reps[prep[i]];
-        int c, b;
-        particle_keys(R, pos[3 * i + 0], pos[3 * i + 1], pos[3 * i + 2], has_mesh, &c, &b, status);
+        int c, b, sub;
+        particle_keys(R, pos[3 * i + 0], pos[3 * i + 1], pos[3 * i + 2], has_mesh, &c, &b, status,
+                      &sub);
         cell_key[i] = c;
+        cell_sub[i] = sub;
         atomicAdd(&cell_count[c], 1);
         if (b >= 0) {
             brick_key[i] = b;
@@ -48,16 +51,17 @@ __global__ void k_keys(const RepDev *__restrict__ reps, const int *__restrict__ 
 // Cell keys of a rebuild step (the drift kernel computed the brick keys).
 __global__ void k_cell_keys(const RepDev *__restrict__ reps, const int *__restrict__ prep,
                             const double *__restrict__ pos, int ntot, int *__restrict__ cell_key,
-                            int *__restrict__ cell_count, const int *__restrict__ rebuild,
-                            int *status)
+                            int *__restrict__ cell_sub, int *__restrict__ cell_count,
+                            const int *__restrict__ rebuild, int *status)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
         const int r = prep[i];
         if (!rebuild[r]) continue;
         const RepDev &R = reps[r];
-        int c, b;
-        particle_keys(R, pos[3 * i + 0], pos[3 * i + 1], pos[3 * i + 2], 0, &c, &b, status);
+        int c, b, sub;
+        particle_keys(R, pos[3 * i + 0], pos[3 * i + 1], pos[3 * i + 2], 0, &c, &b, status, &sub);
         cell_key[i] = c;
+        cell_sub[i] = sub;
         atomicAdd(&cell_count[c], 1);
     }
 }
@@ -133,24 +137,37 @@ __global__ void k_scatter(const int *__restrict__ cell_key, const int *__restric
     }
 }
 
-// One warp per cell: order the cell's particles by index, and remember every
-// particle's position at this rebuild (the reference point of the skin check).
+// One warp per cell: order the cell's particles by (sub-cell Morton code,
+// index) -- z-order inside the cell, so the particles of one warp of the PP
+// kernel are neighbours in space and walk their (similar) lists in step,
+// reading nearby coordinates -- and remember every particle's position at
+// this rebuild (the reference point of the skin check).
 __global__ void k_fix_cells(const RepDev *__restrict__ reps, int nrep,
                             const int *__restrict__ cell_start, const int *__restrict__ cell_tmp,
-                            const double *__restrict__ pos, int *__restrict__ cell_perm,
-                            int *__restrict__ cell_slot, double *__restrict__ pos_ref, int ncell,
+                            const int *__restrict__ cell_sub, const double *__restrict__ pos,
+                            int *__restrict__ cell_perm, int *__restrict__ cell_slot,
+                            double *__restrict__ pos_ref, int ncell,
                             const int *__restrict__ rebuild)
 {
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
+    auto key = [&](int i) { return ((unsigned long long)cell_sub[i] << 32) | (unsigned)i; };
     for (int c = blockIdx.x * wpb + (threadIdx.x >> 5); c < ncell; c += gridDim.x * wpb) {
         if (!rebuild[find_rep(c, nrep, [&](int k) { return reps[k].cell_off; })]) continue;
         const int start = cell_start[c], n = cell_start[c + 1] - start;
         for (int e0 = 0; e0 < n; e0 += 32) {
             int e = e0 + lane;
-            int v = (e < n) ? cell_tmp[start + e] : 0x7fffffff;
+            int v = (e < n) ? cell_tmp[start + e] : 0;
+            const unsigned long long kv = (e < n) ? key(v) : ~0ull;
+            // rank = keys below kv: 32 keys loaded per pass, compared by shuffle
             int rank = 0;
-            for (int f = 0; f < n; ++f) rank += (cell_tmp[start + f] < v) ? 1 : 0;
+            for (int f0 = 0; f0 < n; f0 += 32) {
+                const int f = f0 + lane;
+                const unsigned long long kf = (f < n) ? key(cell_tmp[start + f]) : ~0ull;
+                const int m = min(32, n - f0);
+                for (int t = 0; t < m; ++t)
+                    rank += (__shfl_sync(0xffffffffu, kf, t) < kv) ? 1 : 0;
+            }
             if (e < n) {
                 int s = start + rank;
                 cell_perm[s] = v;
@@ -263,14 +280,15 @@ static int grid_for(int n, int threads, int cap = 148 * 16)
 template <typename T> void launch_keys(const DevState &s, cudaStream_t st)
 {
     k_keys<T><<<grid_for(s.ntot, 256), 256, 0, st>>>(s.reps, s.prep, s.pos, s.ntot, s.cell_key,
-                                                      s.cell_count, s.brick_key, s.brick_count,
-                                                      s.has_mesh, s.status);
+                                                      s.cell_sub, s.cell_count, s.brick_key,
+                                                      s.brick_count, s.has_mesh, s.status);
 }
 
 void launch_cell_keys(const DevState &s, cudaStream_t st)
 {
     k_cell_keys<<<grid_for(s.ntot, 256), 256, 0, st>>>(s.reps, s.prep, s.pos, s.ntot, s.cell_key,
-                                                       s.cell_count, s.rebuild, s.status);
+                                                       s.cell_sub, s.cell_count, s.rebuild,
+                                                       s.status);
 }
 
 void launch_scan(const DevState &s, cudaStream_t st)
@@ -302,8 +320,8 @@ template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st)
 {
     const int wpb = 8;
     int blocks = (s.ncell + wpb - 1) / wpb;
-    k_fix_cells<<<blocks, wpb * 32, 0, st>>>(s.reps, s.nrep, s.cell_start, s.cell_tmp, s.pos,
-                                             s.cell_perm, s.cell_slot, s.pos_ref, s.ncell,
+    k_fix_cells<<<blocks, wpb * 32, 0, st>>>(s.reps, s.nrep, s.cell_start, s.cell_tmp, s.cell_sub,
+                                             s.pos, s.cell_perm, s.cell_slot, s.pos_ref, s.ncell,
                                              s.rebuild);
 }
 
