@@ -127,22 +127,20 @@ static void pair_g_psi(double r, double kappa, double a, double *g, double *psi)
          (a / sqrt(M_PI)) * r * (exp(-up * up) * exp(kappa * r) + exp(-um * um) * exp(-kappa * r));
 }
 
-// Cubic per interval through the samples at u = 0, 1/3, 2/3, 1 (monomial
-// coefficients in u): PP_TABLE_N float4 for g, then PP_TABLE_N for psi.
+// Cubic of psi per interval through the samples at u = 0, 1/3, 2/3, 1
+// (monomial coefficients in u): PP_TABLE_N float4 (the FP32 kernel derives
+// the force from the same cubic).
 static void build_pp_table(const p3m_replica_desc &d, float4 *out)
 {
     const double h = d.rc / PP_TABLE_N;
     for (int i = 0; i < PP_TABLE_N; ++i) {
         double fg[4], fp[4];
         for (int k = 0; k < 4; ++k) pair_g_psi((i + k / 3.0) * h, d.kappa, d.alpha, &fg[k], &fp[k]);
-        auto coef = [](const double *f, float4 &c) {
-            c.x = (float)f[0];
-            c.y = (float)((-11.0 * f[0] + 18.0 * f[1] - 9.0 * f[2] + 2.0 * f[3]) / 2.0);
-            c.z = (float)((18.0 * f[0] - 45.0 * f[1] + 36.0 * f[2] - 9.0 * f[3]) / 2.0);
-            c.w = (float)((-9.0 * f[0] + 27.0 * f[1] - 27.0 * f[2] + 9.0 * f[3]) / 2.0);
-        };
-        coef(fg, out[i]);
-        coef(fp, out[PP_TABLE_N + i]);
+        float4 &c = out[i];
+        c.x = (float)fp[0];
+        c.y = (float)((-11.0 * fp[0] + 18.0 * fp[1] - 9.0 * fp[2] + 2.0 * fp[3]) / 2.0);
+        c.z = (float)((18.0 * fp[0] - 45.0 * fp[1] + 36.0 * fp[2] - 9.0 * fp[3]) / 2.0);
+        c.w = (float)((-9.0 * fp[0] + 27.0 * fp[1] - 27.0 * fp[2] + 9.0 * fp[3]) / 2.0);
     }
 }
 
@@ -409,8 +407,8 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(dalloc(&s.reps, n_reps));
     CKC(cudaMemcpy(s.reps, ctx->rh.data(), sizeof(RepDev) * n_reps, cudaMemcpyHostToDevice));
     {
-        std::vector<float4> tab((size_t)n_reps * 2 * PP_TABLE_N);
-        for (int r = 0; r < n_reps; ++r) build_pp_table(reps[r], tab.data() + (size_t)r * 2 * PP_TABLE_N);
+        std::vector<float4> tab((size_t)n_reps * PP_TABLE_N);
+        for (int r = 0; r < n_reps; ++r) build_pp_table(reps[r], tab.data() + (size_t)r * PP_TABLE_N);
         CKC(dalloc(&s.pp_tables, tab.size()));
         CKC(cudaMemcpy(s.pp_tables, tab.data(), sizeof(float4) * tab.size(), cudaMemcpyHostToDevice));
     }

@@ -29,7 +29,7 @@ enum : int {
 };
 
 // Intervals of the tabulated FP32 pair functions on [0, rc].
-constexpr int PP_TABLE_N = 1024;
+constexpr int PP_TABLE_N = 2048;  // FP32 pair table: cubic intervals on [0, rc]
 
 // Per-replica constants. Offsets index the concatenated device arrays.
 struct RepDev {

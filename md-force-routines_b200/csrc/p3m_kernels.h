@@ -37,7 +37,7 @@ struct DevState {
     int *nlist = nullptr;        // neighbour lists (sorted indices), warp-interleaved
     int *rebuild = nullptr;      // per-replica flags: rebuild cells and lists this step
     double *pos_ref = nullptr;   // positions at the last rebuild (ntot,3)
-    float4 *pp_tables = nullptr; // FP32 pair-function tables [nrep][g, psi][PP_TABLE_N]
+    float4 *pp_tables = nullptr; // FP32 pair tables: cubic of psi = phi r, [nrep][PP_TABLE_N]
     void *acc_pp = nullptr;      // V4<T> PP acceleration, cell-sorted order
     // brick sort
     int *brick_key = nullptr, *brick_count = nullptr, *brick_start = nullptr;

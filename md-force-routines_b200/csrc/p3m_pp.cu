@@ -24,11 +24,12 @@
 // Pair terms: the FP64 path evaluates the reference's formula directly,
 // written with the shared Gaussian factor
 //   e^{+-kr} erfc(u+-) = erfcx(u+-) exp(-(a^2 r^2 + k^2/4a^2)),  u+- = ar +- k/2a,
-// using CUDA's exp and erfcx. The FP32 path interpolates two smooth functions
-// tabulated on [0, rc] from FP64 values computed on the host,
-//   g(r) = F(r) r^2     psi(r) = phi(r) r
-// (both finite at r = 0), cubic per interval, and forms F/r = g/r^3 and
-// phi = psi/r.
+// using CUDA's exp and erfcx. The FP32 path interpolates psi(r) = phi(r) r
+// (finite at r = 0), tabulated on [0, rc] from FP64 values computed on the
+// host, cubic per interval, and takes the force from the same cubic:
+//   g(r) = F(r) r^2 = -r^2 d(psi/r)/dr = psi - r psi',
+// F/r = g/r^3 and phi = psi/r -- one table read per pair, and a force that is
+// exactly minus the gradient of the interpolated potential.
 #include "p3m_kernels.h"
 
 namespace p3m {
@@ -222,10 +223,8 @@ __device__ __forceinline__ void pair_direct(double r2, const RepDev &R, double &
     f_over_r = fr * rinv;
 }
 
-// FP32: tabulated g and psi; tab holds the cubic coefficients (in the
-// interval coordinate u in [0,1)) of g for every interval, then those of psi:
-// float4 slots i and PP_TABLE_N + i. (Interleaving them would put every g
-// read on an even slot, half of shared memory's eight 16-byte bank groups.)
+// FP32: tab holds the cubic coefficients of psi in the interval coordinate
+// u in [0,1), one float4 per interval; t = r / h, g = psi - t dpsi/du.
 __device__ __forceinline__ void pair_table(float r2, const float4 *__restrict__ tab, float inv_h,
                                            float &f_over_r, float &phi)
 {
@@ -237,11 +236,11 @@ __device__ __forceinline__ void pair_table(float r2, const float4 *__restrict__ 
     const float tb = (t - 0.5f) + 12582912.0f;
     const int i = min(__float_as_int(tb) - 0x4B400000, PP_TABLE_N - 1);
     const float u = t - (tb - 12582912.0f);
-    const float4 cg = tab[i], cp = tab[PP_TABLE_N + i];
-    const float g = fmaf(fmaf(fmaf(cg.w, u, cg.z), u, cg.y), u, cg.x);
-    const float ps = fmaf(fmaf(fmaf(cp.w, u, cp.z), u, cp.y), u, cp.x);
-    const float rinv2 = rinv * rinv;
-    f_over_r = g * rinv2 * rinv;
+    const float4 c = tab[i];
+    const float ps = fmaf(fmaf(fmaf(c.w, u, c.z), u, c.y), u, c.x);
+    const float dps = fmaf(fmaf(3.0f * c.w, u, 2.0f * c.z), u, c.y);
+    const float g = fmaf(-t, dps, ps);
+    f_over_r = g * (rinv * rinv) * rinv;
     phi = ps * rinv;
 }
 
@@ -268,8 +267,8 @@ k_pp_list(const RepDev *__restrict__ reps, int nrep, const typename Coord<T>::Q 
     const RepDev &R = reps[r];
     if constexpr (F32) {
         // every block works on one replica: stage its pair-function table
-        const float4 *src = tables + (long long)r * 2 * PP_TABLE_N;
-        for (int k = threadIdx.x; k < 2 * PP_TABLE_N; k += PPL_THREADS) cp_async16(ppl_tab + k, src + k);
+        const float4 *src = tables + (long long)r * PP_TABLE_N;
+        for (int k = threadIdx.x; k < PP_TABLE_N; k += PPL_THREADS) cp_async16(ppl_tab + k, src + k);
         cp_async_wait_all();
         __syncthreads();
     }
@@ -380,7 +379,7 @@ template <typename T> void configure_pp_kernels()
     using Q = typename Coord<T>::Q;
     cudaFuncSetAttribute(k_build_lists<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(lb_scap<T>() * sizeof(Q)));
-    const int tab = sizeof(T) == 4 ? (int)(2 * PP_TABLE_N * sizeof(float4)) : 0;
+    const int tab = sizeof(T) == 4 ? (int)(PP_TABLE_N * sizeof(float4)) : 0;
     cudaFuncSetAttribute(k_pp_list<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
     cudaFuncSetAttribute(k_pp_list<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
     cudaFuncSetAttribute(k_pp_list<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
@@ -406,7 +405,7 @@ template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st
 template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cudaStream_t st)
 {
     using Q = typename Coord<T>::Q;
-    const size_t smem = sizeof(T) == 4 ? 2 * PP_TABLE_N * sizeof(float4) : 0;
+    const size_t smem = sizeof(T) == 4 ? PP_TABLE_N * sizeof(float4) : 0;
     k_pp_list<T, TPI><<<s.pp_nblk, PPL_THREADS, smem, st>>>(s.reps, s.nrep, (const Q *)s.xq, s.nnb,
                                                          s.nlist, s.maxnb, s.pp_tables,
                                                          (typename V4<T>::t *)s.acc_pp, s.u_pp_part);
