@@ -43,6 +43,7 @@ struct p3m_ctx {
     size_t hbuf_bytes = 0;
     bool state_set = false;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    long long graph_kernels[2][2] = {{0, 0}, {0, 0}};  // kernels each graph launches
     int ncell_cap = 0;            // cells allocated (grid with skin 0)
     long long nlist_cap = 0;      // list entries allocated
     int pp_nblk_cap = 0;          // PP blocks allocated (tpi = 8)
@@ -509,22 +510,29 @@ template <typename T> static void seq_sort(p3m_ctx *ctx, bool keys)
     }
 }
 
-template <typename T> static void seq_pp(p3m_ctx *ctx)
+// reduce = false: leave the energy partials to k_step_reduce (inside a step)
+template <typename T> static void seq_pp(p3m_ctx *ctx, bool reduce = true)
 {
     launch_pp<T>(ctx->s, ctx->st);
-    launch_reduce_pp(ctx->s, ctx->st);
-    ctx->launches += 2;
+    ctx->launches++;
+    if (reduce) {
+        launch_reduce_pp(ctx->s, ctx->st);
+        ctx->launches++;
+    }
 }
 
-template <typename T> static void seq_pm(p3m_ctx *ctx)
+template <typename T> static void seq_pm(p3m_ctx *ctx, bool reduce = true)
 {
     DevState &s = ctx->s;
     launch_assign<T>(s, ctx->st);
     launch_fft_forward<T>(s, ctx->st);
-    launch_reduce_pm(s, ctx->st);
+    if (reduce) {
+        launch_reduce_pm(s, ctx->st);
+        ctx->launches++;
+    }
     launch_fft_inverse<T>(s, ctx->st);
     launch_gather<T>(s, ctx->st);
-    ctx->launches += 3 + fft_kernel_count(s);
+    ctx->launches += 2 + fft_kernel_count(s);
 }
 
 // Compute the influence function of every replica that has none yet.
@@ -565,18 +573,29 @@ template <typename T> static void seq_step(p3m_ctx *ctx, int mode, int record_nq
     launch_kick_drift(s, ctx->st);
     ctx->launches++;
     seq_sort<T>(ctx, false);
-    seq_pp<T>(ctx);
-    if (s.has_mesh) seq_pm<T>(ctx);
+    seq_pp<T>(ctx, false);
+    if (s.has_mesh) seq_pm<T>(ctx, false);
     launch_kick_finish<T>(s, 1, nullptr, ctx->st);
     ctx->launches++;
     const int rec = (record_nqt && ctx->nq > 0) ? 1 : 0;
+    StepSums sums;  // the energy sums and this step's n(q,t) row, in the reduction
+    sums.u_pp_part = s.u_pp_part;
+    sums.pp_nblk = s.pp_nblk;
+    sums.u_pm_part = s.u_pm_part;
+    sums.wc_total = s.wc;
+    sums.wp_total = s.wp;
     if (rec) {  // positions of this step are final: row counters[3] of the ring
-        launch_nqt<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nq_consecutive, ctx->nqt_part,
-                      ctx->nqt_ring, ctx->counters, ctx->nqt_cap, ctx->st);
-        ctx->launches += 2;
+        launch_nqt_partial<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nq_consecutive, ctx->nqt_part,
+                              ctx->st);
+        ctx->launches++;
+        sums.nqt_part = ctx->nqt_part;
+        sums.nq = ctx->nq;
+        sums.nq_nblk = s.nq_nblk;
+        sums.nqt_cap = ctx->nqt_cap;
+        sums.nqt_ring = ctx->nqt_ring;
     }
     launch_step_reduce(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, ctx->st, rec,
-                       ctx->snap_interval, ctx->snap_cap);
+                       ctx->snap_interval, ctx->snap_cap, sums);
     ctx->launches++;
     if (mode == P3M_MODE_THERMOSTAT) {
         launch_scale_vel(s, ctx->st);
@@ -1102,6 +1121,7 @@ template <typename T> static int do_run(p3m_ctx *ctx, int n_steps, int mode, int
         CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
         seq_step<T>(ctx, mode, rec);
         cudaError_t e = cudaStreamEndCapture(ctx->st, &g);
+        ctx->graph_kernels[gi][gr] = ctx->launches - before;  // kernels per replay
         ctx->launches = before;
         if (e != cudaSuccess) return fail(ctx, P3M_ECUDA, "cudaStreamEndCapture", cudaGetErrorString(e));
         e = cudaGraphInstantiate(&ctx->graph[gi][gr], g, 0);
@@ -1110,12 +1130,8 @@ template <typename T> static int do_run(p3m_ctx *ctx, int n_steps, int mode, int
     }
     for (int k = 0; k < n_steps; ++k) {
         if (use_graph) {
-            const long long before = ctx->launches;
             CK(cudaGraphLaunch(ctx->graph[gi][gr], ctx->st));
-            // count the kernels the graph holds (same sequence as seq_step)
-            ctx->launches = before + (long long)(11 + (s.has_mesh ? 4 + fft_kernel_count(s) : 0) + (gi ? 1 : 0) +
-                                                 ((gr && ctx->nq > 0) ? 2 : 0) +
-                                                 (ctx->snap_interval > 0 ? 1 : 0));
+            ctx->launches += ctx->graph_kernels[gi][gr];  // counted while capturing
         } else {
             seq_step<T>(ctx, mode, rec);
         }

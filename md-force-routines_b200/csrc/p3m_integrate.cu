@@ -127,7 +127,7 @@ __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nbl
                               const double *__restrict__ kin_part, double *__restrict__ rep_out,
                               int mode, int *__restrict__ counters, double *__restrict__ ring,
                               int ring_cap, int recorded, int snap_interval, int snap_cap,
-                              int *rebuild, int *status)
+                              int *rebuild, int *status, StepSums sums)
 {
     // counters: [0] steps since the run started, [1] energy-ring position,
     // [2] step index of the run's first step (thermostat_p3m_ord6.py:15 tests
@@ -136,8 +136,40 @@ __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nbl
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int it = counters[2] + counters[0];
     const int step = counters[1];
+    // the n(q,t) row of this step (k_nqt_reduce's sums, in its order)
+    if (sums.nqt_part) {
+        const int row = counters[3] % sums.nqt_cap;
+        const int per = sums.nq * 6;
+        for (int e = threadIdx.x; e < nrep * per; e += blockDim.x) {
+            const int r = e / per, k = e % per;
+            const int b0 = reps[r].nq_blk_off, b1 = (r + 1 < nrep) ? reps[r + 1].nq_blk_off : sums.nq_nblk;
+            double v = 0.0;
+            for (int bb = b0; bb < b1; ++bb) v += sums.nqt_part[(long long)bb * per + k];
+            sums.nqt_ring[((long long)row * nrep + r) * per + k] = v;
+        }
+    }
     for (int r = w; r < nrep; r += nw) {
         const RepDev &R = reps[r];
+        if (sums.u_pp_part) {
+            // k_reduce_pp and k_reduce_pm, in their order
+            const int b0 = R.pp_blk_off, b1 = (r + 1 < nrep) ? reps[r + 1].pp_blk_off : sums.pp_nblk;
+            double t = 0.0;
+            for (int k = b0 + lane; k < b1; k += 32) t += sums.u_pp_part[k];
+            t = warp_sum(t);
+            double tm = 0.0;
+            if (R.M > 0) {
+                const int cb = R.wc_off, ce = (r + 1 < nrep) ? reps[r + 1].wc_off : sums.wc_total;
+                const int pb = sums.wc_total + R.wp_off,
+                          pe = sums.wc_total + ((r + 1 < nrep) ? reps[r + 1].wp_off : sums.wp_total);
+                for (int k = cb + lane; k < ce; k += 32) tm += sums.u_pm_part[k];
+                for (int k = pb + lane; k < pe; k += 32) tm += sums.u_pm_part[k];
+                tm = warp_sum(tm);
+            }
+            if (lane == 0) {
+                rep_out[8 * r + RO_UPP] = 0.5 * t;
+                rep_out[8 * r + RO_UPM] = 0.5 * tm;
+            }
+        }
         const int b0 = R.blk_off, b1 = (r + 1 < nrep) ? reps[r + 1].blk_off : nblk;
         double s = 0.0;
         for (int k = b0 + lane; k < b1; k += 32) s += kin_part[k];
@@ -493,11 +525,21 @@ void launch_kick_finish(const DevState &s, int do_kick, double *ep_out, cudaStre
 }
 
 void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring, int ring_cap,
-                        cudaStream_t st, int recorded, int snap_interval, int snap_cap)
+                        cudaStream_t st, int recorded, int snap_interval, int snap_cap,
+                        const StepSums &sums)
 {
     k_step_reduce<<<1, 1024, 0, st>>>(s.reps, s.nrep, s.nblk, s.kin_part, s.rep_out, mode,
                                       counters, ring, ring_cap, recorded, snap_interval, snap_cap,
-                                      s.rebuild, s.status);
+                                      s.rebuild, s.status, sums);
+}
+
+template <typename T>
+void launch_nqt_partial(const DevState &s, const double *pos, const double *qmult, int nq,
+                        int consecutive, double *part, cudaStream_t st)
+{
+    const size_t smem = (size_t)(PBLK / 32) * nq * 6 * sizeof(double);
+    k_nqt_partial<T><<<s.nq_nblk, PBLK, smem, st>>>(s.reps, s.nrep, pos, qmult, nq, consecutive,
+                                                    part);
 }
 
 void launch_snapshot(const DevState &s, const int *counters, double *snap, int *steps,
@@ -556,6 +598,8 @@ void launch_gf_opt(double kappa, double alpha, int p, int m_alias, int M, double
 int gf_opt_blocks(int M) { return (int)(((long long)M * M * M + 255) / 256); }
 
 #define P3M_INST(T)                                                                             \
+    template void launch_nqt_partial<T>(const DevState &, const double *, const double *, int,   \
+                                        int, double *, cudaStream_t);                           \
     template void launch_kick_finish<T>(const DevState &, int, double *, cudaStream_t);          \
     template void launch_nqt<T>(const DevState &, const double *, const double *, int, int,      \
                                 double *, double *, const int *, int, cudaStream_t);            \
