@@ -164,14 +164,16 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
             for (int w0 = 0; w0 < total; w0 += SCAP) {
                 const int wlen = min(SCAP, total - w0);
                 __syncthreads();
-                for (int k = tid; k < wlen; k += LB_THREADS) {
-                    const int g = w0 + k;
-                    int cc = 0;
-                    while (pre[cc + 1] <= g) ++cc;
-                    const int j = nstart[cc] + g - pre[cc];
-                    Q q = xq[j];
-                    q.w = j;  // the staged copy carries the sorted index
-                    stage[k] = q;
+                // warp w copies neighbour cells w, w + 8, ... (their particles
+                // are contiguous): the part of each that falls in this window
+                for (int cc = tid >> 5; cc < 27; cc += LB_THREADS / 32) {
+                    const int lo = max(pre[cc], w0), hi = min(pre[cc + 1], w0 + wlen);
+                    for (int g = lo + lane; g < hi; g += 32) {
+                        const int j = nstart[cc] + g - pre[cc];
+                        Q q = xq[j];
+                        q.w = j;  // the staged copy carries the sorted index
+                        stage[g - w0] = q;
+                    }
                 }
                 __syncthreads();
                 for (int kb = 0; kb < wlen; kb += LB_TPI) {  // uniform over the block

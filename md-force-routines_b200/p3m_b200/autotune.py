@@ -11,7 +11,7 @@ import os
 
 from ._lib import MODE_NVE
 
-CANDIDATES = [(tpi, skin) for tpi in (1, 2, 4) for skin in (0.3, 0.5, 0.8)]
+CANDIDATES = [(tpi, skin) for tpi in (1, 2, 4) for skin in (0.5, 0.8, 1.1, 1.4)]
 CACHE = os.environ.get("P3M_B200_TUNE_CACHE",
                        os.path.join(os.path.expanduser("~"), ".cache", "p3m_b200", "autotune.json"))
 
