@@ -20,6 +20,8 @@ struct p3m_ctx {
     std::vector<char> green_ready;
     DevState s;
     cudaStream_t st = nullptr;
+    cudaStream_t st2 = nullptr;   // the mesh branch of a step (joined back into st)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int *counters = nullptr;      // [0] run step, [1] ring position, [2] it0, [3] n(q,t) rows,
                                   // [4] snapshots taken, [5] this step's snapshot slot
     int snap_interval = 0, snap_cap = 0;
@@ -209,6 +211,12 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (ctx->hbuf) cudaFreeHost(ctx->hbuf);
+    if (ctx->st2) {
+        cudaStreamSynchronize(ctx->st2);
+        cudaStreamDestroy(ctx->st2);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
     return P3M_OK;
@@ -405,6 +413,9 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
         }                                                                    \
     } while (0)
     CKC(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+    CKC(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
+    CKC(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    CKC(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
     CKC(dalloc(&s.reps, n_reps));
     CKC(cudaMemcpy(s.reps, ctx->rh.data(), sizeof(RepDev) * n_reps, cudaMemcpyHostToDevice));
     {
@@ -511,27 +522,29 @@ template <typename T> static void seq_sort(p3m_ctx *ctx, bool keys)
 }
 
 // reduce = false: leave the energy partials to k_step_reduce (inside a step)
-template <typename T> static void seq_pp(p3m_ctx *ctx, bool reduce = true)
+template <typename T> static void seq_pp(p3m_ctx *ctx, bool reduce = true, cudaStream_t st = nullptr)
 {
-    launch_pp<T>(ctx->s, ctx->st);
+    if (!st) st = ctx->st;
+    launch_pp<T>(ctx->s, st);
     ctx->launches++;
     if (reduce) {
-        launch_reduce_pp(ctx->s, ctx->st);
+        launch_reduce_pp(ctx->s, st);
         ctx->launches++;
     }
 }
 
-template <typename T> static void seq_pm(p3m_ctx *ctx, bool reduce = true)
+template <typename T> static void seq_pm(p3m_ctx *ctx, bool reduce = true, cudaStream_t st = nullptr)
 {
+    if (!st) st = ctx->st;
     DevState &s = ctx->s;
-    launch_assign<T>(s, ctx->st);
-    launch_fft_forward<T>(s, ctx->st);
+    launch_assign<T>(s, st);
+    launch_fft_forward<T>(s, st);
     if (reduce) {
-        launch_reduce_pm(s, ctx->st);
+        launch_reduce_pm(s, st);
         ctx->launches++;
     }
-    launch_fft_inverse<T>(s, ctx->st);
-    launch_gather<T>(s, ctx->st);
+    launch_fft_inverse<T>(s, st);
+    launch_gather<T>(s, st);
     ctx->launches += 2 + fft_kernel_count(s);
 }
 
@@ -566,45 +579,76 @@ template <typename T> static int seq_force(p3m_ctx *ctx, bool keys)
     return P3M_OK;
 }
 
-// One integrator step of every replica (mode 0 NVE, 1 thermostat).
-template <typename T> static void seq_step(p3m_ctx *ctx, int mode, int record_nqt)
+// One integrator step of every replica (mode 0 NVE, 1 thermostat). After the
+// drift and the key scan the step forks: the mesh branch (brick sort,
+// assignment, FFTs, gather, and the n(q,t) sums of the new positions) runs
+// on the second stream while the particle branch (cell sort, lists, PP) runs
+// on the first -- they share no arrays -- and they join before the forces are
+// combined, so the latency-bound mesh kernels fill the SMs the PP kernel
+// leaves idle (one graph holds both branches).
+template <typename T> static int seq_step(p3m_ctx *ctx, int mode, int record_nqt)
 {
     DevState &s = ctx->s;
-    launch_kick_drift(s, ctx->st);
-    ctx->launches++;
-    seq_sort<T>(ctx, false);
-    seq_pp<T>(ctx, false);
-    if (s.has_mesh) seq_pm<T>(ctx, false);
-    launch_kick_finish<T>(s, 1, nullptr, ctx->st);
-    ctx->launches++;
+    cudaStream_t st = ctx->st, st2 = ctx->st2;
+    launch_kick_drift(s, st);
+    launch_cell_keys(s, st);
+    launch_scan(s, st);
+    ctx->launches += 3;
     const int rec = (record_nqt && ctx->nq > 0) ? 1 : 0;
+    const bool fork = s.has_mesh || rec;
+    cudaError_t e = cudaSuccess;
+    if (fork) {
+        e = cudaEventRecord(ctx->ev_fork, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st2, ctx->ev_fork, 0);
+        if (e == cudaSuccess) {
+            if (s.has_mesh) {
+                launch_sort_bricks(s, st2);
+                ctx->launches += 3;
+                seq_pm<T>(ctx, false, st2);
+            }
+            if (rec) {  // positions of this step are final: row counters[3] of the ring
+                launch_nqt_partial<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nq_consecutive,
+                                      ctx->nqt_part, st2);
+                ctx->launches++;
+            }
+            e = cudaEventRecord(ctx->ev_join, st2);
+        }
+    }
+    launch_scatter(s, st);
+    launch_fix_cells<T>(s, st);
+    launch_quantize<T>(s, st);     // sorted coordinates of this step
+    launch_build_lists<T>(s, st);  // from those coordinates (rebuild steps)
+    ctx->launches += 4;
+    seq_pp<T>(ctx, false, st);
+    if (fork && e == cudaSuccess) e = cudaStreamWaitEvent(st, ctx->ev_join, 0);
+    launch_kick_finish<T>(s, 1, nullptr, st);
+    ctx->launches++;
     StepSums sums;  // the energy sums and this step's n(q,t) row, in the reduction
     sums.u_pp_part = s.u_pp_part;
     sums.pp_nblk = s.pp_nblk;
     sums.u_pm_part = s.u_pm_part;
     sums.wc_total = s.wc;
     sums.wp_total = s.wp;
-    if (rec) {  // positions of this step are final: row counters[3] of the ring
-        launch_nqt_partial<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nq_consecutive, ctx->nqt_part,
-                              ctx->st);
-        ctx->launches++;
+    if (rec) {
         sums.nqt_part = ctx->nqt_part;
         sums.nq = ctx->nq;
         sums.nq_nblk = s.nq_nblk;
         sums.nqt_cap = ctx->nqt_cap;
         sums.nqt_ring = ctx->nqt_ring;
     }
-    launch_step_reduce(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, ctx->st, rec,
+    launch_step_reduce(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, st, rec,
                        ctx->snap_interval, ctx->snap_cap, sums);
     ctx->launches++;
     if (mode == P3M_MODE_THERMOSTAT) {
-        launch_scale_vel(s, ctx->st);
+        launch_scale_vel(s, st);
         ctx->launches++;
     }
     if (ctx->snap_interval > 0) {  // after the thermostat's rescale: the step's final state
-        launch_snapshot(s, ctx->counters, ctx->snap, ctx->snap_steps, ctx->st);
+        launch_snapshot(s, ctx->counters, ctx->snap, ctx->snap_steps, st);
         ctx->launches++;
     }
+    if (e != cudaSuccess) return fail(ctx, P3M_ECUDA, "step fork/join", cudaGetErrorString(e));
+    return P3M_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -909,7 +953,7 @@ static int do_update(p3m_ctx *ctx, int mode, int it, double *pos, double *vel, d
     launch_set_counters(ctx->counters, 0, -1, it, ctx->st);
     launch_set_flags(s.rebuild, s.nrep, 1, ctx->st);  // the caller's arrays may hold any state
     ctx->launches += 2;
-    seq_step<T>(ctx, mode, 0);
+    RET(seq_step<T>(ctx, mode, 0));
     RET(d2h(ctx, pos, s.pos, b));
     RET(d2h(ctx, vel, s.vel, b));
     RET(d2h(ctx, acc, s.acc, b));
@@ -1119,10 +1163,14 @@ template <typename T> static int do_run(p3m_ctx *ctx, int n_steps, int mode, int
         cudaGraph_t g;
         const long long before = ctx->launches;
         CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
-        seq_step<T>(ctx, mode, rec);
+        const int step_rc = seq_step<T>(ctx, mode, rec);
         cudaError_t e = cudaStreamEndCapture(ctx->st, &g);
         ctx->graph_kernels[gi][gr] = ctx->launches - before;  // kernels per replay
         ctx->launches = before;
+        if (step_rc != P3M_OK) {
+            if (e == cudaSuccess) cudaGraphDestroy(g);
+            return step_rc;
+        }
         if (e != cudaSuccess) return fail(ctx, P3M_ECUDA, "cudaStreamEndCapture", cudaGetErrorString(e));
         e = cudaGraphInstantiate(&ctx->graph[gi][gr], g, 0);
         cudaGraphDestroy(g);
@@ -1133,7 +1181,7 @@ template <typename T> static int do_run(p3m_ctx *ctx, int n_steps, int mode, int
             CK(cudaGraphLaunch(ctx->graph[gi][gr], ctx->st));
             ctx->launches += ctx->graph_kernels[gi][gr];  // counted while capturing
         } else {
-            seq_step<T>(ctx, mode, rec);
+            RET(seq_step<T>(ctx, mode, rec));
         }
     }
     ctx->ring_rows += n_steps;
