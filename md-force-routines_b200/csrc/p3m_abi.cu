@@ -22,6 +22,8 @@ struct p3m_ctx {
     cudaStream_t st = nullptr;
     cudaStream_t st2 = nullptr;   // the mesh branch of a step (joined back into st)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t st3 = nullptr;   // the n(q,t) branch of a step
+    cudaEvent_t ev_join3 = nullptr;
     int *counters = nullptr;      // [0] run step, [1] ring position, [2] it0, [3] n(q,t) rows,
                                   // [4] snapshots taken, [5] this step's snapshot slot
     int snap_interval = 0, snap_cap = 0;
@@ -217,6 +219,11 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->st3) {
+        cudaStreamSynchronize(ctx->st3);
+        cudaStreamDestroy(ctx->st3);
+    }
+    if (ctx->ev_join3) cudaEventDestroy(ctx->ev_join3);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
     return P3M_OK;
@@ -416,6 +423,8 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
     CKC(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
     CKC(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+    CKC(cudaStreamCreateWithFlags(&ctx->st3, cudaStreamNonBlocking));
+    CKC(cudaEventCreateWithFlags(&ctx->ev_join3, cudaEventDisableTiming));
     CKC(dalloc(&s.reps, n_reps));
     CKC(cudaMemcpy(s.reps, ctx->rh.data(), sizeof(RepDev) * n_reps, cudaMemcpyHostToDevice));
     {
@@ -581,11 +590,11 @@ template <typename T> static int seq_force(p3m_ctx *ctx, bool keys)
 
 // One integrator step of every replica (mode 0 NVE, 1 thermostat). After the
 // drift and the key scan the step forks: the mesh branch (brick sort,
-// assignment, FFTs, gather, and the n(q,t) sums of the new positions) runs
-// on the second stream while the particle branch (cell sort, lists, PP) runs
-// on the first -- they share no arrays -- and they join before the forces are
-// combined, so the latency-bound mesh kernels fill the SMs the PP kernel
-// leaves idle (one graph holds both branches).
+// assignment, FFTs, gather) runs on a second stream and the n(q,t) sums of the
+// new positions on a third, while the particle branch (cell sort, lists, PP)
+// runs on the first -- they share no arrays -- and they join before the
+// forces are combined, so the latency-bound mesh kernels fill the SMs the PP
+// kernel leaves idle (one graph holds all branches).
 template <typename T> static int seq_step(p3m_ctx *ctx, int mode, int record_nqt)
 {
     DevState &s = ctx->s;
@@ -599,19 +608,23 @@ template <typename T> static int seq_step(p3m_ctx *ctx, int mode, int record_nqt
     cudaError_t e = cudaSuccess;
     if (fork) {
         e = cudaEventRecord(ctx->ev_fork, st);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(st2, ctx->ev_fork, 0);
-        if (e == cudaSuccess) {
-            if (s.has_mesh) {
+        if (e == cudaSuccess && s.has_mesh) {
+            e = cudaStreamWaitEvent(st2, ctx->ev_fork, 0);
+            if (e == cudaSuccess) {
                 launch_sort_bricks(s, st2);
                 ctx->launches += 3;
                 seq_pm<T>(ctx, false, st2);
+                e = cudaEventRecord(ctx->ev_join, st2);
             }
-            if (rec) {  // positions of this step are final: row counters[3] of the ring
+        }
+        if (e == cudaSuccess && rec) {  // the new positions are final: ring row counters[3]
+            e = cudaStreamWaitEvent(ctx->st3, ctx->ev_fork, 0);
+            if (e == cudaSuccess) {
                 launch_nqt_partial<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nq_consecutive,
-                                      ctx->nqt_part, st2);
+                                      ctx->nqt_part, ctx->st3);
                 ctx->launches++;
+                e = cudaEventRecord(ctx->ev_join3, ctx->st3);
             }
-            e = cudaEventRecord(ctx->ev_join, st2);
         }
     }
     launch_scatter(s, st);
@@ -620,7 +633,8 @@ template <typename T> static int seq_step(p3m_ctx *ctx, int mode, int record_nqt
     launch_build_lists<T>(s, st);  // from those coordinates (rebuild steps)
     ctx->launches += 4;
     seq_pp<T>(ctx, false, st);
-    if (fork && e == cudaSuccess) e = cudaStreamWaitEvent(st, ctx->ev_join, 0);
+    if (e == cudaSuccess && s.has_mesh) e = cudaStreamWaitEvent(st, ctx->ev_join, 0);
+    if (e == cudaSuccess && rec) e = cudaStreamWaitEvent(st, ctx->ev_join3, 0);
     launch_kick_finish<T>(s, 1, nullptr, st);
     ctx->launches++;
     StepSums sums;  // the energy sums and this step's n(q,t) row, in the reduction
