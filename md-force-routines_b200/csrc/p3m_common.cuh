@@ -18,6 +18,8 @@ constexpr int TILE3 = TILE * TILE * TILE;
 
 // Lines per pencil tile in the FFT passes (consecutive y rows or z lines).
 constexpr int PENCIL = 16;
+constexpr int LOG_PENCIL = 4;
+static_assert(PENCIL == 1 << LOG_PENCIL, "PENCIL is 2^LOG_PENCIL");
 constexpr int MAX_LOGM = 8;  // M <= 256
 constexpr int PBLK = 256;      // particles per block in replica-aligned particle kernels
 

@@ -38,7 +38,7 @@
 
 namespace p3m {
 
-constexpr int FFT_THREADS = 256;
+constexpr int FFT_THREADS = 256;  // a multiple of the largest mesh side (256)
 constexpr int LS = PENCIL + 1;  // padded line stride of the shared tiles
 
 template <typename T> using cplx = typename C2<T>::t;
@@ -57,20 +57,20 @@ __device__ __forceinline__ void load_twiddles(cplx<T> *tw, const cplx<T> *g)
 // In-place radix-2 decimation-in-time FFT of `nlines` lines of length 2^logM
 // held in shared memory, element n of line l at buf[l * ls + n * es]; input
 // in bit-reversed order, output natural; unnormalised, the inverse uses
-// conjugate twiddles. Up to three consecutive radix-2 stages are done in
+// conjugate twiddles; nlines = 2^lognl. Up to three consecutive radix-2 stages are done in
 // registers on groups of 8 (4, 2) elements, so the data passes through shared
 // memory -- and the block through a barrier -- once per three stages. Thread
-// b takes line b % nlines, so consecutive threads touch consecutive lines.
+// b takes line b mod nlines, so consecutive threads touch consecutive lines.
 // Ends with a barrier.
 template <typename T, int LOGR>
-__device__ __forceinline__ void fft_group_pass(cplx<T> *buf, int logM, int ls, int es, int nlines,
+__device__ __forceinline__ void fft_group_pass(cplx<T> *buf, int logM, int ls, int es, int lognl,
                                                const cplx<T> *tw, bool inverse, int s)
 {
     constexpr int R = 1 << LOGR;
     const int half = 1 << s;           // distance of the first stage's pairs
-    const int ngroups = nlines * ((1 << logM) >> LOGR);
+    const int ngroups = 1 << (lognl + logM - LOGR);
     for (int b = threadIdx.x; b < ngroups; b += blockDim.x) {
-        const int l = b % nlines, g = b / nlines;
+        const int l = b & ((1 << lognl) - 1), g = b >> lognl;
         const int k = g & (half - 1), blk = g >> s;
         const int base = (blk << (s + LOGR)) + k;
         cplx<T> x[R];
@@ -97,20 +97,20 @@ __device__ __forceinline__ void fft_group_pass(cplx<T> *buf, int logM, int ls, i
 }
 
 template <typename T>
-__device__ void fft_lines(cplx<T> *buf, int logM, int ls, int es, int nlines, const cplx<T> *tw,
+__device__ void fft_lines(cplx<T> *buf, int logM, int ls, int es, int lognl, const cplx<T> *tw,
                           bool inverse)
 {
     int s = 0;
-    for (; s + 3 <= logM; s += 3) fft_group_pass<T, 3>(buf, logM, ls, es, nlines, tw, inverse, s);
-    if (logM - s == 2) fft_group_pass<T, 2>(buf, logM, ls, es, nlines, tw, inverse, s);
-    else if (logM - s == 1) fft_group_pass<T, 1>(buf, logM, ls, es, nlines, tw, inverse, s);
+    for (; s + 3 <= logM; s += 3) fft_group_pass<T, 3>(buf, logM, ls, es, lognl, tw, inverse, s);
+    if (logM - s == 2) fft_group_pass<T, 2>(buf, logM, ls, es, lognl, tw, inverse, s);
+    else if (logM - s == 1) fft_group_pass<T, 1>(buf, logM, ls, es, lognl, tw, inverse, s);
 }
 
 // PENCIL lines, element n of line l at buf[n * LS + l]
 template <typename T>
 __device__ __forceinline__ void fft_pencil(cplx<T> *buf, int logM, const cplx<T> *tw, bool inverse)
 {
-    fft_lines<T>(buf, logM, 1, LS, PENCIL, tw, inverse);
+    fft_lines<T>(buf, logM, 1, LS, LOG_PENCIL, tw, inverse);
 }
 
 // ---------------------------------------------------------------------------
@@ -329,27 +329,58 @@ k_assign_i32(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ 
     }
 }
 
-// Charge on node (x,y,z) of replica R: the sum of the (up to 8) brick tiles
-// that cover it, in a fixed order (dz, dy, dx), with all loads independent.
+// A node's charge is the sum of the (up to 8) brick tiles that cover it. Along
+// each axis node n lies in the tile of brick n / BRICK at offset n mod BRICK
+// and, when that offset is below HALO, also in the halo of the previous
+// (periodic) brick's tile at offset + BRICK. A tile element's address is a sum
+// of one term per axis, so each axis contributes two candidate offsets.
+struct AxisOff {
+    int a, b;  // offset in the own brick's tile, in the previous brick's halo
+    bool two;  // the halo term exists
+};
+
+// sb: elements between consecutive bricks along the axis; st: between
+// consecutive tile rows along the axis
+__device__ __forceinline__ AxisOff axis_off(int n, int nb, int sb, int st)
+{
+    const int bk = n / BRICK, o = n - bk * BRICK;
+    AxisOff r;
+    r.a = bk * sb + o * st;
+    r.b = (bk == 0 ? nb - 1 : bk - 1) * sb + (o + BRICK) * st;
+    r.two = o < HALO;
+    return r;
+}
+__device__ __forceinline__ AxisOff axis_x(int x, int nb) { return axis_off(x, nb, TILE3, 1); }
+__device__ __forceinline__ AxisOff axis_y(int y, int nb) { return axis_off(y, nb, nb * TILE3, TILE); }
+__device__ __forceinline__ AxisOff axis_z(int z, int nb)
+{
+    return axis_off(z, nb, nb * nb * TILE3, TILE * TILE);
+}
+
+// The sum over the covering tiles in a fixed order (dz, dy, dx), all loads
+// independent; t = the replica's tiles.
+template <typename T>
+__device__ __forceinline__ T rho_sum(const T *__restrict__ t, const AxisOff &X, const AxisOff &Y,
+                                     const AxisOff &Z)
+{
+    const int zy0 = Z.a + Y.a, zy1 = Z.a + Y.b, zy2 = Z.b + Y.a, zy3 = Z.b + Y.b;
+    const bool y1 = Y.two, z1 = Z.two;
+    const T v0 = __ldg(t + zy0 + X.a);
+    const T v1 = X.two ? __ldg(t + zy0 + X.b) : (T)0;
+    const T v2 = y1 ? __ldg(t + zy1 + X.a) : (T)0;
+    const T v3 = (y1 && X.two) ? __ldg(t + zy1 + X.b) : (T)0;
+    const T v4 = z1 ? __ldg(t + zy2 + X.a) : (T)0;
+    const T v5 = (z1 && X.two) ? __ldg(t + zy2 + X.b) : (T)0;
+    const T v6 = (z1 && y1) ? __ldg(t + zy3 + X.a) : (T)0;
+    const T v7 = (z1 && y1 && X.two) ? __ldg(t + zy3 + X.b) : (T)0;
+    return ((v0 + v1) + (v2 + v3)) + ((v4 + v5) + (v6 + v7));
+}
+
+// Charge on node (x,y,z) of replica R.
 template <typename T>
 __device__ __forceinline__ T rho_at(const RepDev &R, const T *__restrict__ tiles, int x, int y, int z)
 {
-    const int nb = R.nb;
-    const int bx = x / BRICK, by = y / BRICK, bz = z / BRICK;
-    const int ox = x - bx * BRICK, oy = y - by * BRICK, oz = z - bz * BRICK;
-    const bool hx = ox < HALO, hy = oy < HALO, hz = oz < HALO;
-    const int cx[2] = {bx, (bx - 1 + nb) % nb}, cy[2] = {by, (by - 1 + nb) % nb},
-              cz[2] = {bz, (bz - 1 + nb) % nb};
-    T v[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
-        const bool use = (!dx || hx) && (!dy || hy) && (!dz || hz);
-        const long long brick = cx[dx] + nb * (cy[dy] + (long long)nb * cz[dz]);
-        const int t = ((oz + dz * BRICK) * TILE + (oy + dy * BRICK)) * TILE + ox + dx * BRICK;
-        v[k] = use ? __ldg(tiles + R.tile_off + brick * TILE3 + t) : (T)0;
-    }
-    return ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
+    return rho_sum<T>(tiles + R.tile_off, axis_x(x, R.nb), axis_y(y, R.nb), axis_z(z, R.nb));
 }
 
 // ---------------------------------------------------------------------------
@@ -374,13 +405,14 @@ k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const T *__restrict__ til
         const int M = R.M, logM = R.logM, w = item - R.wa_off;
         const int nyt = M / (2 * PENCIL);
         const int z = w / nyt, y0 = (w % nyt) * (2 * PENCIL);
+        // blockDim.x is a multiple of M: each thread keeps one x
+        const int x = threadIdx.x & (M - 1);
+        const AxisOff X = axis_x(x, R.nb), Z = axis_z(z, R.nb);
+        const T *t = tiles + R.tile_off;
+        T *dst = reinterpret_cast<T *>(&buf[brev(x, logM) * LS]);
         __syncthreads();
-        for (int e = threadIdx.x; e < 2 * PENCIL * M; e += blockDim.x) {
-            const int x = e % M, j = e / M;
-            const T v = rho_at<T>(R, tiles, x, y0 + j, z);
-            T *dst = reinterpret_cast<T *>(&buf[brev(x, logM) * LS + (j >> 1)]);
-            dst[j & 1] = v;
-        }
+        for (int j = threadIdx.x >> logM; j < 2 * PENCIL; j += blockDim.x >> logM)
+            dst[j] = rho_sum<T>(t, X, axis_y(y0 + j, R.nb), Z);  // line j/2, part j%2
         __syncthreads();
         fft_pencil<T>(buf, logM, tw, false);
         // split the two real rows: Xa = (Z[k] + conj Z[M-k])/2, Xb = (Z[k] - conj Z[M-k])/2i
@@ -426,13 +458,13 @@ k_fft_y(const RepDev *__restrict__ reps, int nrep, cplx<T> *__restrict__ data, l
         cplx<T> *base = data + comp * stride + R.spec_off + ((long long)kx * M + z0) * M;
         __syncthreads();
         for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
-            const int y = e % M, l = e / M;
+            const int y = e & (M - 1), l = e >> logM;
             buf[brev(y, logM) * LS + l] = base[(long long)l * M + y];
         }
         __syncthreads();
         fft_pencil<T>(buf, logM, tw, inverse);
         for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
-            const int y = e % M, l = e / M;
+            const int y = e & (M - 1), l = e >> logM;
             base[(long long)l * M + y] = buf[y * LS + l];
         }
     }
@@ -542,8 +574,8 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
             A[brev(z, logM) * LD + brev(y, logM)] = spec[lbase + e];
         }
         __syncthreads();
-        fft_lines<T>(A, logM, LD, 1, M, tw, false);  // along y
-        fft_lines<T>(A, logM, 1, LD, M, tw, false);  // along z
+        fft_lines<T>(A, logM, LD, 1, logM, tw, false);  // along y
+        fft_lines<T>(A, logM, 1, LD, logM, tw, false);  // along z
         const double wkx = (kx == 0 || kx == (M >> 1)) ? 1.0 : 2.0;
         double u = 0.0;
         for (int e = threadIdx.x; e < MM; e += blockDim.x) {
@@ -563,9 +595,9 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
             A[zb * LD + yb] = make_c<T>(kz * ph.y, -kz * ph.x);  // -i kz phi
         }
         __syncthreads();
-        fft_lines<T>(A, logM, 1, LD, M, tw, true);  // z, of -i kz phi
-        fft_lines<T>(B, logM, 1, LD, M, tw, true);  // z, of phi: psi
-        fft_lines<T>(A, logM, LD, 1, M, tw, true);  // y: E_z
+        fft_lines<T>(A, logM, 1, LD, logM, tw, true);  // z, of -i kz phi
+        fft_lines<T>(B, logM, 1, LD, logM, tw, true);  // z, of phi: psi
+        fft_lines<T>(A, logM, LD, 1, logM, tw, true);  // y: E_z
         cplx<T> *Ez = ek + 2 * nspec + lbase;
         for (int e = threadIdx.x; e < MM; e += blockDim.x) {
             const int z = e >> logM, y = e & (M - 1);
@@ -580,8 +612,8 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
             A[z * LD + yb] = make_c<T>(ky * ps.y, -ky * ps.x);  // -i ky psi
         }
         __syncthreads();
-        fft_lines<T>(A, logM, LD, 1, M, tw, true);  // y: E_y
-        fft_lines<T>(B, logM, LD, 1, M, tw, true);  // y: IFFT(psi)
+        fft_lines<T>(A, logM, LD, 1, logM, tw, true);  // y: E_y
+        fft_lines<T>(B, logM, LD, 1, logM, tw, true);  // y: IFFT(psi)
         const T kxv = (kx == (M >> 1)) ? (T)0 : twopi_L * (T)kx;
         cplx<T> *Ey = ek + nspec + lbase;
         cplx<T> *Ex = ek + lbase;
@@ -623,7 +655,15 @@ k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
         for (int e = threadIdx.x; e < PENCIL * nk; e += blockDim.x) {
             const int l = e & (PENCIL - 1), k = e >> 4;
             const long long o = ((long long)k * M + z) * M + y0 + 2 * l;
-            const cplx<T> a = src[o], b = src[o + 1];
+            cplx<T> a, b;  // o is even: one 16-byte load in FP32
+            if constexpr (sizeof(T) == 4) {
+                const float4 ab = __ldg(reinterpret_cast<const float4 *>(src + o));
+                a = make_c<T>(ab.x, ab.y);
+                b = make_c<T>(ab.z, ab.w);
+            } else {
+                a = src[o];
+                b = src[o + 1];
+            }
             if (k == 0 || k == (M >> 1)) {
                 buf[brev(k, logM) * LS + l] = make_c<T>(a.x, b.x);
             } else {
@@ -635,7 +675,7 @@ k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
         fft_pencil<T>(buf, logM, tw, true);
         T *dst = efield + comp * nmesh + R.mesh_off + ((long long)z * M + y0) * M;
         for (int e = threadIdx.x; e < 2 * PENCIL * M; e += blockDim.x) {
-            const int x = e % M, j = e / M;
+            const int x = e & (M - 1), j = e >> logM;
             const cplx<T> v = buf[x * LS + (j >> 1)];
             dst[(long long)j * M + x] = (j & 1) ? v.y : v.x;
         }

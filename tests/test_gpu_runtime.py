@@ -225,10 +225,11 @@ def test_launch_count_grows():
         assert c.launch_count() - n0 >= 3 * 15
 
 
-@pytest.mark.parametrize("M", [64, 128])
+@pytest.mark.parametrize("M", [32, 64, 128])
 def test_pm_fp64_against_oracle_mesh_paths(M):
-    """PM force and energy at M = 64 (fused plane FFT) and M = 128 (multi-pass
-    FFT) against the oracle's numpy chain on the same influence function."""
+    """PM force and energy at M = 32 and 64 (fused plane FFT) and M = 128
+    (multi-pass FFT) against the oracle's numpy chain on the same influence
+    function."""
     from p3m_b200 import FP64, Context, Replica, gf_opt_device
 
     N = 4000
@@ -360,3 +361,4 @@ def test_async_state_copies_on_two_contexts():
     finally:
         for c in ctxs:
             c.close()
+
