@@ -359,7 +359,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
             mesh += (long long)M * M * M;
             spec += (long long)(M / 2 + 1) * M * M;
             tile += (long long)R.nb * R.nb * R.nb * TILE3;
-            wa += M * (M / (2 * PENCIL));
+            wa += M * (M >> (x_lines_log(R.logM) + 1));
             if (M <= plane_max_mesh()) {
                 wp += M / 2 + 1;
                 if (M > maxp) maxp = M;

@@ -20,6 +20,10 @@ constexpr int TILE3 = TILE * TILE * TILE;
 constexpr int PENCIL = 16;
 constexpr int LOG_PENCIL = 4;
 static_assert(PENCIL == 1 << LOG_PENCIL, "PENCIL is 2^LOG_PENCIL");
+// Complex lines per item of the x passes (two real rows each): 32, or M/2 for
+// M = 32, so each radix pass has a group for every one of 256 threads.
+constexpr int XL_MAX = 32;
+__host__ __device__ constexpr int x_lines_log(int logM) { return logM - 1 < 5 ? logM - 1 : 5; }
 constexpr int MAX_LOGM = 8;  // M <= 256
 constexpr int PBLK = 256;      // particles per block in replica-aligned particle kernels
 
@@ -43,7 +47,7 @@ struct RepDev {
     long long spec_off;    // offset into half spectra ((M/2+1) M^2)
     long long tile_off;    // offset into assignment tiles (nb^3 TILE^3)
     // work-item offsets of the mesh passes (prefix sums over replicas)
-    int wa_off;            // x-R2C / x-C2R items: M * M/(2 PENCIL)
+    int wa_off;            // x-R2C / x-C2R items: M * M/(2 x_lines)
     int wb_off;            // y-line items: (M/2+1) * M/PENCIL (multi-pass replicas)
     int wc_off;            // z-line items: (M/2+1) * M/PENCIL (multi-pass replicas)
     int wp_off;            // plane items: M/2+1 (replicas with M <= PLANE_MAX)

@@ -40,6 +40,7 @@ namespace p3m {
 
 constexpr int FFT_THREADS = 256;  // a multiple of the largest mesh side (256)
 constexpr int LS = PENCIL + 1;  // padded line stride of the shared tiles
+constexpr int LSX = XL_MAX + 1;  // the same for the x passes
 
 template <typename T> using cplx = typename C2<T>::t;
 
@@ -388,8 +389,8 @@ __device__ __forceinline__ T rho_at(const RepDev &R, const T *__restrict__ tiles
 // ---------------------------------------------------------------------------
 
 // Pass A: rows of the charge mesh (reduced from the tiles) -> R2C along x,
-// written transposed into spec[kx][z][y]. Item = (replica, z, 32-row tile);
-// two real rows share one complex line.
+// written transposed into spec[kx][z][y]. Item = (replica, z, tile of
+// 2 x_lines rows); two real rows share one complex line.
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS)
 k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const T *__restrict__ tiles,
@@ -403,26 +404,27 @@ k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const T *__restrict__ til
         const int r = find_rep(item, nrep, [&](int k) { return reps[k].wa_off; });
         const RepDev &R = reps[r];
         const int M = R.M, logM = R.logM, w = item - R.wa_off;
-        const int nyt = M / (2 * PENCIL);
-        const int z = w / nyt, y0 = (w % nyt) * (2 * PENCIL);
+        const int lnl = x_lines_log(logM), nrow = 2 << lnl;  // complex lines, real rows
+        const int nyt = M >> (lnl + 1);
+        const int z = w / nyt, y0 = (w % nyt) * nrow;
         // blockDim.x is a multiple of M: each thread keeps one x
         const int x = threadIdx.x & (M - 1);
-        const AxisOff X = axis_x(x, R.nb), Z = axis_z(z, R.nb);
+        const AxisOff ax = axis_x(x, R.nb), az = axis_z(z, R.nb);
         const T *t = tiles + R.tile_off;
-        T *dst = reinterpret_cast<T *>(&buf[brev(x, logM) * LS]);
+        T *dst = reinterpret_cast<T *>(&buf[brev(x, logM) * LSX]);
         __syncthreads();
-        for (int j = threadIdx.x >> logM; j < 2 * PENCIL; j += blockDim.x >> logM)
-            dst[j] = rho_sum<T>(t, X, axis_y(y0 + j, R.nb), Z);  // line j/2, part j%2
+        for (int j = threadIdx.x >> logM; j < nrow; j += blockDim.x >> logM)
+            dst[j] = rho_sum<T>(t, ax, axis_y(y0 + j, R.nb), az);  // line j/2, part j%2
         __syncthreads();
-        fft_pencil<T>(buf, logM, tw, false);
+        fft_lines<T>(buf, logM, 1, LSX, lnl, tw, false);
         // split the two real rows: Xa = (Z[k] + conj Z[M-k])/2, Xb = (Z[k] - conj Z[M-k])/2i
         const int nk = (M >> 1) + 1;
         cplx<T> *out = spec + R.spec_off;
-        for (int e = threadIdx.x; e < 2 * PENCIL * nk; e += blockDim.x) {
-            const int j = e & (2 * PENCIL - 1), k = e >> 5;
+        for (int e = threadIdx.x; e < nrow * nk; e += blockDim.x) {
+            const int j = e & (nrow - 1), k = e >> (lnl + 1);
             const int l = j >> 1;
-            const cplx<T> Z = buf[k * LS + l];
-            const cplx<T> Zm = buf[((M - k) & (M - 1)) * LS + l];
+            const cplx<T> Z = buf[k * LSX + l];
+            const cplx<T> Zm = buf[((M - k) & (M - 1)) * LSX + l];
             cplx<T> X;
             if ((j & 1) == 0) {
                 X.x = (T)0.5 * (Z.x + Zm.x);
@@ -629,7 +631,7 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
 }
 
 // Pass E: C2R along x of the three field spectra, written as real meshes
-// efield[c][z][y][x]. Item = (replica, component, z, 32-row tile); rows
+// efield[c][z][y][x]. Item = (replica, component, z, tile of 2 x_lines rows); rows
 // 2l and 2l+1 share complex line l: Z[k] = Xa[k] + i Xb[k] over the
 // Hermitian extension, with the imaginary parts at k = 0 and M/2 dropped.
 template <typename T>
@@ -647,13 +649,14 @@ k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
         const int r = find_rep(it, nrep, [&](int k) { return reps[k].wa_off; });
         const RepDev &R = reps[r];
         const int M = R.M, logM = R.logM, w = it - R.wa_off;
-        const int nyt = M / (2 * PENCIL);
-        const int z = w / nyt, y0 = (w % nyt) * (2 * PENCIL);
+        const int lnl = x_lines_log(logM), nrow = 2 << lnl;  // complex lines, real rows
+        const int nyt = M >> (lnl + 1);
+        const int z = w / nyt, y0 = (w % nyt) * nrow;
         const cplx<T> *src = ek + comp * nspec + R.spec_off;
         const int nk = (M >> 1) + 1;
         __syncthreads();
-        for (int e = threadIdx.x; e < PENCIL * nk; e += blockDim.x) {
-            const int l = e & (PENCIL - 1), k = e >> 4;
+        for (int e = threadIdx.x; e < (nk << lnl); e += blockDim.x) {
+            const int l = e & ((1 << lnl) - 1), k = e >> lnl;
             const long long o = ((long long)k * M + z) * M + y0 + 2 * l;
             cplx<T> a, b;  // o is even: one 16-byte load in FP32
             if constexpr (sizeof(T) == 4) {
@@ -665,18 +668,18 @@ k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
                 b = src[o + 1];
             }
             if (k == 0 || k == (M >> 1)) {
-                buf[brev(k, logM) * LS + l] = make_c<T>(a.x, b.x);
+                buf[brev(k, logM) * LSX + l] = make_c<T>(a.x, b.x);
             } else {
-                buf[brev(k, logM) * LS + l] = make_c<T>(a.x - b.y, a.y + b.x);
-                buf[brev(M - k, logM) * LS + l] = make_c<T>(a.x + b.y, b.x - a.y);
+                buf[brev(k, logM) * LSX + l] = make_c<T>(a.x - b.y, a.y + b.x);
+                buf[brev(M - k, logM) * LSX + l] = make_c<T>(a.x + b.y, b.x - a.y);
             }
         }
         __syncthreads();
-        fft_pencil<T>(buf, logM, tw, true);
+        fft_lines<T>(buf, logM, 1, LSX, lnl, tw, true);
         T *dst = efield + comp * nmesh + R.mesh_off + ((long long)z * M + y0) * M;
-        for (int e = threadIdx.x; e < 2 * PENCIL * M; e += blockDim.x) {
+        for (int e = threadIdx.x; e < nrow * M; e += blockDim.x) {
             const int x = e & (M - 1), j = e >> logM;
-            const cplx<T> v = buf[x * LS + (j >> 1)];
+            const cplx<T> v = buf[x * LSX + (j >> 1)];
             dst[(long long)j * M + x] = (j & 1) ? v.y : v.x;
         }
     }
@@ -892,6 +895,11 @@ template <typename T> static size_t plane_smem(int M)
     return (128 + 2 * (size_t)M * (M + 1)) * sizeof(cplx<T>);
 }
 
+template <typename T> static size_t x_smem(int maxM)
+{
+    return (128 + (size_t)maxM * LSX) * sizeof(cplx<T>);
+}
+
 template <typename K> static void set_smem(K kernel, size_t bytes)
 {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -903,10 +911,10 @@ template <typename T> void configure_mesh_kernels()
 {
     set_smem(k_assign<T>, assign_smem<T>());
     set_smem(k_assign_i32, 2 * TILE3 * sizeof(int));
-    set_smem(k_fft_x_r2c<T>, fft_smem<T>(256, 1));
+    set_smem(k_fft_x_r2c<T>, x_smem<T>(256));
     set_smem(k_fft_y<T>, fft_smem<T>(256, 1));
     set_smem(k_fft_z_green<T>, fft_smem<T>(256, 2));
-    set_smem(k_fft_x_c2r<T>, fft_smem<T>(256, 1));
+    set_smem(k_fft_x_c2r<T>, x_smem<T>(256));
     set_smem(k_gather<T>, GNBUF<T> * GTILE * sizeof(T));
     set_smem(k_fft_plane<T>, plane_smem<T>(PLANE_MAX));
 }
@@ -930,7 +938,7 @@ template <typename T> void launch_fft_forward(const DevState &s, cudaStream_t st
     using C = cplx<T>;
     const int maxM = s.max_mesh;
     const size_t sm1 = fft_smem<T>(maxM, 1), sm2 = fft_smem<T>(maxM, 2);
-    k_fft_x_r2c<T><<<grid_items(s.wa), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, (const T *)s.tiles,
+    k_fft_x_r2c<T><<<grid_items(s.wa), FFT_THREADS, x_smem<T>(maxM), st>>>(s.reps, s.nrep, (const T *)s.tiles,
                                                                 (C *)s.spec, (const C *)s.twiddle, s.wa);
     if (s.wb > 0) {
         k_fft_y<T><<<grid_items(s.wb), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, (C *)s.spec, s.nspec,
@@ -956,7 +964,7 @@ template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st
     if (s.wb > 0)
         k_fft_y<T><<<grid_items(3 * s.wb), FFT_THREADS, sm1, st>>>(s.reps, s.nrep, (C *)s.ek, s.nspec,
                                                                     3, (const C *)s.twiddle, s.wb, true);
-    k_fft_x_c2r<T><<<grid_items(3 * s.wa), FFT_THREADS, sm1, st>>>(
+    k_fft_x_c2r<T><<<grid_items(3 * s.wa), FFT_THREADS, x_smem<T>(s.max_mesh), st>>>(
         s.reps, s.nrep, (const C *)s.ek, s.nspec, (T *)s.efield, s.nmesh, (const C *)s.twiddle,
         s.wa);
 }
