@@ -390,7 +390,8 @@ def run_ours(args):
                        "pp_config": dict(zip(("threads_per_particle", "skin", "list_capacity"),
                                              ctx.pp_config())),
                        "list_rebuilds_per_replica_step": rebuilds / (len(reps) * args.steps),
-                       "autotune_ms_per_step": tuned["ms_per_step"] if tuned else None},
+                       "autotune_ms_per_step": tuned["ms_per_step"] if tuned else None,
+                       "autotune_final_ms_per_step": tuned.get("final_ms_per_step") if tuned else None},
             "gpu_launches": launches, "clocks": clocks}
 
     if not args.no_extras and rank == 0:

@@ -162,12 +162,13 @@ static void plan_lists(p3m_ctx *ctx, double skin_override, int tpi)
         const p3m_replica_desc &d = ctx->desc[r];
         RepDev &R = ctx->rh[r];
         double skin = skin_override >= 0.0 ? skin_override : (d.skin >= 0.0 ? d.skin : kDefaultSkin);
-        const double smax = d.box / 3.0 * (1.0 - 1e-12) - d.rc;  // keeps >= 3 cells per side
+        // rc + skin <= L/3 keeps >= 3 CELL_DIV cells per side, more than
+        // the stencil spans (no cell is visited twice)
+        const double smax = d.box / 3.0 * (1.0 - 1e-12) - d.rc;
         if (skin > smax) skin = smax > 0.0 ? smax : 0.0;
         R.skin = skin;
         R.rcl = d.rc + skin;
-        R.nc = (int)floor(d.box / R.rcl);
-        if (R.nc < 3) R.nc = 3;
+        R.nc = (int)floor(CELL_DIV * d.box / R.rcl);  // >= 6
         R.cellw = d.box / R.nc;
         R.inv_cellw = 1.0 / R.cellw;
         R.cell_off = cell;
@@ -377,7 +378,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
         }
         p += d.n;
         {
-            const int ncmax = (int)floor(d.box / d.rc);  // the finest grid any skin can ask for
+            const int ncmax = (int)floor(CELL_DIV * d.box / d.rc);  // the finest grid any skin asks for
             cell += ncmax * ncmax * ncmax;
         }
         blk += (d.n + PBLK - 1) / PBLK;

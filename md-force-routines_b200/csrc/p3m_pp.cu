@@ -98,19 +98,19 @@ __device__ __forceinline__ long long list_index(int s, int k, int maxnb)
 // ---------------------------------------------------------------------------
 // list build (rebuild steps only)
 // ---------------------------------------------------------------------------
-constexpr int LB_THREADS = 256;
+constexpr int LB_THREADS = 128;
 constexpr int LB_TPI = 8;                     // lanes per particle
 constexpr int LB_PPB = LB_THREADS / LB_TPI;   // particles per pass
-constexpr int LB_ITEMS = 4;                   // work items per cell
-template <typename T> __host__ __device__ constexpr int lb_scap() { return sizeof(T) == 4 ? 3072 : 1536; }
+template <typename T> __host__ __device__ constexpr int lb_scap() { return sizeof(T) == 4 ? 1024 : 512; }
+static_assert(CELL_STENCIL <= LB_THREADS, "one thread per stencil cell");
 
-// Work item (cell, c): the cell's home particles c*32 + 128 k + [0, 32), so a
-// cell's particles spread over four CTAs (a rebuild of a few replicas keeps
-// the GPU busy). The 27 neighbour cells' coordinates are staged in shared
-// memory in the fixed stencil order; the 8 lanes of a particle test 8
-// consecutive candidates per round, and a warp ballot gives each candidate
-// in range its place: the list holds the in-range candidates in stencil
-// order, as a scan by one thread would, with no padding.
+// One CTA per cell (about 10 particles: cells are (rc + skin)/2 wide). The
+// CELL_STENCIL neighbour cells' coordinates are staged in shared memory in
+// the fixed stencil order (x fastest, offsets -CELL_DIV .. CELL_DIV); the 8
+// lanes of a particle test 8 consecutive candidates per round, and a warp
+// ballot gives each candidate in range its place: the list holds the
+// in-range candidates in stencil order, as a scan by one thread would, with
+// no padding.
 template <typename T>
 __global__ void __launch_bounds__(LB_THREADS)
 k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
@@ -122,39 +122,48 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
     constexpr int SCAP = lb_scap<T>();
     extern __shared__ __align__(16) unsigned char lb_smem[];
     Q *stage = reinterpret_cast<Q *>(lb_smem);
-    __shared__ int pre[28];
-    __shared__ int nstart[27];
+    __shared__ int pre[CELL_STENCIL + 1];  // candidates before stencil cell k
+    __shared__ int nstart[CELL_STENCIL];   // first sorted index of stencil cell k
+    __shared__ int wsum[LB_THREADS / 32];
     const int tid = threadIdx.x, lane = tid & 31;
     const int sub = tid % LB_TPI;
     const int gshift = lane & ~(LB_TPI - 1);            // first lane of this particle's group
     const unsigned below = (1u << (lane & (LB_TPI - 1))) - 1u;
-    for (int item = blockIdx.x; item < ncell * LB_ITEMS; item += gridDim.x) {
-        const int hc = item / LB_ITEMS, part = item % LB_ITEMS;
+    for (int hc = blockIdx.x; hc < ncell; hc += gridDim.x) {
         const int r = find_rep(hc, nrep, [&](int k) { return reps[k].cell_off; });
         if (!rebuild[r]) continue;  // uniform over the block
         const int hstart = cell_start[hc], nhome = cell_start[hc + 1] - hstart;
-        if (part * LB_PPB >= nhome) continue;
+        if (nhome == 0) continue;
         const RepDev &R = reps[r];
         const int nc = R.nc, local = hc - R.cell_off;
         const int cx = local % nc, cy = (local / nc) % nc, cz = local / (nc * nc);
         const float sc = (float)(R.L / Coord<T>::scale);
         const float rl2 = (float)(R.rcl * R.rcl);
-        __syncthreads();
-        if (tid < 27) {
-            const int dx = tid % 3 - 1, dy = (tid / 3) % 3 - 1, dz = tid / 9 - 1;
+        __syncthreads();  // the previous cell is done with pre, nstart and stage
+        // stencil cell tid: its start and count; pre = exclusive prefix sum
+        int cntc = 0;
+        if (tid < CELL_STENCIL) {
+            const int dx = tid % CELL_SPAN - CELL_DIV, dy = (tid / CELL_SPAN) % CELL_SPAN - CELL_DIV,
+                      dz = tid / (CELL_SPAN * CELL_SPAN) - CELL_DIV;
             const int nx = (cx + dx + nc) % nc, ny = (cy + dy + nc) % nc, nz = (cz + dz + nc) % nc;
             const int nb = R.cell_off + nx + nc * (ny + nc * nz);
             nstart[tid] = cell_start[nb];
-            pre[tid + 1] = cell_start[nb + 1] - cell_start[nb];
+            cntc = cell_start[nb + 1] - cell_start[nb];
         }
-        __syncthreads();
-        if (tid == 0) {
-            pre[0] = 0;
-            for (int k = 0; k < 27; ++k) pre[k + 1] += pre[k];
+        int v = cntc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += t;
         }
+        if (lane == 31) wsum[tid >> 5] = v;
         __syncthreads();
-        const int total = pre[27];
-        for (int i0 = part * LB_PPB; i0 < nhome; i0 += LB_ITEMS * LB_PPB) {
+        for (int w = 0; w < (tid >> 5); ++w) v += wsum[w];
+        if (tid < CELL_STENCIL) pre[tid + 1] = v;
+        if (tid == 0) pre[0] = 0;
+        __syncthreads();
+        const int total = pre[CELL_STENCIL];
+        for (int i0 = 0; i0 < nhome; i0 += LB_PPB) {
             const int i = i0 + tid / LB_TPI;
             const bool have = i < nhome;
             const int s = hstart + i;
@@ -164,16 +173,19 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
             for (int w0 = 0; w0 < total; w0 += SCAP) {
                 const int wlen = min(SCAP, total - w0);
                 __syncthreads();
-                // warp w copies neighbour cells w, w + 8, ... (their particles
-                // are contiguous): the part of each that falls in this window
-                for (int cc = tid >> 5; cc < 27; cc += LB_THREADS / 32) {
-                    const int lo = max(pre[cc], w0), hi = min(pre[cc + 1], w0 + wlen);
-                    for (int g = lo + lane; g < hi; g += 32) {
-                        const int j = nstart[cc] + g - pre[cc];
-                        Q q = xq[j];
-                        q.w = j;  // the staged copy carries the sorted index
-                        stage[g - w0] = q;
+                // candidate g of the window: the stencil cell holding it by
+                // binary search over pre
+                for (int g = tid; g < wlen; g += LB_THREADS) {
+                    const int gg = w0 + g;
+                    int lo = 0, hi = CELL_STENCIL - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (pre[mid] <= gg) lo = mid; else hi = mid - 1;
                     }
+                    const int j = nstart[lo] + gg - pre[lo];
+                    Q q = xq[j];
+                    q.w = j;  // the staged copy carries the sorted index
+                    stage[g] = q;
                 }
                 __syncthreads();
                 for (int kb = 0; kb < wlen; kb += LB_TPI) {  // uniform over the block
@@ -397,8 +409,7 @@ template <typename T> void launch_quantize(const DevState &s, cudaStream_t st)
 template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st)
 {
     using Q = typename Coord<T>::Q;
-    const int items = s.ncell * LB_ITEMS;
-    const int grid = items < 148 * 8 ? items : 148 * 8;
+    const int grid = s.ncell < 148 * 16 ? s.ncell : 148 * 16;
     k_build_lists<T><<<grid, LB_THREADS, lb_scap<T>() * sizeof(Q), st>>>(
         s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.ncell,
         s.rebuild, s.status);

@@ -37,11 +37,14 @@ def _save(d):
         pass
 
 
-def tune(ctx, steps=40, warm=5, use_cache=True, candidates=None):
+def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3):
     """Time each (threads per particle, skin) candidate over `steps` NVE steps
-    (CUDA events on the context's stream) and install the fastest. Returns
-    {"choice": (tpi, skin), "ms_per_step": {...}}. Advances the system by
-    (warm + steps) steps per candidate."""
+    (CUDA events on the context's stream), time the `finalists` fastest again
+    over 2 `steps` (list rebuilds come every few tens of steps, so short runs
+    rank close candidates by chance) and install the fastest of those.
+    Returns {"choice": (tpi, skin), "ms_per_step": {...}, "final_ms_per_step":
+    {...}}. Advances the system by warm + steps per candidate and warm + 2
+    steps per finalist."""
     import torch
 
     sig = signature(ctx)
@@ -51,25 +54,32 @@ def tune(ctx, steps=40, warm=5, use_cache=True, candidates=None):
         max_skin = min(0.5 * r.rc for r in ctx.replicas)
         ctx.set_pp_config(tpi, min(skin, max_skin))
         return cache[sig]
-    times = {}
     stream = torch.cuda.ExternalStream(ctx.stream())
     max_skin = min(0.5 * r.rc for r in ctx.replicas)
-    for tpi, skin in (candidates or CANDIDATES):
-        if skin > max_skin:
-            continue
+
+    def timed(tpi, skin, n):
         ctx.set_pp_config(tpi, skin)
         ctx.run(warm, MODE_NVE, graph=True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        ctx.run(steps, MODE_NVE, graph=True, sync=False)
+        ctx.run(n, MODE_NVE, graph=True, sync=False)
         e1.record(stream)
         e1.synchronize()
-        times[f"{tpi},{skin}"] = e0.elapsed_time(e1) / steps
-    best = min(times, key=times.get)
+        return e0.elapsed_time(e1) / n
+
+    times = {}
+    for tpi, skin in (candidates or CANDIDATES):
+        if skin <= max_skin:
+            times[f"{tpi},{skin}"] = timed(tpi, skin, steps)
+    final = {}
+    for key in sorted(times, key=times.get)[:max(1, finalists)]:
+        tpi, skin = key.split(",")
+        final[key] = timed(int(tpi), float(skin), 2 * steps)
+    best = min(final, key=final.get)
     tpi, skin = best.split(",")
     choice = (int(tpi), float(skin))
     ctx.set_pp_config(*choice)
-    result = {"choice": choice, "ms_per_step": times}
+    result = {"choice": choice, "ms_per_step": times, "final_ms_per_step": final}
     if use_cache:
         cache[sig] = result
         _save(cache)

@@ -362,3 +362,25 @@ def test_async_state_copies_on_two_contexts():
         for c in ctxs:
             c.close()
 
+
+
+def test_autotune_installs_a_finalist():
+    """The PP autotuner times the candidates, re-times the fastest and
+    installs the best finalist."""
+    from p3m_b200 import FP32, Context, Replica
+    from p3m_b200.autotune import tune
+
+    N = 3000
+    L = (4 * np.pi * N / 3) ** (1 / 3)
+    r = Replica(N=N, L=L, kappa=1.0, alpha=0.8, rc=L / 4, M=32)  # skins up to L/3 - rc = 1.2
+    pos, vel = _init_state(r, 9)
+    with Context([r, r], precision=FP32) as c:
+        c.set_state_all(np.concatenate([pos, pos]), np.concatenate([vel, vel]))
+        c.init_forces()
+        res = tune(c, steps=10, use_cache=False, candidates=[(1, 0.5), (2, 0.8), (4, 1.1)],
+                   finalists=2)
+        assert len(res["ms_per_step"]) == 3 and len(res["final_ms_per_step"]) == 2
+        best = min(res["final_ms_per_step"], key=res["final_ms_per_step"].get)
+        assert tuple(res["choice"]) == (int(best.split(",")[0]), float(best.split(",")[1]))
+        tpi, skin, _ = c.pp_config()
+        assert (tpi, skin) == tuple(res["choice"])
