@@ -714,6 +714,13 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
 {
     extern __shared__ __align__(16) unsigned char g_smem[];
     T *tile = reinterpret_cast<T *>(g_smem);
+    // per thread of the chunk: its particle (slot p, or -1), node offsets,
+    // local tile offset of the stencil's first node (or -1)
+    __shared__ int g_src[G_THREADS];
+    __shared__ T g_o[3][G_THREADS];
+    __shared__ int g_base[G_THREADS];
+    __shared__ int g_cnt[32];
+    const int lane = threadIdx.x & 31;
     for (int b = blockIdx.x; b < nbrick; b += gridDim.x) {
         const int r = find_rep(b, nrep, [&](int k) { return reps[k].brick_off; });
         const RepDev &R = reps[r];
@@ -722,12 +729,17 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                   bz = (local / (nb * nb)) * BRICK;
         const int p0 = brick_start[b], p1 = brick_start[b + 1];
         for (int c0 = p0; c0 < p1; c0 += G_THREADS) {
-            T wx[6], wy[6], wz[6];
-            int base = -1;  // local tile offset of the stencil's first node, or -1
-            T e[3] = {(T)0, (T)0, (T)0};
-            const int p = c0 + threadIdx.x;
-            if (p < p1) {
-                const int i = brick_perm[p];
+            // Lanes of a warp read their particles' stencils at the same
+            // offsets from different bases, so two lanes whose bases share a
+            // shared-memory bank conflict on every read. The chunk's particles
+            // are ranked by bank (base mod 32) and dealt round-robin to the
+            // warps: each warp gets bases spread over the banks. Which thread
+            // handles a particle does not change its sums.
+            const int nch = min(G_THREADS, p1 - c0);
+            int bank = 0, rank = 0, base0 = -1;
+            T ox0 = 0, oy0 = 0, oz0 = 0;
+            if (threadIdx.x < nch) {
+                const int i = brick_perm[c0 + threadIdx.x];
                 double ox, oy, oz;
                 const int ix = base_offset(pos[3 * i + 0], R.h, ox);
                 const int iy = base_offset(pos[3 * i + 1], R.h, oy);
@@ -736,11 +748,48 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                 // (a particle outside [-L, 2L) was flagged by the key pass)
                 if ((unsigned)lx < (unsigned)BRICK && (unsigned)ly < (unsigned)BRICK &&
                     (unsigned)lz < (unsigned)BRICK) {
-                    base = (lz * TILE + ly) * GTX + lx;
-                    weights6<T>((T)ox, wx);
-                    weights6<T>((T)oy, wy);
-                    weights6<T>((T)oz, wz);
+                    base0 = (lz * TILE + ly) * GTX + lx;
+                    bank = base0 & 31;
                 }
+                ox0 = (T)ox;
+                oy0 = (T)oy;
+                oz0 = (T)oz;
+            }
+            __syncthreads();  // the previous chunk / brick is done with g_* and the buffers
+            g_src[threadIdx.x] = -1;
+            if (threadIdx.x < 32) g_cnt[threadIdx.x] = 0;
+            __syncthreads();
+            if (threadIdx.x < nch) rank = atomicAdd(&g_cnt[bank], 1);
+            __syncthreads();
+            if (threadIdx.x < 32) {  // exclusive scan of the bank counts
+                const int v = g_cnt[lane];
+                int x = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += t;
+                }
+                g_cnt[lane] = x - v;
+            }
+            __syncthreads();
+            if (threadIdx.x < nch) {
+                const int q = g_cnt[bank] + rank, nw = (nch + 31) >> 5;
+                const int tgt = (q % nw) * 32 + q / nw;
+                g_src[tgt] = c0 + threadIdx.x;
+                g_o[0][tgt] = ox0;
+                g_o[1][tgt] = oy0;
+                g_o[2][tgt] = oz0;
+                g_base[tgt] = base0;
+            }
+            __syncthreads();
+            const int p = g_src[threadIdx.x];
+            T wx[6], wy[6], wz[6];
+            const int base = p >= 0 ? g_base[threadIdx.x] : -1;
+            T e[3] = {(T)0, (T)0, (T)0};
+            if (base >= 0) {
+                weights6<T>(g_o[0][threadIdx.x], wx);
+                weights6<T>(g_o[1][threadIdx.x], wy);
+                weights6<T>(g_o[2][threadIdx.x], wz);
             }
             // component tiles through NBUF buffers: with two, the copy of
             // component c+1 is in flight while component c is summed
@@ -758,7 +807,6 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                 }
                 asm volatile("cp.async.commit_group;\n" ::: "memory");
             };
-            __syncthreads();  // the previous chunk / brick is done with the buffers
             issue(0);
             for (int comp = 0; comp < 3; ++comp) {
                 if (GNBUF<T> == 2 && comp + 1 < 3) {
@@ -794,7 +842,7 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                     __syncthreads();  // buffer (comp % 2) is refilled next
                 }
             }
-            if (p < p1) {
+            if (p >= 0) {
                 typename V4<T>::t out;
                 out.x = e[0];
                 out.y = e[1];
