@@ -264,6 +264,9 @@ k_assign_i32(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ 
     extern __shared__ __align__(16) int a32_smem[];
     int *thi = a32_smem;
     int *tlo = a32_smem + TILE3;
+    __shared__ int a_src[A32_THREADS];  // the chunk's particle slot of each thread, or -1
+    __shared__ int a_cnt[32];
+    const int lane = threadIdx.x & 31;
     for (int b = blockIdx.x; b < nbrick; b += gridDim.x) {
         const int r = find_rep(b, nrep, [&](int k) { return reps[k].brick_off; });
         const RepDev &R = reps[r];
@@ -285,7 +288,46 @@ k_assign_i32(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ 
             tlo[k] = 0;
         }
         __syncthreads();
-        for (int p = p0 + threadIdx.x; p < p0 + n; p += A32_THREADS) {
+        for (int c0 = p0; c0 < p0 + n; c0 += A32_THREADS) {
+            // The lanes of a warp add at the same offsets from their
+            // particles' stencil bases: lanes whose bases share a shared-memory
+            // bank conflict on every atomic. The chunk's particles are ranked
+            // by bank (from floor(x / h) by multiplication: only the balance
+            // depends on it) and dealt round-robin to the warps. Integer sums
+            // do not depend on which thread adds what.
+            const int nch = min(A32_THREADS, p0 + n - c0);
+            int bank = 0, rank = 0;
+            if (threadIdx.x < nch) {
+                const int i = brick_perm[c0 + threadIdx.x];
+                const int qx = wrapM((int)floor(pos[3 * i + 0] * R.inv_h), M) - bx;
+                const int qy = wrapM((int)floor(pos[3 * i + 1] * R.inv_h), M) - by;
+                const int qz = wrapM((int)floor(pos[3 * i + 2] * R.inv_h), M) - bz;
+                bank = (int)((((unsigned)qz * TILE + (unsigned)qy) * TILE + (unsigned)qx) & 31u);
+            }
+            __syncthreads();  // the previous chunk is done with a_src
+            a_src[threadIdx.x] = -1;
+            if (threadIdx.x < 32) a_cnt[threadIdx.x] = 0;
+            __syncthreads();
+            if (threadIdx.x < nch) rank = atomicAdd(&a_cnt[bank], 1);
+            __syncthreads();
+            if (threadIdx.x < 32) {  // exclusive scan of the bank counts
+                const int v = a_cnt[lane];
+                int x = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += t;
+                }
+                a_cnt[lane] = x - v;
+            }
+            __syncthreads();
+            if (threadIdx.x < nch) {
+                const int q = a_cnt[bank] + rank, nw = (nch + 31) >> 5;
+                a_src[(q % nw) * 32 + q / nw] = c0 + threadIdx.x;
+            }
+            __syncthreads();
+            const int p = a_src[threadIdx.x];
+            if (p < 0) continue;
             const int i = brick_perm[p];
             double ox, oy, oz;
             const int ix = base_offset(pos[3 * i + 0], R.h, ox);
