@@ -215,6 +215,16 @@ int p3m_set_state_all_async(p3m_ctx *ctx, const double *pos, const double *vel, 
                             int keep_lists);
 int p3m_get_state_all_async(p3m_ctx *ctx, double *pos, double *vel, double *acc);
 
+/* What velocity_verlet_p3m_ord6.update (velocity_verlet_p3m_ord6.py:8-30)
+ * hands back after a step -- the updated pos, vel, acc and the energies --
+ * queued on the context's stream like p3m_get_state_all_async, for a caller
+ * that keeps its state in host arrays: energies (may be NULL) receives
+ * (U, K, T, thermostat factor) of every replica after the last step, (R, 4).
+ * The device status word is staged with the copies, so the next p3m_sync
+ * waits for the stream and reads no more device memory (unless more work
+ * was queued after this call); energies is written when p3m_sync returns. */
+int p3m_get_step_async(p3m_ctx *ctx, double *pos, double *vel, double *acc, double *energies);
+
 /* Compute acc for the uploaded positions of all replicas (the driver's
  * initial force call, yukawa_MD_p3m_ord6.py:171). */
 int p3m_init_forces(p3m_ctx *ctx);

@@ -45,6 +45,11 @@ struct p3m_ctx {
     int tmp_nq_cap = 0;
     double *hbuf = nullptr;       // pinned host staging
     size_t hbuf_bytes = 0;
+    // p3m_get_step_async: pinned copy of rep_out ([R][8]) and the status word
+    double *h_step = nullptr;
+    double *step_out = nullptr;   // caller's (R, 4) energies, filled at p3m_sync
+    bool step_pending = false;
+    long long step_launches = 0;  // launches when the copies were queued
     bool state_set = false;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     long long graph_kernels[2][2] = {{0, 0}, {0, 0}};  // kernels each graph launches
@@ -214,6 +219,7 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (ctx->hbuf) cudaFreeHost(ctx->hbuf);
+    if (ctx->h_step) cudaFreeHost(ctx->h_step);
     if (ctx->st2) {
         cudaStreamSynchronize(ctx->st2);
         cudaStreamDestroy(ctx->st2);
@@ -686,21 +692,26 @@ static int d2h(p3m_ctx *ctx, void *dst, const void *src, size_t bytes)
     return P3M_OK;
 }
 
+// A device status word read back: clear it on the device and report it.
+static int status_error(p3m_ctx *ctx, int st)
+{
+    if (!st) return P3M_OK;
+    CK(cudaMemset(ctx->s.status, 0, sizeof(int)));
+    if (st & ST_BOX) return fail(ctx, P3M_EBOX, "particle outside [-L, 2L) or non-finite position", "");
+    if (st & ST_NONFINITE) return fail(ctx, P3M_ENONFINITE, "non-finite force or energy", "");
+    if (st & ST_NBOVF)
+        return fail(ctx, P3M_ENBOVF, "a particle has more neighbours than the list holds",
+                    "raise the capacity with a smaller skin or report the density");
+    return P3M_OK;
+}
+
 static int finish(p3m_ctx *ctx)
 {
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->st));
     int st = 0;
     CK(cudaMemcpy(&st, ctx->s.status, sizeof(int), cudaMemcpyDeviceToHost));
-    if (st) {
-        CK(cudaMemset(ctx->s.status, 0, sizeof(int)));
-        if (st & ST_BOX) return fail(ctx, P3M_EBOX, "particle outside [-L, 2L) or non-finite position", "");
-        if (st & ST_NONFINITE) return fail(ctx, P3M_ENONFINITE, "non-finite force or energy", "");
-        if (st & ST_NBOVF)
-            return fail(ctx, P3M_ENBOVF, "a particle has more neighbours than the list holds",
-                        "raise the capacity with a smaller skin or report the density");
-    }
-    return P3M_OK;
+    return status_error(ctx, st);
 }
 
 static int compat_check(p3m_ctx *ctx, int replica)
@@ -1120,6 +1131,22 @@ extern "C" int p3m_get_state_all_async(p3m_ctx *ctx, double *pos, double *vel, d
     return get_state_all(ctx, pos, vel, acc, false);
 }
 
+extern "C" int p3m_get_step_async(p3m_ctx *ctx, double *pos, double *vel, double *acc,
+                                  double *energies)
+{
+    RET(get_state_all(ctx, pos, vel, acc, false));
+    const size_t nrep = (size_t)ctx->nrep;
+    if (!ctx->h_step) CK(cudaHostAlloc(&ctx->h_step, sizeof(double) * (8 * nrep + 1), cudaHostAllocDefault));
+    CK(cudaMemcpyAsync(ctx->h_step, ctx->s.rep_out, sizeof(double) * 8 * nrep, cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CK(cudaMemcpyAsync(ctx->h_step + 8 * nrep, ctx->s.status, sizeof(int), cudaMemcpyDeviceToHost,
+                       ctx->st));
+    ctx->step_out = energies;
+    ctx->step_pending = true;
+    ctx->step_launches = ctx->launches;
+    return P3M_OK;
+}
+
 template <typename T> static int do_init_forces(p3m_ctx *ctx)
 {
     RET(seq_force<T>(ctx, true));
@@ -1357,7 +1384,25 @@ extern "C" int p3m_sync(p3m_ctx *ctx)
 {
     if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
     CK(cudaSetDevice(ctx->device));
-    return finish(ctx);  // waits, then reports a device status raised meanwhile
+    if (!ctx->step_pending) return finish(ctx);  // waits, then reports a device status
+    // copies of p3m_get_step_async are queued: wait, deliver the energies
+    ctx->step_pending = false;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+    const double *h = ctx->h_step;
+    if (ctx->step_out)
+        for (int r = 0; r < ctx->nrep; ++r) {
+            double *o = ctx->step_out + 4 * (size_t)r;
+            o[0] = h[8 * r + RO_U];
+            o[1] = h[8 * r + RO_K];
+            o[2] = h[8 * r + RO_T];
+            o[3] = h[8 * r + RO_FACT];
+        }
+    ctx->step_out = nullptr;
+    if (ctx->launches != ctx->step_launches) return finish(ctx);  // later work: read the status now
+    int st;
+    memcpy(&st, h + 8 * (size_t)ctx->nrep, sizeof st);
+    return status_error(ctx, st);
 }
 
 extern "C" int p3m_set_pp_config(p3m_ctx *ctx, int tpi, double skin)

@@ -87,6 +87,7 @@ SIGNATURES = {
     "p3m_get_state_all": (_I, [_V, _D, _D, _D]),
     "p3m_set_state_all_async": (_I, [_V, _D, _D, _D, _I]),
     "p3m_get_state_all_async": (_I, [_V, _D, _D, _D]),
+    "p3m_get_step_async": (_I, [_V, _D, _D, _D, _D]),
     "p3m_set_t_desired": (_I, [_V, _D]),
     "p3m_init_forces": (_I, [_V]),
     "p3m_set_nqt": (_I, [_V, _D, _I, _I]),

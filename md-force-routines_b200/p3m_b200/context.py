@@ -240,6 +240,20 @@ class Context:
         self._ck(fn(self.handle, dptr(pos), dptr(vel), dptr(acc)))
         return pos, vel, acc
 
+    def get_step_async(self, pos, vel, acc, energies):
+        """Queue the copies of the state and of every replica's (U, K, T,
+        thermostat factor) after the last step, (R, 4), into the given arrays;
+        they hold the values once sync() returns (which then needs no further
+        device read). Pass pinned arrays for full copy speed."""
+        if any(a is None for a in (pos, vel, acc, energies)):
+            raise ValueError("asynchronous reads need the four output arrays")
+        n = sum(r.N for r in self.replicas)
+        for a in (pos, vel, acc):
+            _out(a, (n, 3))
+        _out(energies, (len(self.replicas), 4))
+        self._ck(lib().p3m_get_step_async(self.handle, dptr(pos), dptr(vel), dptr(acc),
+                                          dptr(energies)))
+
     def set_t_desired(self, t_desired):
         """Thermostat targets for the following thermostat-mode runs: one
         value per replica, or one for all."""

@@ -384,3 +384,41 @@ def test_autotune_installs_a_finalist():
         assert tuple(res["choice"]) == (int(best.split(",")[0]), float(best.split(",")[1]))
         tpi, skin, _ = c.pp_config()
         assert (tpi, skin) == tuple(res["choice"])
+
+
+def test_get_step_async_matches_sync_reads():
+    """p3m_get_step_async + p3m_sync deliver the state and the last step's
+    (U, K, T, factor) that the synchronous reads give, and a device status
+    raised by the step (a particle still outside [-L, 2L) after the step's
+    periodic wrap) still surfaces at p3m_sync."""
+    import torch
+
+    from p3m_b200 import FP32, MODE_NVE, Context, P3MError, Replica
+
+    N = 3000
+    L = (4 * np.pi * N / 3) ** (1 / 3)
+    reps = [Replica(N=N, L=L, kappa=1.0, alpha=0.8, rc=L / 3.2, M=32, seed=s) for s in (4, 5)]
+    st = [_init_state(r, r.seed) for r in reps]
+    pos = np.concatenate([p for p, _ in st])
+    vel = np.concatenate([v for _, v in st])
+    hb = [torch.empty((2 * N, 3), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+    en = torch.empty((2, 4), dtype=torch.float64, pin_memory=True).numpy()
+    with Context(reps, precision=FP32) as c:
+        c.set_state_all(pos, vel)
+        c.init_forces()
+        c.run(3, MODE_NVE, sync=False)
+        c.get_step_async(*hb, en)
+        c.sync()
+        p, v, a = c.get_state_all()
+        E = c.energies(max_steps=1)[0]
+        for x, y in zip(hb, (p, v, a)):
+            assert np.array_equal(x, y)
+        assert np.array_equal(en, E)
+        bad = p.copy()
+        bad[7, 0] = 3.5 * L  # one wrap (velocity_verlet_p3m_ord6.py:16-19) leaves 2.5 L
+        c.set_state_all(bad, v, a, keep_lists=True, sync=False)
+        c.run(1, MODE_NVE, sync=False)
+        c.get_step_async(*hb, en)
+        with pytest.raises(P3MError) as e:
+            c.sync()
+        assert e.value.code == -4
