@@ -209,7 +209,7 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
     void *ptrs[] = {s.reps, s.pos, s.vel, s.acc, s.charge, s.prep, s.cell_key, s.cell_count,
                     s.cell_start, s.cell_cursor, s.cell_tmp, s.cell_perm, s.cell_slot, s.xq, s.nnb,
                     s.cell_sub,
-                    s.nlist, s.rebuild, s.pos_ref, s.pp_tables,
+                    s.nlist, s.rebuild, s.rb_list, s.pos_ref, s.pp_tables,
                     s.acc_pp, s.brick_key, s.brick_count, s.brick_start, s.brick_cursor,
                     s.brick_perm, s.brick_slot, s.brick_hist, s.tiles, s.spec, s.ek, s.green, s.efield,
                     s.acc_pm, s.twiddle, s.u_pp_part, s.u_pm_part, s.kin_part, s.rep_out,
@@ -462,6 +462,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     ctx->nlist_cap = (long long)((p + 31) / 32) * 32 * s.maxnb;
     CKC(dalloc(&s.nlist, (size_t)ctx->nlist_cap));
     CKC(dalloc(&s.rebuild, (size_t)n_reps));
+    CKC(dalloc(&s.rb_list, (size_t)2 * n_reps + 2));
     CKC(dalloc(&s.pos_ref, (size_t)3 * p));
     CKC(dalloc(&s.cell_tmp, (size_t)p));
     CKC(dalloc(&s.cell_perm, (size_t)p));

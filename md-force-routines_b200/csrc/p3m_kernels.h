@@ -36,6 +36,9 @@ struct DevState {
     int *cell_sub = nullptr;     // [particle] sub-cell Morton code (rebuild steps)
     int *nlist = nullptr;        // neighbour lists (sorted indices), warp-interleaved
     int *rebuild = nullptr;      // per-replica flags: rebuild cells and lists this step
+    // the replicas rebuilding this step (written by k_scan): [0] = count k,
+    // [1 .. k] replica indices, [nrep + 1 + j] = cells of the first j of them
+    int *rb_list = nullptr;
     double *pos_ref = nullptr;   // positions at the last rebuild (ntot,3)
     float4 *pp_tables = nullptr; // FP32 pair tables: cubic of psi = phi r, [nrep][PP_TABLE_N]
     void *acc_pp = nullptr;      // V4<T> PP acceleration, cell-sorted order

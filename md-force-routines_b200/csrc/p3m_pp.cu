@@ -98,16 +98,17 @@ __device__ __forceinline__ long long list_index(int s, int k, int maxnb)
 // ---------------------------------------------------------------------------
 // list build (rebuild steps only)
 // ---------------------------------------------------------------------------
-constexpr int LB_THREADS = 128;
-constexpr int LB_TPI = 8;                     // lanes per particle
+constexpr int LB_THREADS = 256;
+constexpr int LB_TPI = 16;                    // lanes per particle
 constexpr int LB_PPB = LB_THREADS / LB_TPI;   // particles per pass
 template <typename T> __host__ __device__ constexpr int lb_scap() { return sizeof(T) == 4 ? 1024 : 512; }
 static_assert(CELL_STENCIL <= LB_THREADS, "one thread per stencil cell");
 
-// One CTA per cell (about 10 particles: cells are (rc + skin)/2 wide). The
-// CELL_STENCIL neighbour cells' coordinates are staged in shared memory in
-// the fixed stencil order (x fastest, offsets -CELL_DIV .. CELL_DIV); the 8
-// lanes of a particle test 8 consecutive candidates per round, and a warp
+// One CTA per cell (about 10 particles: cells are (rc + skin)/2 wide) of the
+// replicas rebuilding this step (the list k_scan wrote). The CELL_STENCIL
+// neighbour cells' coordinates are staged in shared memory in the fixed
+// stencil order (x fastest, offsets -CELL_DIV .. CELL_DIV); the LB_TPI lanes
+// of a particle test LB_TPI consecutive candidates per round, and a warp
 // ballot gives each candidate in range its place: the list holds the
 // in-range candidates in stencil order, as a scan by one thread would, with
 // no padding.
@@ -115,7 +116,7 @@ template <typename T>
 __global__ void __launch_bounds__(LB_THREADS)
 k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
               const typename Coord<T>::Q *__restrict__ xq, int *__restrict__ nnb,
-              int *__restrict__ nlist, int maxnb, int ncell, const int *__restrict__ rebuild,
+              int *__restrict__ nlist, int maxnb, const int *__restrict__ rb_list, int nrep_all,
               int *status)
 {
     using Q = typename Coord<T>::Q;
@@ -129,9 +130,12 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
     const int sub = tid % LB_TPI;
     const int gshift = lane & ~(LB_TPI - 1);            // first lane of this particle's group
     const unsigned below = (1u << (lane & (LB_TPI - 1))) - 1u;
-    for (int hc = blockIdx.x; hc < ncell; hc += gridDim.x) {
-        const int r = find_rep(hc, nrep, [&](int k) { return reps[k].cell_off; });
-        if (!rebuild[r]) continue;  // uniform over the block
+    const int nrb = rb_list[0];
+    const int *rb_cells = rb_list + nrep_all + 1;
+    for (int item = blockIdx.x; item < rb_cells[nrb]; item += gridDim.x) {
+        const int k = find_rep(item, nrb, [&](int j) { return rb_cells[j]; });
+        const int r = rb_list[1 + k];
+        const int hc = reps[r].cell_off + item - rb_cells[k];
         const int hstart = cell_start[hc], nhome = cell_start[hc + 1] - hstart;
         if (nhome == 0) continue;
         const RepDev &R = reps[r];
@@ -200,7 +204,8 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                         j = (int)q.w;
                         in = (dx * dx + dy * dy + dz * dz < rl2) && j != s;
                     }
-                    const unsigned grp = (__ballot_sync(0xffffffffu, in) >> gshift) & 0xffu;
+                    const unsigned grp = (__ballot_sync(0xffffffffu, in) >> gshift) &
+                                         ((1u << LB_TPI) - 1u);
                     if (in) {
                         const int pos = cnt + __popc(grp & below);
                         if (pos < maxnb) nlist[list_index(s, pos, maxnb)] = j;
@@ -411,8 +416,8 @@ template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st
     using Q = typename Coord<T>::Q;
     const int grid = s.ncell < 148 * 16 ? s.ncell : 148 * 16;
     k_build_lists<T><<<grid, LB_THREADS, lb_scap<T>() * sizeof(Q), st>>>(
-        s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.ncell,
-        s.rebuild, s.status);
+        s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.rb_list, s.nrep,
+        s.status);
 }
 
 template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cudaStream_t st)

@@ -109,16 +109,28 @@ __device__ void block_scan_array(int *count, int *start, int *cursor, int n, int
 // its own particle range [p_off, p_off + n). Block 1: all bricks.
 __global__ void k_scan(const RepDev *__restrict__ reps, int nrep, int *cell_count,
                        int *cell_start, int *cell_cursor, int *brick_count, int *brick_start,
-                       int *brick_cursor, int nbrick, const int *__restrict__ rebuild)
+                       int *brick_cursor, int nbrick, const int *__restrict__ rebuild,
+                       int *__restrict__ rb_list)
 {
     __shared__ int sm[64];
     if (blockIdx.x == 0) {
+        int k = 0, cells = 0;
         for (int r = 0; r < nrep; ++r) {
             if (!rebuild[r]) continue;
             const RepDev &R = reps[r];
             const int c0 = R.cell_off, nc = R.nc * R.nc * R.nc;
             block_scan_array(cell_count + c0, cell_start + c0, cell_cursor + c0, nc, R.p_off, sm);
+            if (threadIdx.x == 0) {
+                rb_list[1 + k] = r;
+                rb_list[nrep + 1 + k] = cells;
+            }
+            ++k;
+            cells += nc;
             __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            rb_list[0] = k;
+            rb_list[nrep + 1 + k] = cells;
         }
     } else if (nbrick > 0) {
         block_scan_array(brick_count, brick_start, brick_cursor, nbrick, 0, sm);
@@ -295,7 +307,7 @@ void launch_scan(const DevState &s, cudaStream_t st)
 {
     k_scan<<<2, 1024, 0, st>>>(s.reps, s.nrep, s.cell_count, s.cell_start, s.cell_cursor,
                                s.brick_count, s.brick_start, s.brick_cursor,
-                               s.has_mesh ? s.nbrick : 0, s.rebuild);
+                               s.has_mesh ? s.nbrick : 0, s.rebuild, s.rb_list);
 }
 
 void launch_scatter(const DevState &s, cudaStream_t st)
