@@ -97,14 +97,38 @@ __device__ __forceinline__ void fft_group_pass(cplx<T> *buf, int logM, int ls, i
     __syncthreads();
 }
 
-template <typename T>
-__device__ void fft_lines(cplx<T> *buf, int logM, int ls, int es, int lognl, const cplx<T> *tw,
-                          bool inverse)
+// The passes of one line length 2^LOGM from stage S on, unrolled at compile
+// time (stage offsets, group counts and twiddle strides become constants).
+template <typename T, int LOGM, int S = 0>
+__device__ __forceinline__ void fft_lines_t(cplx<T> *buf, int ls, int es, int lognl,
+                                            const cplx<T> *tw, bool inverse)
 {
-    int s = 0;
-    for (; s + 3 <= logM; s += 3) fft_group_pass<T, 3>(buf, logM, ls, es, lognl, tw, inverse, s);
-    if (logM - s == 2) fft_group_pass<T, 2>(buf, logM, ls, es, lognl, tw, inverse, s);
-    else if (logM - s == 1) fft_group_pass<T, 1>(buf, logM, ls, es, lognl, tw, inverse, s);
+    if constexpr (S + 3 <= LOGM) {
+        fft_group_pass<T, 3>(buf, LOGM, ls, es, lognl, tw, inverse, S);
+        fft_lines_t<T, LOGM, S + 3>(buf, ls, es, lognl, tw, inverse);
+    } else if constexpr (LOGM - S == 2) {
+        fft_group_pass<T, 2>(buf, LOGM, ls, es, lognl, tw, inverse, S);
+    } else if constexpr (LOGM - S == 1) {
+        fft_group_pass<T, 1>(buf, LOGM, ls, es, lognl, tw, inverse, S);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void fft_lines(cplx<T> *buf, int logM, int ls, int es, int lognl,
+                                          const cplx<T> *tw, bool inverse)
+{
+    switch (logM) {  // the mesh sides a context accepts: 32 .. 256
+    case 5: fft_lines_t<T, 5>(buf, ls, es, lognl, tw, inverse); break;
+    case 6: fft_lines_t<T, 6>(buf, ls, es, lognl, tw, inverse); break;
+    case 7: fft_lines_t<T, 7>(buf, ls, es, lognl, tw, inverse); break;
+    case 8: fft_lines_t<T, 8>(buf, ls, es, lognl, tw, inverse); break;
+    default: {
+        int s = 0;
+        for (; s + 3 <= logM; s += 3) fft_group_pass<T, 3>(buf, logM, ls, es, lognl, tw, inverse, s);
+        if (logM - s == 2) fft_group_pass<T, 2>(buf, logM, ls, es, lognl, tw, inverse, s);
+        else if (logM - s == 1) fft_group_pass<T, 1>(buf, logM, ls, es, lognl, tw, inverse, s);
+    }
+    }
 }
 
 // PENCIL lines, element n of line l at buf[n * LS + l]
