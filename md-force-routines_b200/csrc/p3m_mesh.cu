@@ -862,14 +862,17 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
             auto issue = [&](int comp) {
                 constexpr int EPC = 16 / sizeof(T);   // elements per 16-byte chunk
                 constexpr int CPR = GTX / EPC;        // chunks per tile row
-                const T *E = efield + comp * nmesh + R.mesh_off;
-                T *dst = tile + (comp % GNBUF<T>) * GTILE;
-                for (int k = threadIdx.x; k < TILE * TILE * CPR; k += G_THREADS) {
-                    const int ch = k % CPR, row = k / CPR;
-                    const int ty = row % TILE, tz = row / TILE;
-                    const int gx = (bx + ch * EPC) & (M - 1), gy = (by + ty) & (M - 1),
-                              gz = (bz + tz) & (M - 1);
-                    cp_async16(dst + row * GTX + ch * EPC, E + ((long long)gz * M + gy) * M + gx);
+                constexpr int RP = G_THREADS / CPR;   // tile rows per pass
+                static_assert(RP % TILE == 0, "a thread keeps its row's y");
+                if (threadIdx.x < RP * CPR) {
+                    // thread: chunk ch of rows r0, r0 + RP, ... -- fixed x and
+                    // y, z advancing by RP / TILE
+                    const int ch = threadIdx.x % CPR, r0 = threadIdx.x / CPR;
+                    const int gx = (bx + ch * EPC) & (M - 1), gy = (by + r0 % TILE) & (M - 1);
+                    const T *exy = efield + comp * nmesh + R.mesh_off + (long long)gy * M + gx;
+                    T *d = tile + (comp % GNBUF<T>) * GTILE + r0 * GTX + ch * EPC;
+                    for (int tz = r0 / TILE; tz < TILE; tz += RP / TILE, d += RP * GTX)
+                        cp_async16(d, exy + (long long)((bz + tz) & (M - 1)) * M * M);
                 }
                 asm volatile("cp.async.commit_group;\n" ::: "memory");
             };
