@@ -626,11 +626,12 @@ template <typename T> static int seq_step(p3m_ctx *ctx, int mode, int record_nqt
             }
         }
         if (e == cudaSuccess && rec) {  // the new positions are final: ring row counters[3]
+            // (the reduction advances counters[3] after the join)
             e = cudaStreamWaitEvent(ctx->st3, ctx->ev_fork, 0);
             if (e == cudaSuccess) {
-                launch_nqt_partial<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nq_consecutive,
-                                      ctx->nqt_part, ctx->st3);
-                ctx->launches++;
+                launch_nqt<T>(s, s.pos, ctx->qmult, ctx->nq, ctx->nq_consecutive, ctx->nqt_part,
+                              ctx->nqt_ring, ctx->counters, ctx->nqt_cap, ctx->st3);
+                ctx->launches += 2;
                 e = cudaEventRecord(ctx->ev_join3, ctx->st3);
             }
         }
@@ -645,19 +646,12 @@ template <typename T> static int seq_step(p3m_ctx *ctx, int mode, int record_nqt
     if (e == cudaSuccess && rec) e = cudaStreamWaitEvent(st, ctx->ev_join3, 0);
     launch_kick_finish<T>(s, 1, nullptr, st);
     ctx->launches++;
-    StepSums sums;  // the energy sums and this step's n(q,t) row, in the reduction
+    StepSums sums;  // the energy sums, in the reduction (the n(q,t) row is summed on its branch)
     sums.u_pp_part = s.u_pp_part;
     sums.pp_nblk = s.pp_nblk;
     sums.u_pm_part = s.u_pm_part;
     sums.wc_total = s.wc;
     sums.wp_total = s.wp;
-    if (rec) {
-        sums.nqt_part = ctx->nqt_part;
-        sums.nq = ctx->nq;
-        sums.nq_nblk = s.nq_nblk;
-        sums.nqt_cap = ctx->nqt_cap;
-        sums.nqt_ring = ctx->nqt_ring;
-    }
     launch_step_reduce(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, st, rec,
                        ctx->snap_interval, ctx->snap_cap, sums);
     ctx->launches++;

@@ -136,18 +136,6 @@ __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nbl
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int it = counters[2] + counters[0];
     const int step = counters[1];
-    // the n(q,t) row of this step (k_nqt_reduce's sums, in its order)
-    if (sums.nqt_part) {
-        const int row = counters[3] % sums.nqt_cap;
-        const int per = sums.nq * 6;
-        for (int e = threadIdx.x; e < nrep * per; e += blockDim.x) {
-            const int r = e / per, k = e % per;
-            const int b0 = reps[r].nq_blk_off, b1 = (r + 1 < nrep) ? reps[r + 1].nq_blk_off : sums.nq_nblk;
-            double v = 0.0;
-            for (int bb = b0; bb < b1; ++bb) v += sums.nqt_part[(long long)bb * per + k];
-            sums.nqt_ring[((long long)row * nrep + r) * per + k] = v;
-        }
-    }
     for (int r = w; r < nrep; r += nw) {
         const RepDev &R = reps[r];
         if (sums.u_pp_part) {
@@ -533,15 +521,6 @@ void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring
                                       s.rebuild, s.status, sums);
 }
 
-template <typename T>
-void launch_nqt_partial(const DevState &s, const double *pos, const double *qmult, int nq,
-                        int consecutive, double *part, cudaStream_t st)
-{
-    const size_t smem = (size_t)(PBLK / 32) * nq * 6 * sizeof(double);
-    k_nqt_partial<T><<<s.nq_nblk, PBLK, smem, st>>>(s.reps, s.nrep, pos, qmult, nq, consecutive,
-                                                    part);
-}
-
 void launch_snapshot(const DevState &s, const int *counters, double *snap, int *steps,
                      cudaStream_t st)
 {
@@ -598,8 +577,6 @@ void launch_gf_opt(double kappa, double alpha, int p, int m_alias, int M, double
 int gf_opt_blocks(int M) { return (int)(((long long)M * M * M + 255) / 256); }
 
 #define P3M_INST(T)                                                                             \
-    template void launch_nqt_partial<T>(const DevState &, const double *, const double *, int,   \
-                                        int, double *, cudaStream_t);                           \
     template void launch_kick_finish<T>(const DevState &, int, double *, cudaStream_t);          \
     template void launch_nqt<T>(const DevState &, const double *, const double *, int, int,      \
                                 double *, double *, const int *, int, cudaStream_t);            \

@@ -110,16 +110,10 @@ struct StepSums {
     int pp_nblk = 0;
     const double *u_pm_part = nullptr;
     int wc_total = 0, wp_total = 0;
-    const double *nqt_part = nullptr;   // n(q,t) block partials -> nqt_ring row counters[3]
-    int nq = 0, nq_nblk = 0, nqt_cap = 0;
-    double *nqt_ring = nullptr;
 };
 void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring, int ring_cap,
                         cudaStream_t st, int recorded = 0, int snap_interval = 0,
                         int snap_cap = 0, const StepSums &sums = StepSums());
-template <typename T>
-void launch_nqt_partial(const DevState &s, const double *pos, const double *qmult, int nq,
-                        int consecutive, double *part, cudaStream_t st);
 void launch_snapshot(const DevState &s, const int *counters, double *snap, int *steps,
                      cudaStream_t st);
 void launch_set_counters(int *counters, int run_step, int ring_pos, int it0, cudaStream_t st);
