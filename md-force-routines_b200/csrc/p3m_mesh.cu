@@ -97,13 +97,72 @@ __device__ __forceinline__ void fft_group_pass(cplx<T> *buf, int logM, int ls, i
     __syncthreads();
 }
 
+// The first three stages (a pass of fft_group_pass with s = 0): each group is
+// an 8-point DFT of elements base + r, r < 8, whose twiddles are the eighth
+// roots of unity 1, -i and (+-1 - i)/sqrt 2 (conjugated for the inverse), so
+// no table reads and only two real products per non-trivial rotation.
+template <typename T>
+__device__ __forceinline__ void fft_first_pass8(cplx<T> *buf, int logM, int ls, int es, int lognl,
+                                                bool inverse)
+{
+    const T h = (T)0.70710678118654752440L;  // cos(pi/4), as the twiddle table holds it
+    const int ngroups = 1 << (lognl + logM - 3);
+    for (int b = threadIdx.x; b < ngroups; b += blockDim.x) {
+        const int l = b & ((1 << lognl) - 1), base = (b >> lognl) << 3;
+        cplx<T> x[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) x[r] = buf[l * ls + (base + r) * es];
+        // stage 0: pairs (r, r+1), twiddle 1
+#pragma unroll
+        for (int r = 0; r < 8; r += 2) {
+            const cplx<T> a = x[r], c = x[r + 1];
+            x[r] = make_c<T>(a.x + c.x, a.y + c.y);
+            x[r + 1] = make_c<T>(a.x - c.x, a.y - c.y);
+        }
+        // stage 1: pairs (r, r+2); twiddle 1 for even r, -i (inverse: +i) for odd r
+#pragma unroll
+        for (int r = 0; r < 8; r += (r & 1) ? 3 : 1) {
+            const cplx<T> a = x[r], v = x[r + 2];
+            cplx<T> c = v;
+            if (r & 1) c = inverse ? make_c<T>(-v.y, v.x) : make_c<T>(v.y, -v.x);
+            x[r] = make_c<T>(a.x + c.x, a.y + c.y);
+            x[r + 2] = make_c<T>(a.x - c.x, a.y - c.y);
+        }
+        // stage 2: pairs (r, r+4), twiddle W_8^r (inverse: conjugate)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const cplx<T> a = x[r], v = x[r + 4];
+            cplx<T> c;
+            if (r == 0) {
+                c = v;
+            } else if (r == 2) {
+                c = inverse ? make_c<T>(-v.y, v.x) : make_c<T>(v.y, -v.x);
+            } else if (r == 1) {  // (1 - i)/sqrt 2, inverse (1 + i)/sqrt 2
+                c = inverse ? make_c<T>(h * (v.x - v.y), h * (v.x + v.y))
+                            : make_c<T>(h * (v.x + v.y), h * (v.y - v.x));
+            } else {              // (-1 - i)/sqrt 2, inverse (-1 + i)/sqrt 2
+                c = inverse ? make_c<T>(-h * (v.x + v.y), h * (v.x - v.y))
+                            : make_c<T>(h * (v.y - v.x), -h * (v.x + v.y));
+            }
+            x[r] = make_c<T>(a.x + c.x, a.y + c.y);
+            x[r + 4] = make_c<T>(a.x - c.x, a.y - c.y);
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) buf[l * ls + (base + r) * es] = x[r];
+    }
+    __syncthreads();
+}
+
 // The passes of one line length 2^LOGM from stage S on, unrolled at compile
 // time (stage offsets, group counts and twiddle strides become constants).
 template <typename T, int LOGM, int S = 0>
 __device__ __forceinline__ void fft_lines_t(cplx<T> *buf, int ls, int es, int lognl,
                                             const cplx<T> *tw, bool inverse)
 {
-    if constexpr (S + 3 <= LOGM) {
+    if constexpr (S == 0 && LOGM >= 3) {
+        fft_first_pass8<T>(buf, LOGM, ls, es, lognl, inverse);
+        fft_lines_t<T, LOGM, 3>(buf, ls, es, lognl, tw, inverse);
+    } else if constexpr (S + 3 <= LOGM) {
         fft_group_pass<T, 3>(buf, LOGM, ls, es, lognl, tw, inverse, S);
         fft_lines_t<T, LOGM, S + 3>(buf, ls, es, lognl, tw, inverse);
     } else if constexpr (LOGM - S == 2) {
@@ -641,15 +700,26 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
             const int z = e >> logM, y = e & (M - 1);
             A[brev(z, logM) * LD + brev(y, logM)] = spec[lbase + e];
         }
+        // this thread's influence-function values, in flight during the sweeps
+        constexpr int GPT = PLANE_MAX * PLANE_MAX / FFT_THREADS;
+        T gr[GPT];
+#pragma unroll
+        for (int i = 0; i < GPT; ++i) {
+            const int e = threadIdx.x + i * FFT_THREADS;
+            gr[i] = e < MM ? __ldg(green + lbase + e) : (T)0;
+        }
         __syncthreads();
         fft_lines<T>(A, logM, LD, 1, logM, tw, false);  // along y
         fft_lines<T>(A, logM, 1, LD, logM, tw, false);  // along z
         const double wkx = (kx == 0 || kx == (M >> 1)) ? 1.0 : 2.0;
         double u = 0.0;
-        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
+#pragma unroll
+        for (int i = 0; i < GPT; ++i) {
+            const int e = threadIdx.x + i * FFT_THREADS;
+            if (e >= MM) break;
             const int z = e >> logM, y = e & (M - 1);
             const cplx<T> rk = A[z * LD + y];
-            const T g = green[lbase + e];
+            const T g = gr[i];
             u += wkx * (double)g * ((double)rk.x * rk.x + (double)rk.y * rk.y);
             B[brev(z, logM) * LD + brev(y, logM)] = make_c<T>(g * rk.x, g * rk.y);
         }
