@@ -501,6 +501,10 @@ def extras(args, line, ctx, reps, states, device):
         host.append(hb)
     ctxs = [Context(h, precision=FP32, device=device) for h in halves]
     try:
+        # descending stream priorities: the first part finishes its step first
+        # and its copies back overlap the later parts' steps
+        for k, c in enumerate(ctxs):
+            c.set_priority(k)
         for c, hb in zip(ctxs, host):
             c.set_state_all(hb[0], hb[1])
             c.init_forces()
@@ -531,8 +535,8 @@ def extras(args, line, ctx, reps, states, device):
                    "h2d_bytes_per_step": 3 * nb, "d2h_bytes_per_step": 3 * nb + 8 * 8 * len(reps) + 4 * len(halves),
                    "how": ("p3m_set_state_all_async (pinned host -> device, lists kept), "
                            "p3m_run(1, sync=0), p3m_get_step_async (state and energies back) "
-                           f"per step on each of {len(halves)} contexts (its own stream), "
-                           "then p3m_sync")}
+                           f"per step on each of {len(halves)} contexts (its own streams, "
+                           "priority levels 0, 1, ...), then p3m_sync")}
 
     # -- CPU baseline: the oracle port on one host core ------------------------------
     G, _ = gf_opt_device(r0.kappa, r0.alpha, 6, 3, r0.M, r0.L, device=device)

@@ -282,6 +282,17 @@ int p3m_get_replica_stats(p3m_ctx *ctx, int replica, double *out);
  * error seen by a kernel), then cleared. Synchronises the stream. */
 int p3m_check(p3m_ctx *ctx);
 
+/* Scheduling priority of the context's streams (no counterpart in the
+ * reference): level 0 is the highest priority the device offers, larger
+ * levels are lower ones (clamped to the lowest). When several contexts share
+ * a GPU -- an ensemble split so that one part's host copies overlap another
+ * part's steps -- descending levels let the first part finish its step (and
+ * start its copies back) while the others still compute. Waits for the
+ * context's work, recreates its streams (p3m_stream then returns the new
+ * one) and drops its captured step graphs, which the next p3m_run captures
+ * again. */
+int p3m_set_priority(p3m_ctx *ctx, int level);
+
 /* Wait for all work on the context's stream; then, like p3m_check, report
  * a device status (out-of-box particle, non-finite force, list overflow)
  * raised by that work. */

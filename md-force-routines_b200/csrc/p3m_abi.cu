@@ -1400,6 +1400,27 @@ extern "C" int p3m_sync(p3m_ctx *ctx)
     return status_error(ctx, st);
 }
 
+extern "C" int p3m_set_priority(p3m_ctx *ctx, int level)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (level < 0) return fail(ctx, P3M_EARG, "p3m_set_priority", "level must be >= 0");
+    CK(cudaSetDevice(ctx->device));
+    int least = 0, greatest = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    const int prio = (greatest + level < least) ? greatest + level : least;
+    cudaStream_t *streams[3] = {&ctx->st, &ctx->st2, &ctx->st3};
+    for (cudaStream_t *p : streams) CK(cudaStreamSynchronize(*p));
+    for (auto &row : ctx->graph)
+        for (auto &g : row)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (cudaStream_t *p : streams) {
+        CK(cudaStreamDestroy(*p));
+        *p = nullptr;
+        CK(cudaStreamCreateWithPriority(p, cudaStreamNonBlocking, prio));
+    }
+    return P3M_OK;
+}
+
 extern "C" int p3m_set_pp_config(p3m_ctx *ctx, int tpi, double skin)
 {
     if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");

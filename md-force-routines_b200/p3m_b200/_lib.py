@@ -106,6 +106,7 @@ SIGNATURES = {
                           ctypes.c_double, _D]),
     "p3m_get_replica_stats": (_I, [_V, _I, _D]),
     "p3m_sync": (_I, [_V]),
+    "p3m_set_priority": (_I, [_V, _I]),
     "p3m_stream": (_V, [_V]),
     "p3m_set_pp_config": (_I, [_V, _I, ctypes.c_double]),
     "p3m_get_pp_config": (_I, [_V, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double),

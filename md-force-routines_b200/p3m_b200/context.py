@@ -360,6 +360,13 @@ class Context:
     def sync(self):
         self._ck(lib().p3m_sync(self.handle))
 
+    def set_priority(self, level):
+        """Scheduling priority of this context's streams: 0 is the device's
+        highest, larger levels are lower. For several contexts sharing a GPU
+        (copies of one overlapping steps of another). Recreates the streams:
+        query stream() afterwards."""
+        self._ck(lib().p3m_set_priority(self.handle, int(level)))
+
     def launch_count(self):
         return int(lib().p3m_launch_count(self.handle))
 

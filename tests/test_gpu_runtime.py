@@ -422,3 +422,26 @@ def test_get_step_async_matches_sync_reads():
         with pytest.raises(P3MError) as e:
             c.sync()
         assert e.value.code == -4
+
+
+def test_set_priority_keeps_results():
+    """Recreating a context's streams at another priority level changes no
+    result: the steps after it equal those of a context left at the default."""
+    from p3m_b200 import FP32, MODE_NVE, Context, Replica
+
+    N = 3000
+    L = (4 * np.pi * N / 3) ** (1 / 3)
+    r = Replica(N=N, L=L, kappa=1.0, alpha=0.8, rc=L / 3.2, M=32)
+    pos, vel = _init_state(r, 12)
+    out = []
+    for level in (None, 3):
+        with Context(r, precision=FP32) as c:
+            c.set_state(0, pos, vel)
+            c.init_forces()
+            c.run(2, MODE_NVE)
+            if level is not None:
+                c.set_priority(level)
+            c.run(3, MODE_NVE)
+            out.append(c.get_state(0) + (c.energies(max_steps=5),))
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
