@@ -482,11 +482,11 @@ def extras(args, line, ctx, reps, states, device):
     # -- end to end through the C ABI with host buffers ----------------------------
     # per step: H2D of the whole ensemble's (pos, vel, acc) from pinned host
     # memory, one step, D2H of the state and of the step's energies. An
-    # ensemble of several replicas is held as up to four contexts on their
+    # ensemble of several replicas is held as up to five contexts on their
     # own streams with asynchronous copies, so one part's copies overlap the
     # others' steps (the copy engines and the SMs work at the same time).
     ntot = sum(r.N for r in reps)
-    nparts = min(4, len(reps))
+    nparts = min(5, len(reps))
     cuts = [round(k * len(reps) / nparts) for k in range(nparts + 1)]
     halves = [reps[cuts[k]:cuts[k + 1]] for k in range(nparts)]
     offs = np.cumsum([0] + [sum(r.N for r in h) for h in halves])
