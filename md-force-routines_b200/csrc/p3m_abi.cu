@@ -154,7 +154,7 @@ static void build_pp_table(const p3m_replica_desc &d, float4 *out)
     }
 }
 
-// Cell grid (cells >= rc + skin, at least 3 per side), list capacity and
+// Cell grid (cells >= (rc + skin) / CELL_DIV, at least 6 per side), list capacity and
 // PP block layout of every replica for a given skin and threads-per-particle.
 // Updates ctx->rh and ctx->s counts; the caller uploads and (re)allocates.
 static void plan_lists(p3m_ctx *ctx, double skin_override, int tpi)

@@ -7,7 +7,7 @@
 // BRICK^3 block of base indices floor(x/h) (yukawa_pm_ord6.py:17-27), folded
 // into [0, M).
 //
-// The cell sort (the grid of the neighbour-list build, cells >= rc + skin)
+// The cell sort (the grid of the neighbour-list build, cells >= (rc + skin)/2)
 // runs only on rebuild steps, per replica: each replica has its own rebuild
 // flag, its cells are scanned within its own particle range, and the cell
 // kernels skip the work of replicas whose flag is clear -- so a replica's
