@@ -1408,15 +1408,23 @@ extern "C" int p3m_set_priority(p3m_ctx *ctx, int level)
     int least = 0, greatest = 0;
     CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     const int prio = (greatest + level < least) ? greatest + level : least;
+    // the new streams first: on a failure the context keeps its old ones
+    cudaStream_t fresh[3] = {nullptr, nullptr, nullptr};
+    for (int k = 0; k < 3; ++k) {
+        const cudaError_t e = cudaStreamCreateWithPriority(&fresh[k], cudaStreamNonBlocking, prio);
+        if (e != cudaSuccess) {
+            for (int j = 0; j < k; ++j) cudaStreamDestroy(fresh[j]);
+            return fail(ctx, P3M_ECUDA, "cudaStreamCreateWithPriority", cudaGetErrorString(e));
+        }
+    }
     cudaStream_t *streams[3] = {&ctx->st, &ctx->st2, &ctx->st3};
     for (cudaStream_t *p : streams) CK(cudaStreamSynchronize(*p));
     for (auto &row : ctx->graph)
         for (auto &g : row)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-    for (cudaStream_t *p : streams) {
-        CK(cudaStreamDestroy(*p));
-        *p = nullptr;
-        CK(cudaStreamCreateWithPriority(p, cudaStreamNonBlocking, prio));
+    for (int k = 0; k < 3; ++k) {
+        cudaStreamDestroy(*streams[k]);
+        *streams[k] = fresh[k];
     }
     return P3M_OK;
 }
