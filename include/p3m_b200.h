@@ -36,7 +36,7 @@ extern "C" {
 #define P3M_ECUDA (-2)         /* CUDA runtime error                          */
 #define P3M_ENODEV (-3)        /* no usable sm_100 device                     */
 #define P3M_EBOX (-4)          /* particle outside [-L, 2L) or non-finite     */
-#define P3M_ENONFINITE (-5)    /* NaN/Inf in forces or energies               */
+#define P3M_ENONFINITE (-5)    /* NaN/Inf in velocities, forces or energies   */
 #define P3M_ESTATE (-6)        /* call out of order (e.g. no state uploaded)  */
 #define P3M_ENBOVF (-7)        /* neighbour-list capacity exceeded            */
 
@@ -107,9 +107,12 @@ int p3m_gf_opt(int device, double kappa, double alpha, int p, int m_alias, int M
  * per 256-point block) lives in a fixed file-scope device array of 8192
  * doubles (64 KiB, held on every GPU that loads the library until exit), so
  * M is limited to 128; larger M is rejected with P3M_EARG. The call
- * allocates nothing. The first call on a device looks up that array's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture. All calls on a device share the array: calls that
+ * allocates nothing. Every call made outside stream capture looks up that
+ * array's device address (cudaGetSymbolAddress); a call under capture reuses
+ * the address the last uncaptured call found on that device, so make the
+ * first call on a device -- and the first one after a cudaDeviceReset, which
+ * unloads the library's device code -- before any stream capture (otherwise
+ * P3M_ECUDA). All calls on a device share the array: calls that
  * overlap on the GPU race and must be ordered by the caller. Runs on the
  * current device. Message of the last failure: p3m_gf_opt_static_error(). */
 int p3m_gf_opt_static(double kappa, double alpha, int p, int m_alias, int M, double box,

@@ -692,8 +692,10 @@ static int status_error(p3m_ctx *ctx, int st)
 {
     if (!st) return P3M_OK;
     CK(cudaMemset(ctx->s.status, 0, sizeof(int)));
+    // a non-finite velocity also makes a non-finite position: name the cause
+    if (st & ST_NONFINITE)
+        return fail(ctx, P3M_ENONFINITE, "non-finite velocity, force or energy", "");
     if (st & ST_BOX) return fail(ctx, P3M_EBOX, "particle outside [-L, 2L) or non-finite position", "");
-    if (st & ST_NONFINITE) return fail(ctx, P3M_ENONFINITE, "non-finite force or energy", "");
     if (st & ST_NBOVF)
         return fail(ctx, P3M_ENBOVF, "a particle has more neighbours than the list holds",
                     "raise the capacity with a smaller skin or report the density");
@@ -725,8 +727,11 @@ static int upload_charge(p3m_ctx *ctx, const double *Z)
     const int n = ctx->s.ntot;
     if (!Z) return P3M_OK;
     double qmax = 0.0;
-    for (int i = 0; i < n; ++i) qmax = fmax(qmax, fabs(Z[i]));
-    if (!(qmax < 1e300)) return fail(ctx, P3M_EARG, "charges", "not finite");
+    for (int i = 0; i < n; ++i) {
+        if (!std::isfinite(Z[i])) return fail(ctx, P3M_EARG, "charges", "not finite");
+        qmax = fmax(qmax, fabs(Z[i]));
+    }
+    if (!(qmax < 1e300)) return fail(ctx, P3M_EARG, "charges", "too large");
     if (qmax != ctx->rh[0].qmax) {
         ctx->rh[0].qmax = qmax > 0.0 ? qmax : 1.0;
         CK(cudaMemcpyAsync(&ctx->s.reps[0].qmax, &ctx->rh[0].qmax, sizeof(double),
@@ -1418,7 +1423,13 @@ extern "C" int p3m_set_priority(p3m_ctx *ctx, int level)
         }
     }
     cudaStream_t *streams[3] = {&ctx->st, &ctx->st2, &ctx->st3};
-    for (cudaStream_t *p : streams) CK(cudaStreamSynchronize(*p));
+    for (cudaStream_t *p : streams) {
+        const cudaError_t e = cudaStreamSynchronize(*p);
+        if (e != cudaSuccess) {  // keep the old streams and graphs; drop the new streams
+            for (int k = 0; k < 3; ++k) cudaStreamDestroy(fresh[k]);
+            return fail(ctx, P3M_ECUDA, "cudaStreamSynchronize", cudaGetErrorString(e));
+        }
+    }
     for (auto &row : ctx->graph)
         for (auto &g : row)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }

@@ -35,7 +35,7 @@ constexpr int PBLK = 256;      // particles per block in replica-aligned particl
 // Device status bits (first error wins in the host's reading order).
 enum : int {
     ST_BOX = 1,        // particle outside [-L, 2L) or position not finite
-    ST_NONFINITE = 2,  // NaN/Inf in forces or energies
+    ST_NONFINITE = 2,  // NaN/Inf in velocities, forces or energies (read first)
     ST_NBOVF = 4,      // a particle has more list neighbours than the list holds
 };
 

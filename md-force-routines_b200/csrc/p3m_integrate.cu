@@ -43,9 +43,11 @@ __global__ void k_kick_drift(const RepDev *__restrict__ reps, const int *__restr
         const RepDev &R = reps[r];
         double x[3];
         double d2 = 0.0;
+        bool vfin = true;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             double v = kick(vel[3 * i + d], acc[3 * i + d], R.dt);
+            vfin = vfin && isfinite(v);
             vel[3 * i + d] = v;
             x[d] = wrap_once(__dadd_rn(pos[3 * i + d], __dmul_rn(v, R.dt)), R.L);
             pos[3 * i + d] = x[d];
@@ -54,6 +56,9 @@ __global__ void k_kick_drift(const RepDev *__restrict__ reps, const int *__restr
             dd -= R.L * rint(dd * R.inv_L);
             d2 += dd * dd;
         }
+        // a non-finite velocity (or acceleration) is reported as such; the
+        // position it makes is also flagged by particle_keys below
+        if (!vfin) raise_status(status, ST_NONFINITE);
         if (d2 > 0.25 * R.skin * R.skin && !rebuild[r]) atomicOr(rebuild + r, 1);
         int b;
         particle_keys(R, x[0], x[1], x[2], has_mesh, nullptr, &b, status);
@@ -257,7 +262,7 @@ __global__ void k_combine(const RepDev *__restrict__ reps, const int *__restrict
                           const typename V4<T>::t *__restrict__ acc_pp,
                           const typename V4<T>::t *__restrict__ acc_pm, int use_pp, int use_pm,
                           int scale_af, double *__restrict__ out, double *__restrict__ ep_out,
-                          int ntot)
+                          int ntot, int *status)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
         double a[3] = {0.0, 0.0, 0.0};
@@ -283,6 +288,7 @@ __global__ void k_combine(const RepDev *__restrict__ reps, const int *__restrict
         out[3 * i + 0] = scale_af ? f * a[0] : a[0];
         out[3 * i + 1] = scale_af ? f * a[1] : a[1];
         out[3 * i + 2] = scale_af ? f * a[2] : a[2];
+        if (!(isfinite(a[0]) && isfinite(a[1]) && isfinite(a[2]))) raise_status(status, ST_NONFINITE);
     }
 }
 
@@ -539,7 +545,8 @@ void launch_combine(const DevState &s, int use_pp, int use_pm, int scale_af, dou
     using T4 = typename V4<T>::t;
     k_combine<T><<<pgrid(s.ntot), 256, 0, st>>>(s.reps, s.prep, s.cell_slot, s.brick_slot,
                                                 (const T4 *)s.acc_pp, (const T4 *)s.acc_pm,
-                                                use_pp, use_pm, scale_af, out, ep_out, s.ntot);
+                                                use_pp, use_pm, scale_af, out, ep_out, s.ntot,
+                                                s.status);
 }
 
 void launch_scale_vel(const DevState &s, cudaStream_t st)

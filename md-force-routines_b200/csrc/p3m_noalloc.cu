@@ -34,17 +34,26 @@ static __device__ __align__(256) double g_gf_scratch[kMaxBlocks];
 std::mutex g_setup_mu;
 double *g_scratch_addr[kMaxDevices] = {};
 
-// Device address of g_gf_scratch on the current device, looked up once per
-// device. (In host code the array's name is only a host-side stand-in and
-// must never be passed to a kernel.)
-cudaError_t scratch_address(int device, double **out)
+// Device address of g_gf_scratch on the current device. (In host code the
+// array's name is only a host-side stand-in and must never be passed to a
+// kernel.) The address is looked up again on every call made outside stream
+// capture -- a cudaDeviceReset, or any teardown of the primary context,
+// unloads the module and the array may come back elsewhere -- and the last
+// address found is reused while `st` is capturing, when no CUDA call that
+// could load a module may run.
+cudaError_t scratch_address(int device, cudaStream_t st, double **out)
 {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_addr[device]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_gf_scratch);
+        e = cudaGetSymbolAddress(&p, g_gf_scratch);
         if (e != cudaSuccess) return e;
         g_scratch_addr[device] = static_cast<double *>(p);
+    } else if (!g_scratch_addr[device]) {
+        return cudaErrorStreamCaptureUnsupported;  // first call on this device under capture
     }
     *out = g_scratch_addr[device];
     return cudaSuccess;
@@ -92,10 +101,10 @@ extern "C" int p3m_gf_opt_static(double kappa, double alpha, int p, int m_alias,
     e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
     if (e != cudaSuccess || major != 10)
         return fail_static(P3M_ENODEV, "library is built for sm_100a (B200)");
-    double *part = nullptr;
-    e = scratch_address(dev, &part);
-    if (e != cudaSuccess) return fail_static(P3M_ECUDA, "cudaGetSymbolAddress", cudaGetErrorString(e));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double *part = nullptr;
+    e = scratch_address(dev, st, &part);
+    if (e != cudaSuccess) return fail_static(P3M_ECUDA, "scratch address", cudaGetErrorString(e));
     p3m::launch_gf_opt(kappa, alpha, p, m_alias, M, box, G_k_dev, part, st);
     k_sum_partials<<<1, 32, 0, st>>>(part, p3m::gf_opt_blocks(M), A_pm_dev);
     e = cudaGetLastError();

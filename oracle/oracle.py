@@ -13,6 +13,7 @@ FP64 algorithm of the reference (xgdhar/MD-force-routines):
 * ``gather6``      yukawa_pm_ord6.py:213-312      (C: oracle_gather6)
 * ``pm``           yukawa_pm_ord6.py:440-484      (numpy FFT chain)
 * ``gf_opt``       yukawa_gf_opt.py:5-98          (C: oracle_gf_opt)
+* ``gf_opt_points`` the same at chosen k points   (C: oracle_gf_opt_points)
 * ``force_pot``    yukawa_p3m_ord6.py:6-29
 * ``update``       velocity_verlet_p3m_ord6.py:5-26
 * ``vscale``       thermostat_p3m_ord6.py:5-25
@@ -72,6 +73,11 @@ def _load():
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                       dp, dp]
         lib.oracle_gf_opt.restype = None
+        lib.oracle_gf_opt_points.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_int), dp]
+        lib.oracle_gf_opt_points.restype = None
         _lib = lib
     return _lib
 
@@ -134,6 +140,18 @@ def gf_opt(kappa, Gew, p, mx_max, my_max, mz_max, Mx, My, Mz, hx, hy, hz, Lx, Ly
     ky_v = 2 * np.pi * (np.arange(My).reshape((My, 1)) - ny_mid) / Ly
     kz_v = 2 * np.pi * (np.arange(Mz).reshape((Mz, 1, 1)) - nz_mid) / Lz
     return G_k, kx_v, ky_v, kz_v, float(A[0])
+
+
+def gf_opt_points(kappa, Gew, p, m_max, M, L, idx):
+    """yukawa_gf_opt.py:5-98 on a cubic M^3 mesh at chosen points only:
+    idx (n, 3) integer (nz, ny, nx) of the fftshifted layout -> G_k there
+    (same arithmetic as gf_opt, point by point)."""
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    out = np.zeros(idx.shape[0])
+    _load().oracle_gf_opt_points(float(kappa), float(Gew), int(p), int(m_max), int(M),
+                                 float(L) / M, float(L), idx.shape[0],
+                                 idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _p(out))
+    return out
 
 
 def pm_fields(pos, Z, G_k, kx_v, ky_v, kz_v, Mx, My, Mz, hx, hy, hz, Lx, Ly, Lz):

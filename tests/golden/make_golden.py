@@ -1,9 +1,8 @@
 """Generate the golden vectors in this directory from the reference's own code.
 
-Run here, where the reference tree is mounted (default /root/reference, or
-$P3M_REFERENCE_DIR):
+Run where the reference tree is present, naming it in $P3M_REFERENCE_DIR:
 
-    python tests/golden/make_golden.py
+    P3M_REFERENCE_DIR=<reference tree> python tests/golden/make_golden.py
 
 It imports the reference's numba modules unchanged, with two shims:
 ``numba.autojit`` (removed from numba) is aliased to ``numba.jit``, and a
@@ -31,7 +30,7 @@ sys.dont_write_bytecode = True
 import numpy as np  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("P3M_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("P3M_REFERENCE_DIR", "")
 
 
 def _install_shims():
@@ -171,6 +170,8 @@ def make_case(R, name, N, Gamma, kappa, alpha, rc, M, seed, dt):
 
 
 def main():
+    if not REF or not os.path.isdir(REF):
+        raise SystemExit("set P3M_REFERENCE_DIR to the reference tree")
     R = load_reference()
     for name, args in CASES.items():
         make_case(R, name, *args)

@@ -1,0 +1,146 @@
+"""Parity against the oracle at the benchmark configurations' own sizes.
+
+* the N = 1e5, Gamma = 50, kappa = 1, alpha = 0.5, r_c = 7, 128^3 system
+  from seed 2 (PP over 10^3 list cells, yukawa_pp.py:6-139; the multi-pass
+  128^3 FFT chain, yukawa_pm_ord6.py:440-484);
+* the N = 1e6, kappa = 2, alpha = 0.6, r_c = 6, 256^3 system from seed 7
+  (the 256^3 instantiation of every mesh kernel);
+* an uneven batch holding one replica of each mesh size the uneven
+  64-replica ensemble picks (32^3, 64^3, 128^3), each compared with its own
+  oracle run.
+
+The oracle runs the reference's FP64 algorithm on the CPU (PP and the mesh
+stages in C, the FFT chain in numpy) on the same positions, with the
+influence function the device computes -- itself checked against the
+oracle's gf_opt (yukawa_gf_opt.py:5-98) at sampled k points, because the
+full 256^3 alias sum takes the CPU minutes. Bars: FP64 path 1e-9 RMS force
+error and 1e-10 in U; FP32 path 1e-5 RMS force error
+(sqrt(sum |a - a_ref|^2 / sum |a_ref|^2)).
+"""
+import numpy as np
+import pytest
+
+from gpu_util import rel_max, rel_rms
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _state(N, L, T, seed):
+    import initialize_pos_vel
+
+    pos, vel = np.zeros((N, 3)), np.zeros((N, 3))
+    initialize_pos_vel.initial(seed, N, [L] * 3, pos, vel, T)
+    return pos, vel
+
+
+def _checked_green(kappa, alpha, M, L, npts=3000, seed=0):
+    """The device influence function, checked against the oracle at npts
+    random points plus the k = 0 line, the kx = 0 plane's corners and the
+    lowest / Nyquist indices of every axis."""
+    from p3m_b200 import gf_opt_device
+
+    G, A = gf_opt_device(kappa, alpha, 6, 3, M, L)
+    rng = np.random.default_rng(seed)
+    idx = rng.integers(0, M, size=(npts, 3))
+    edge = np.array([0, 1, M // 2 - 1, M // 2, M // 2 + 1, M - 1])
+    grid = np.stack(np.meshgrid(edge, edge, edge, indexing="ij"), -1).reshape(-1, 3)
+    idx = np.concatenate([idx, grid])
+    ref = O.gf_opt_points(kappa, alpha, 6, 3, M, L, idx)
+    got = G[idx[:, 0], idx[:, 1], idx[:, 2]]
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+    return G
+
+
+def _oracle_params(N, L, kappa, alpha, rc, M, Gamma, G):
+    P = O.Params(N, kappa, alpha, rc, M, L=L, Gamma=Gamma)
+    kv = 2 * np.pi * (np.arange(M) - M // 2) / L
+    P._gk = (G, kv.reshape(1, M), kv.reshape(M, 1), kv.reshape(M, 1, 1), 0.0)
+    return P
+
+
+def _force_both(rep, pos, G):
+    from p3m_b200 import FP32, FP64, Context
+
+    out = {}
+    for name, prec in (("fp64", FP64), ("fp32", FP32)):
+        with Context(rep, precision=prec) as c:
+            c.set_green(G)
+            out[name] = c.force(pos)
+    return out
+
+
+def _check(out, Uo, ao, parts_o):
+    U64, a64, parts64 = out["fp64"]
+    U32, a32, _ = out["fp32"]
+    assert U64 == pytest.approx(Uo, rel=1e-10)
+    for p, q in zip(parts64, parts_o):
+        assert p == pytest.approx(q, rel=1e-10, abs=1e-10 * abs(parts_o[0]))
+    assert rel_rms(a64, ao) < 1e-9
+    e32 = rel_rms(a32, ao)
+    assert e32 <= 1e-5, e32
+    assert rel_max(a32, ao) <= 1e-4
+    # U = U_pp + U_pm + U_self cancels strongly: judge U's error on |U_pp|
+    assert abs(U32 - Uo) < 1e-6 * abs(parts_o[0])
+
+
+def test_n1e5_128_mesh_rc7_against_oracle():
+    from p3m_b200.configs import cfg2
+
+    rep = cfg2()[0]
+    pos, _ = _state(rep.N, rep.L, rep.T_desired, 2)
+    G = _checked_green(rep.kappa, rep.alpha, rep.M, rep.L)
+    P = _oracle_params(rep.N, rep.L, rep.kappa, rep.alpha, rep.rc, rep.M, 50.0, G)
+    Uo, ao, parts_o = O.force_pot(P, pos)
+    _check(_force_both(rep, pos, G), Uo, ao, parts_o)
+
+
+def test_n1e6_256_mesh_against_oracle():
+    from p3m_b200.configs import cfg5
+
+    rep = cfg5()[0]
+    pos, _ = _state(rep.N, rep.L, rep.T_desired, 7)
+    G = _checked_green(rep.kappa, rep.alpha, rep.M, rep.L)
+    P = _oracle_params(rep.N, rep.L, rep.kappa, rep.alpha, rep.rc, rep.M, 100.0, G)
+    Uo, ao, parts_o = O.force_pot(P, pos)
+    _check(_force_both(rep, pos, G), Uo, ao, parts_o)
+
+
+def test_uneven_batch_each_replica_against_its_oracle():
+    """One replica of each mesh size of the uneven ensemble (N, Gamma, kappa
+    drawn per seed, (M, alpha, r_c) from the error-estimate picker), run as
+    one batch: every replica's forces and energy match its own oracle run."""
+    from p3m_b200 import FP32, FP64, Context
+    from p3m_b200.configs import cfg4
+
+    reps, _ = cfg4()
+    chosen = {}
+    for r in sorted(reps, key=lambda r: r.N):  # the smallest replica of each mesh size
+        chosen.setdefault(r.M, r)
+    assert sorted(chosen) == [32, 64, 128]
+    batch = [chosen[M] for M in (64, 32, 128)]
+    states = [_state(r.N, r.L, r.T_desired, r.seed)[0] for r in batch]
+    greens = [_checked_green(r.kappa, r.alpha, r.M, r.L, npts=1000, seed=r.seed) for r in batch]
+    oracle = []
+    for r, pos, G in zip(batch, states, greens):
+        P = _oracle_params(r.N, r.L, r.kappa, r.alpha, r.rc, r.M, 1.0 / r.T_desired, G)
+        oracle.append(O.force_pot(P, pos))
+    pos_all = np.concatenate(states)
+    for name, prec in (("fp64", FP64), ("fp32", FP32)):
+        with Context(batch, precision=prec) as c:
+            for i, G in enumerate(greens):
+                c.set_green(G, replica=i)
+            c.set_state_all(pos_all, np.zeros_like(pos_all))
+            c.init_forces()
+            _, _, acc = c.get_state_all()
+            off = 0
+            for i, (r, (Uo, ao, parts_o)) in enumerate(zip(batch, oracle)):
+                a = acc[off:off + r.N]
+                off += r.N
+                st = c.replica_stats(i)
+                if name == "fp64":
+                    assert rel_rms(a, ao) < 1e-9, (r.M, rel_rms(a, ao))
+                    assert st["U"] == pytest.approx(Uo, rel=1e-10)
+                else:
+                    assert rel_rms(a, ao) <= 1e-5, (r.M, rel_rms(a, ao))
+                    assert abs(st["U"] - Uo) < 1e-6 * abs(parts_o[0])

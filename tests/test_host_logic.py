@@ -40,3 +40,42 @@ def test_no_device_fails_loudly():
     pos = np.random.default_rng(0).random((100, 3)) * 10.0
     with pytest.raises(P3MError):
         yukawa_pp.particle_particle(1.0, 0.8, 3.0, np.array([10.0] * 3), pos, np.zeros((100, 3)))
+
+
+def test_reference_driver_calls_bind_to_package_modules():
+    """Every call the reference's driver makes into the modules this package
+    shadows (yukawa_MD_p3m_ord6.py:15-21 imports, :152-229 calls) binds to
+    this package's function of the same name with the same arguments. Reads
+    the Python-3 copy of the driver that the build writes into oracle/_ref/
+    where the reference tree is present."""
+    import ast
+    import importlib
+    import inspect
+    import os
+
+    from conftest import ROOT
+
+    path = os.path.join(ROOT, "oracle", "_ref", "yukawa_MD_p3m_ord6_py3.py")
+    if not os.path.isfile(path):
+        pytest.skip("the copy of the reference's driver was not built here")
+    tree = ast.parse(open(path).read())
+    alias = {}
+    for node in ast.walk(tree):
+        if isinstance(node, ast.Import):
+            for a in node.names:
+                if a.name not in ("numpy", "time"):
+                    alias[a.asname or a.name] = a.name
+    assert set(alias.values()) == {"read", "initialize_pos_vel", "velocity_verlet_p3m_ord6",
+                                   "thermostat_p3m_ord6", "yukawa_gf_opt", "yukawa_p3m_ord6"}
+    seen = set()
+    for node in ast.walk(tree):
+        if (isinstance(node, ast.Call) and isinstance(node.func, ast.Attribute)
+                and isinstance(node.func.value, ast.Name) and node.func.value.id in alias):
+            mod = importlib.import_module(alias[node.func.value.id])
+            fn = getattr(mod, node.func.attr)
+            assert not node.keywords
+            inspect.signature(fn).bind(*range(len(node.args)))
+            seen.add((mod.__name__, node.func.attr))
+    assert seen == {("yukawa_gf_opt", "gf_opt"), ("yukawa_p3m_ord6", "force_pot"),
+                    ("thermostat_p3m_ord6", "vscale"), ("velocity_verlet_p3m_ord6", "update"),
+                    ("read", "initL"), ("initialize_pos_vel", "initial")}

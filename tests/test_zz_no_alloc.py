@@ -5,9 +5,12 @@ passes device output buffers and a stream; the library keeps its scratch in
 a fixed device array instead of calling cudaMalloc.
 
 This file is named so that pytest collects it last. It compares the
-allocation-free entry point with p3m_gf_opt, through the C ABI, on two calls
-in a row with different parameters (the second call must not see the first
-call's scratch contents), within the tolerance the other gf_opt tests use.
+allocation-free entry point with p3m_gf_opt, through the C ABI, on calls in a
+row with different parameters, within the tolerance the other gf_opt tests
+use. The largest mesh goes first: its 8192 block partials stay in the shared
+array, and the smaller meshes after it read only the first of those slots,
+which they wrote themselves (the A_pm comparison would catch a sum that
+picked up stale partials).
 """
 import ctypes
 
@@ -16,7 +19,8 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-CASES = [  # kappa, alpha, M, L
+CASES = [  # kappa, alpha, M, L -- largest mesh first
+    (1.0, 0.5, 128, 74.8),
     (2.0, 0.6, 32, 20.31),
     (1.0, 0.5, 64, 34.73),
 ]
