@@ -8,15 +8,15 @@ CPU restatement of the reference's algorithm). For a workload of
   sqrt(sum |a32 - a64|^2 / sum |a64|^2) and eps_max = max_i |a32 - a64|_i /
   rms |a64|, on the total acceleration, at the first step and every 100 steps
   of the FP64 trajectory;
-* energy conservation of the FP32 path: the drift of E = K + U over
-  ``drift_steps`` NVE steps from the equilibrated state, per replica (the
-  largest |E(t) - E(0)| relative to |E(0)| and to the kinetic energy -- E(0)
-  nears zero in weakly coupled replicas -- and the change from the first to
-  the last 100-step mean);
+* energy conservation of the FP32 path, and of the FP64 path from the same
+  equilibrated state as the control: per replica, the largest |E(t) - E(0)|
+  over ``drift_steps`` NVE steps relative to |E(0)| and to the kinetic
+  energy (E(0) nears zero in weakly coupled replicas), and the drift proper,
+  the least-squares slope of E(t) times the run length over |E(0)|;
 * for the ensemble with n(q,t) (cfg3): S(q, w) of the FP32 and the FP64
   ensembles, both from their own trajectories (which part after a few hundred
   steps: the comparison is statistical), the frequency and height of the peak
-  of each q.
+  of each q, with replica-bootstrap standard deviations.
 
   python -m p3m_b200.validate --workload cfg1 [--drift-steps 10000]
 """
@@ -54,14 +54,30 @@ def _force_errors(a32, a64, offs):
 
 
 def _run_energies(ctx, steps, chunk=8000):
-    """E = K + U of every replica after each of `steps` NVE steps."""
-    E = []
+    """(E, K) of every replica after each of `steps` NVE steps: (steps, R)."""
+    E, K = [], []
     for k0 in range(0, steps, chunk):
         k = min(chunk, steps - k0)
         ctx.run(k, MODE_NVE)
         e = ctx.energies(max_steps=k)
         E.append(e[:, :, 0] + e[:, :, 1])
-    return np.concatenate(E)
+        K.append(e[:, :, 1])
+    return np.concatenate(E), np.concatenate(K)
+
+
+def _drift_stats(E, K, E0, K0):
+    """Per replica: the largest |E(t) - E(0)| relative to |E(0)| and to K(0),
+    and the drift proper -- the least-squares slope of E(t) times the run
+    length, relative to |E(0)| (fluctuations about a level, which the
+    largest deviation also counts, do not grow with the run)."""
+    t = np.arange(1, E.shape[0] + 1, dtype=np.float64)
+    dev = np.max(np.abs(E - E0[None, :]), axis=0)
+    slope = np.polyfit(t, E, 1)[0]  # per replica
+    return {"max_abs_dev_rel_E0": (dev / np.abs(E0)).tolist(),
+            "max_abs_dev_rel_K0": (dev / K0).tolist(),
+            "fit_drift_rel_E0": (np.abs(slope) * E.shape[0] / np.abs(E0)).tolist(),
+            "E0": E0.tolist(), "K0": K0.tolist(),
+            "K_mean_rel_K0": (K.mean(axis=0) / K0).tolist()}
 
 
 def _sqw_peaks(S, dw):
@@ -71,11 +87,26 @@ def _sqw_peaks(S, dw):
     return k * dw, S[np.arange(S.shape[0]), k]
 
 
+def _bootstrap_peaks(S_rep, dw, n_boot=400, seed=0):
+    """Standard deviation of the replica-mean S(q,w) peak frequency and height
+    over bootstrap resamples of the replicas."""
+    rng = np.random.default_rng(seed)
+    R = S_rep.shape[0]
+    ws, hs = [], []
+    for _ in range(n_boot):
+        S = S_rep[rng.integers(0, R, size=R)].mean(axis=0)
+        w, h = _sqw_peaks(S, dw)
+        ws.append(w)
+        hs.append(h)
+    return np.std(ws, axis=0), np.std(hs, axis=0)
+
+
 def validate(workload="cfg1", equil=1000, traj_steps=1000, drift_steps=10000, sqw_steps=4096,
-             quench=200, device=0):
+             quench=200, device=0, fp64_drift=True):
     reps = WORKLOADS[workload]()
     offs = np.cumsum([0] + [r.N for r in reps])
-    res = {"workload": workload, "replicas": len(reps), "particles": int(offs[-1])}
+    res = {"workload": workload, "replicas": len(reps), "particles": int(offs[-1]),
+           "equil": {"quench_steps": quench, "thermostat_steps": equil}}
     pos0, vel0 = _initial(reps)
     with Context(reps, precision=FP64, device=device) as c64, \
             Context(reps, precision=FP32, device=device) as c32:
@@ -100,37 +131,48 @@ def validate(workload="cfg1", equil=1000, traj_steps=1000, drift_steps=10000, sq
                             "max_rel_max_over_samples": float(s[:, :, 1].max()),
                             "samples": int(s.shape[0]),
                             "definition": "eps_rms = sqrt(sum|a32-a64|^2/sum|a64|^2), eps_max = "
-                                          "max_i |a32-a64|_i / rms|a64|, total acceleration"}
-        # FP32 energy conservation from the equilibrated state
-        c32.set_state_all(pos_eq, vel_eq)
-        c32.init_forces()
-        E = _run_energies(c32, drift_steps)
-        E0 = E[0]
-        dev = np.max(np.abs(E - E0[None, :]), axis=0) / np.abs(E0)
-        n = min(100, len(E) // 2)
-        trend = np.abs(E[-n:].mean(axis=0) - E[:n].mean(axis=0)) / np.abs(E0)
-        K0 = c32.energies(max_steps=1)[0, :, 1]
-        res["nve_drift"] = {"steps": drift_steps, "max_abs_rel_dev": float(dev.max()),
-                            "first_to_last_100_mean_rel": float(trend.max()),
-                            "max_abs_dev_over_K": float(
-                                (np.max(np.abs(E - E0[None, :]), axis=0) / K0).max()),
-                            "dt": reps[0].dt}
+                                          "max_i |a32-a64|_i / rms|a64|, total acceleration, "
+                                          "FP32 against the FP64 device path"}
+        # energy conservation from the equilibrated state: FP32, and FP64 as
+        # the control that separates the integrator's error (dt) from FP32's
+        drift = {"steps": drift_steps, "dt": reps[0].dt}
+        for name, c in (("fp32", c32), ("fp64", c64)) if fp64_drift else (("fp32", c32),):
+            c.set_state_all(pos_eq, vel_eq)
+            c.init_forces()
+            E, K = _run_energies(c, drift_steps)
+            E0, K0 = E[0], K[0]  # after the first step
+            st = _drift_stats(E, K, E0, K0)
+            drift[name] = {"max_abs_dev_rel_E0_max": float(np.max(st["max_abs_dev_rel_E0"])),
+                           "fit_drift_rel_E0_max": float(np.max(st["fit_drift_rel_E0"])),
+                           "max_abs_dev_rel_K0_max": float(np.max(st["max_abs_dev_rel_K0"])),
+                           "per_replica": st}
+        res["nve_drift"] = drift
         if workload == "cfg3" and sqw_steps:
             dt = reps[0].dt
+            dw = 2 * np.pi / (sqw_steps * dt)
             peaks = {}
             for name, c in (("fp32", c32), ("fp64", c64)):
                 c.set_state_all(pos_eq, vel_eq)
                 c.init_forces()
                 c.set_nqt(CFG3_QMULT, sqw_steps)
                 c.run(sqw_steps, MODE_NVE, record_nqt=True)
-                S = c.sqw(dt, sqw_steps)
-                peaks[name] = _sqw_peaks(S[:6], 2 * np.pi / (sqw_steps * dt))
-            w32, h32 = peaks["fp32"]
-            w64, h64 = peaks["fp64"]
-            res["sqw_peaks"] = {"q_multiples": [1, 2, 3, 4, 5, 6],
+                S, S_rep = c.sqw(dt, sqw_steps, per_replica=True)
+                w, h = _sqw_peaks(S[:6], dw)
+                sw, sh = _bootstrap_peaks(S_rep[:, :6], dw)
+                peaks[name] = (w, h, sw, sh)
+            w32, h32, sw32, sh32 = peaks["fp32"]
+            w64, h64, sw64, sh64 = peaks["fp64"]
+            dh = h32 - h64
+            sd = np.sqrt(sh32 ** 2 + sh64 ** 2)
+            res["sqw_peaks"] = {"q_multiples": [1, 2, 3, 4, 5, 6], "dw": dw,
                                 "w_fp32": w32.tolist(), "w_fp64": w64.tolist(),
-                                "dw": 2 * np.pi / (sqw_steps * dt),
-                                "height_rel_diff": ((h32 - h64) / h64).tolist()}
+                                "w_boot_sd_fp32": sw32.tolist(), "w_boot_sd_fp64": sw64.tolist(),
+                                "h_fp32": h32.tolist(), "h_fp64": h64.tolist(),
+                                "h_boot_sd_fp32": sh32.tolist(), "h_boot_sd_fp64": sh64.tolist(),
+                                "height_rel_diff": (dh / h64).tolist(),
+                                "height_diff_in_sd": (dh / sd).tolist(),
+                                "note": "each ensemble from its own trajectories; sd: replica "
+                                        "bootstrap (400 resamples) of the replica-mean peak"}
     return res
 
 
@@ -142,9 +184,10 @@ def main(argv=None):
     ap.add_argument("--drift-steps", type=int, default=10000)
     ap.add_argument("--sqw-steps", type=int, default=4096)
     ap.add_argument("--quench", type=int, default=200)
+    ap.add_argument("--no-fp64-drift", action="store_true")
     a = ap.parse_args(argv)
     print(json.dumps(validate(a.workload, a.equil, a.traj_steps, a.drift_steps, a.sqw_steps,
-                              a.quench)))
+                              a.quench, fp64_drift=not a.no_fp64_drift)))
 
 
 if __name__ == "__main__":
