@@ -147,6 +147,27 @@ def pp_flop(reps):
     return float(sum(r.N * r.rc ** 3 / 2.0 * FLOP_PER_PAIR for r in reps))
 
 
+def hbm_peak_gbs():
+    """HBM copy bandwidth: the measured figure of MEASURED_PEAKS.json where
+    the file is present, else this pool's earlier measurement (fallback)."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        v = float(json.load(open(path))["hbm_gbs"])
+        return v, "of measured (MEASURED_PEAKS.json)"
+    except Exception:
+        return 6650.0, "of fallback (6.65 TB/s: MEASURED_PEAKS.json absent)"
+
+
+def step_roofline_s(reps, fp32_tflops, hbm_gbs, nq=32):
+    """Time of one step of every replica at the roofline: the PP pairs and
+    the n(q,t) sums on the FP32 pipe, the mesh arrays (each FP32 stage array
+    written and read once: 66 M^3 bytes) and the particle state (FP64
+    pos/vel read and written, FP32 accelerations: 120 N bytes) at HBM speed."""
+    flop = pp_flop(reps) + sum(r.N * 3 * nq * 8.0 for r in reps)
+    byts = sum(66.0 * r.M ** 3 + 120.0 * r.N for r in reps)
+    return flop / (fp32_tflops * 1e12) + byts / (hbm_gbs * 1e9)
+
+
 def working_set_mb(reps):
     b = 0
     for r in reps:
@@ -470,21 +491,30 @@ def extras(args, line, ctx, reps, states, device):
     peak = fp32_peak_tflops(device)
     pp_ms = stages.get("pp", 0.0)
     flop = pp_flop(reps)
-    traffic = None
+    traffic, traffic_src = None, None
     tpath = os.path.join(ROOT, "profiles", "pp_traffic.json")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and args.workload == "cfg3":
         try:
-            traffic = (json.load(open(tpath)).get("cfg3_bytes_per_launch")
-                       if args.workload == "cfg3" else None)
+            tj = json.load(open(tpath))
+            traffic = tj.get("cfg3_bytes_per_launch")
+            traffic_src = f"profiles/pp_traffic.json: {tj.get('source', 'ncu capture')}"
         except Exception:
             traffic = None
     achieved = flop / (pp_ms * 1e-3) / 1e12 if pp_ms > 0 else None
-    line["roofline"] = {"kernel": "k_pp (PP pair loop, FP32)", "bound": "fp32",
+    hbm, hbm_src = hbm_peak_gbs()
+    t_roof = step_roofline_s(reps, peak, hbm)
+    line["roofline"] = {"kernel": "k_pp_f32 (PP pair loop, FP32)", "bound": "fp32",
                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                        "traffic_source": traffic_src,
                         "peak_source": "measured FP32 FMA probe (p3m_fp32_peak) on this GPU; "
                                        "MEASURED_PEAKS.json has no FP32 figure",
-                        "work": f"{flop:.3e} FLOP per launch = sum N rc^3/2 pairs x {FLOP_PER_PAIR}"}
+                        "work": f"{flop:.3e} FLOP per launch = sum N rc^3/2 pairs x {FLOP_PER_PAIR}",
+                        "step_t_roof_ms": t_roof * 1e3,
+                        "step_frac": t_roof * 1e3 / line["ms_per_step"],
+                        "step_roof_how": (f"sum over replicas of N rc^3/2 x {FLOP_PER_PAIR} FLOP and "
+                                          f"n(q,t) N x 3 x Nq x 8 FLOP at {peak:.1f} TFLOP/s, plus "
+                                          f"66 M^3 + 120 N bytes at {hbm:.0f} GB/s ({hbm_src})")}
     if "fft_both" in stages and "fft_forward" in stages:
         stages["fft_inverse"] = stages["fft_both"] - stages["fft_forward"]
     line["stages_ms"] = {k: round(v, 5) for k, v in stages.items()}

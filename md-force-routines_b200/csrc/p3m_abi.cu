@@ -186,7 +186,8 @@ static void plan_lists(p3m_ctx *ctx, double skin_override, int tpi)
     s.ncell = cell;
     s.pp_tpi = tpi;
     s.pp_nblk = blk;
-    s.maxnb = ((int)ceil(1.5 * maxmean + 64.0) + 7) / 8 * 8;
+    // a multiple of PP_LIST_PAD: the builder pads every list to one
+    s.maxnb = ((int)ceil(1.5 * maxmean + 64.0) + PP_LIST_PAD - 1) / PP_LIST_PAD * PP_LIST_PAD;
 }
 
 extern "C" int p3m_version(void) { return P3M_VERSION; }

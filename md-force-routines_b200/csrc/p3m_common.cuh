@@ -40,7 +40,14 @@ enum : int {
 };
 
 // Intervals of the tabulated FP32 pair functions on [0, rc].
-constexpr int PP_TABLE_N = 2048;  // FP32 pair table: cubic intervals on [0, rc]
+#ifndef P3M_PP_TABLE_N
+#define P3M_PP_TABLE_N 2048
+#endif
+constexpr int PP_TABLE_N = P3M_PP_TABLE_N;  // FP32 pair table: cubic intervals on [0, rc]
+// Neighbour lists are padded with the particle's own index to a multiple of
+// this many entries (a padded entry has r = 0 and adds nothing), so the FP32
+// pair loop reads whole blocks of entries without a bounds test.
+constexpr int PP_LIST_PAD = 16;
 
 // Per-replica constants. Offsets index the concatenated device arrays.
 struct RepDev {

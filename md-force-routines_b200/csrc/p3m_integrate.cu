@@ -306,7 +306,9 @@ __global__ void k_scale_vel(const RepDev *__restrict__ reps, const int *__restri
 // n(q,t) partial sums: per replica-aligned block of NQ_PPT * PBLK particles,
 // for each wave number q_m = m 2 pi / L (m = qmult[iq]) and axis,
 // sum_i exp(-i q x_i) (yukawa_MD_p3m_ord6.py:215-219). Each thread sums
-// NQ_PPT particles before the block reduction. The phase is reduced in FP64
+// NQ_PPT particles, a warp its 32 threads' sums (in the bulk precision T: a
+// warp's total holds 32 NQ_PPT terms), and the block its warps' totals in
+// FP64. The phase is reduced in FP64
 // as frac(m x / L) before the sine/cosine of the bulk precision T; when the
 // multiples are 1, 2, ..., nq (`consecutive`), exp(-i m theta) follows from
 // exp(-i theta) by complex multiplication instead.
@@ -328,10 +330,40 @@ __device__ __forceinline__ void sincospi_t(double two_t, T *s, T *c)
     }
 }
 
+// Sum over the 32 lanes of a warp of eight values v[0..7] per lane, by
+// recursive halving: at each of the first three levels a lane keeps half of
+// its values, sends the other half to its partner (lane ^ 16, ^ 8, ^ 4) and
+// adds the partner's copy of the half it keeps; two butterfly levels finish
+// the one value left. Lane l returns the total of value (l >> 2) & 7. Nine
+// shuffles for eight sums (five per value in a plain butterfly), in a fixed
+// order.
 template <typename T>
+__device__ __forceinline__ T warp_sum8(const T (&v)[8])
+{
+    const int lane = threadIdx.x & 31;
+    T a[4], b[2];
+    const bool h4 = lane & 16, h3 = lane & 8, h2 = lane & 4;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const T send = h4 ? v[i] : v[i + 4];
+        a[i] = (h4 ? v[i + 4] : v[i]) + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const T send = h3 ? a[i] : a[i + 2];
+        b[i] = (h3 ? a[i + 2] : a[i]) + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    const T send = h2 ? b[0] : b[1];
+    T c = (h2 ? b[1] : b[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
+    c += __shfl_xor_sync(0xffffffffu, c, 2);
+    c += __shfl_xor_sync(0xffffffffu, c, 1);
+    return c;
+}
+
+template <typename T, bool consecutive>
 __global__ void __launch_bounds__(PBLK)
 k_nqt_partial(const RepDev *__restrict__ reps, int nrep, const double *__restrict__ pos,
-              const double *__restrict__ qmult, int nq, int consecutive, double *__restrict__ part)
+              const double *__restrict__ qmult, int nq, double *__restrict__ part)
 {
     extern __shared__ double nsm[];  // [nwarps][nq*6]
     const int b = blockIdx.x;
@@ -349,31 +381,36 @@ k_nqt_partial(const RepDev *__restrict__ reps, int nrep, const double *__restric
 #pragma unroll
         for (int d = 0; d < 3; ++d) xl[m][d] = have[m] ? pos[3 * i + d] * R.inv_L : 0.0;
     }
-    // per-particle base rotation exp(-i 2 pi x/L) for the recurrence
-    T c1[NQ_PPT][3], s1[NQ_PPT][3], cm[NQ_PPT][3], sm[NQ_PPT][3];
-    if (consecutive) {
+    // per-particle base rotation exp(-i 2 pi x/L) for the recurrence; a
+    // missing particle rotates by 1 and is weighted by 0
+    T c1[NQ_PPT][3], s1[NQ_PPT][3], cm[NQ_PPT][3], sm[NQ_PPT][3], wt[NQ_PPT];
 #pragma unroll
-        for (int m = 0; m < NQ_PPT; ++m)
+    for (int m = 0; m < NQ_PPT; ++m) {
+        wt[m] = have[m] ? (T)1 : (T)0;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                T st, ct;
+        for (int d = 0; d < 3; ++d) {
+            T st = (T)0, ct = (T)1;
+            if constexpr (consecutive) {
                 const double t = xl[m][d] - floor(xl[m][d]);
                 sincospi_t<T>(2.0 * t, &st, &ct);
-                c1[m][d] = ct;
-                s1[m][d] = -st;
-                cm[m][d] = (T)1;
-                sm[m][d] = (T)0;
             }
+            c1[m][d] = ct;
+            s1[m][d] = -st;
+            cm[m][d] = (T)1;
+            sm[m][d] = (T)0;
+        }
     }
     for (int iq = 0; iq < nq; ++iq) {
-        const double mq = qmult[iq];
-        double acc[6] = {0, 0, 0, 0, 0, 0};
+        const double mq = consecutive ? 0.0 : qmult[iq];
+        T acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = (T)0;
 #pragma unroll
         for (int m = 0; m < NQ_PPT; ++m) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 T c, sn;
-                if (consecutive) {
+                if constexpr (consecutive) {
                     // exp(-i (k+1) theta) = exp(-i k theta) exp(-i theta)
                     const T nc = cm[m][d] * c1[m][d] - sm[m][d] * s1[m][d];
                     const T ns = cm[m][d] * s1[m][d] + sm[m][d] * c1[m][d];
@@ -389,17 +426,14 @@ k_nqt_partial(const RepDev *__restrict__ reps, int nrep, const double *__restric
                     c = ct;
                     sn = -st;
                 }
-                if (have[m]) {
-                    acc[2 * d + 0] += (double)c;
-                    acc[2 * d + 1] += (double)sn;
-                }
+                acc[2 * d + 0] += wt[m] * c;
+                acc[2 * d + 1] += wt[m] * sn;
             }
         }
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const double v = warp_sum(acc[k]);
-            if (lane == 0) nsm[w * nq * 6 + iq * 6 + k] = v;
-        }
+        // lane l holds the warp's total of value (l >> 2) & 7 (6, 7: padding)
+        const T tot = warp_sum8<T>(acc);
+        const int k = (lane >> 2) & 7;
+        if ((lane & 3) == 0 && k < 6) nsm[w * nq * 6 + iq * 6 + k] = (double)tot;
     }
     __syncthreads();
     for (int k = threadIdx.x; k < nq * 6; k += blockDim.x) {
@@ -559,8 +593,10 @@ void launch_nqt(const DevState &s, const double *pos, const double *qmult, int n
                 double *part, double *out, const int *counters, int ring_cap, cudaStream_t st)
 {
     const size_t smem = (size_t)(PBLK / 32) * nq * 6 * sizeof(double);
-    k_nqt_partial<T><<<s.nq_nblk, PBLK, smem, st>>>(s.reps, s.nrep, pos, qmult, nq, consecutive,
-                                                    part);
+    if (consecutive)
+        k_nqt_partial<T, true><<<s.nq_nblk, PBLK, smem, st>>>(s.reps, s.nrep, pos, qmult, nq, part);
+    else
+        k_nqt_partial<T, false><<<s.nq_nblk, PBLK, smem, st>>>(s.reps, s.nrep, pos, qmult, nq, part);
     k_nqt_reduce<<<s.nrep, 256, 0, st>>>(s.reps, s.nrep, s.nq_nblk, part, nq, out, counters,
                                          ring_cap);
 }
@@ -569,8 +605,9 @@ int nqt_particles_per_block() { return PBLK * NQ_PPT; }
 
 template <typename T> void configure_integrate_kernels(int max_nq)
 {
-    cudaFuncSetAttribute(k_nqt_partial<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)((PBLK / 32) * max_nq * 6 * sizeof(double)));
+    const int smem = (int)((PBLK / 32) * max_nq * 6 * sizeof(double));
+    cudaFuncSetAttribute(k_nqt_partial<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_nqt_partial<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 void launch_gf_opt(double kappa, double alpha, int p, int m_alias, int M, double L, double *G_k,

@@ -103,6 +103,7 @@ constexpr int LB_TPI = 16;                    // lanes per particle
 constexpr int LB_PPB = LB_THREADS / LB_TPI;   // particles per pass
 template <typename T> __host__ __device__ constexpr int lb_scap() { return sizeof(T) == 4 ? 1024 : 512; }
 static_assert(CELL_STENCIL <= LB_THREADS, "one thread per stencil cell");
+static_assert(LB_TPI >= PP_LIST_PAD, "one pad entry per lane at most");
 
 // One CTA per cell (about 10 particles: cells are (rc + skin)/2 wide) of the
 // replicas rebuilding this step (the list k_scan wrote). The CELL_STENCIL
@@ -213,9 +214,18 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                     cnt += __popc(grp);
                 }
             }
-            if (have && sub == 0) {
-                if (cnt > maxnb) raise_status(status, ST_NBOVF);
-                nnb[s] = min(cnt, maxnb);
+            if (have) {
+                const int nn = min(cnt, maxnb);
+                if (sub == 0) {
+                    if (cnt > maxnb) raise_status(status, ST_NBOVF);
+                    nnb[s] = nn;
+                }
+                // pad to a whole block of PP_LIST_PAD entries with the
+                // particle itself (r = 0: no contribution); maxnb is a
+                // multiple of PP_LIST_PAD, so the pad stays in the list
+                const int pe = nn + sub;
+                if (pe < ((nn + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1)))
+                    nlist[list_index(s, pe, maxnb)] = s;
             }
         }
     }
@@ -369,6 +379,152 @@ k_pp_list(const RepDev *__restrict__ reps, int nrep, const typename Coord<T>::Q 
     if (threadIdx.x == 0) u_part[b] = ut;
 }
 
+// ---------------------------------------------------------------------------
+// FP32 forces from the padded lists, two candidates per packed FP32x2 op
+// ---------------------------------------------------------------------------
+// sm_100 issues FP32 multiply-adds on pairs of registers (fma.rn.f32x2 and
+// friends): the pair loop is issue-bound, so each thread evaluates its list
+// entries two at a time with packed operations -- the same rounding, operand
+// by operand, as the scalar evaluation of pair_table. Lists are padded with
+// the particle's own index to whole blocks of PP_LIST_PAD entries, so the
+// loop reads them without a bounds test.
+#ifndef P3M_PP_PACK
+#define P3M_PP_PACK 1
+#endif
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+template <bool P> __device__ __forceinline__ float2 v_fma(float2 a, float2 b, float2 c)
+{
+    if constexpr (P) return __ffma2_rn(a, b, c);
+    else return f2(__fmaf_rn(a.x, b.x, c.x), __fmaf_rn(a.y, b.y, c.y));
+}
+template <bool P> __device__ __forceinline__ float2 v_mul(float2 a, float2 b)
+{
+    if constexpr (P) return __fmul2_rn(a, b);
+    else return f2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+}
+template <bool P> __device__ __forceinline__ float2 v_add(float2 a, float2 b)
+{
+    if constexpr (P) return __fadd2_rn(a, b);
+    else return f2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+}
+
+// Two candidates a, b of particle xi: adds F/r * (dx, dy, dz) and phi of the
+// ones closer than rc (and not the particle itself) to p*.
+template <bool P>
+__device__ __forceinline__ void pair_table2(const uint4 &xi, const uint4 &qa, const uint4 &qb,
+                                            float2 sc, float2 sc_lo, float rc2, float2 inv_h,
+                                            const float4 *__restrict__ tab, float2 &px,
+                                            float2 &py, float2 &pz, float2 &pu)
+{
+    constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: round-to-integer constant
+    const float2 ix = f2((float)(int)(xi.x - qa.x), (float)(int)(xi.x - qb.x));
+    const float2 iy = f2((float)(int)(xi.y - qa.y), (float)(int)(xi.y - qb.y));
+    const float2 iz = f2((float)(int)(xi.z - qa.z), (float)(int)(xi.z - qb.z));
+    const float2 dx = v_fma<P>(ix, sc_lo, v_mul<P>(ix, sc));
+    const float2 dy = v_fma<P>(iy, sc_lo, v_mul<P>(iy, sc));
+    const float2 dz = v_fma<P>(iz, sc_lo, v_mul<P>(iz, sc));
+    const float2 r2 = v_fma<P>(dz, dz, v_fma<P>(dy, dy, v_mul<P>(dx, dx)));
+    // r = 0 (the particle itself: list padding) would make r = 0 * inf: take
+    // rc^2 there (a valid table interval) and mask the result; beyond rc the
+    // last interval's cubic is extrapolated, finite, and masked as well
+    const float2 rs = f2(r2.x > 0.f ? r2.x : rc2, r2.y > 0.f ? r2.y : rc2);
+    const float2 m = f2((r2.x < rc2 && r2.x > 0.f) ? 1.f : 0.f, (r2.y < rc2 && r2.y > 0.f) ? 1.f : 0.f);
+    const float2 rinv = f2(rsqrtf(rs.x), rsqrtf(rs.y));
+    const float2 t = v_mul<P>(v_mul<P>(rs, rinv), inv_h);
+    const float2 tb = v_add<P>(v_add<P>(t, f2(-0.5f, -0.5f)), f2(kMagic, kMagic));
+    const int ia = min(__float_as_int(tb.x) - 0x4B400000, PP_TABLE_N - 1);
+    const int ib = min(__float_as_int(tb.y) - 0x4B400000, PP_TABLE_N - 1);
+    const float2 fl = v_add<P>(tb, f2(-kMagic, -kMagic));       // the interval index, exact
+    const float2 u = v_fma<P>(fl, f2(-1.f, -1.f), t);            // t - fl, exact
+    const float4 ca = tab[ia], cb = tab[ib];
+    const float2 c0 = f2(ca.x, cb.x), c1 = f2(ca.y, cb.y), c2 = f2(ca.z, cb.z), c3 = f2(ca.w, cb.w);
+    const float2 ps = v_fma<P>(v_fma<P>(v_fma<P>(c3, u, c2), u, c1), u, c0);
+    const float2 dps = v_fma<P>(v_fma<P>(v_mul<P>(c3, f2(3.f, 3.f)), u, v_add<P>(c2, c2)), u, c1);
+    const float2 g = v_fma<P>(v_mul<P>(t, f2(-1.f, -1.f)), dps, ps);  // psi - t psi'
+    const float2 fr = v_mul<P>(v_mul<P>(v_mul<P>(g, v_mul<P>(rinv, rinv)), rinv), m);
+    const float2 ph = v_mul<P>(v_mul<P>(ps, rinv), m);
+    px = v_fma<P>(fr, dx, px);
+    py = v_fma<P>(fr, dy, py);
+    pz = v_fma<P>(fr, dz, pz);
+    pu = v_add<P>(pu, ph);
+}
+
+#ifndef P3M_PP_MINB
+#define P3M_PP_MINB 3
+#endif
+
+template <int TPI>
+__global__ void __launch_bounds__(PPL_THREADS, P3M_PP_MINB)
+k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq,
+         const int *__restrict__ nnb, const int *__restrict__ nlist, int maxnb,
+         const float4 *__restrict__ tables, float4 *__restrict__ acc_out,
+         double *__restrict__ u_part)
+{
+    constexpr bool P = P3M_PP_PACK != 0;
+    constexpr int PPB = PPL_THREADS / TPI;               // particles per block
+    constexpr int UNR = PP_LIST_PAD / TPI < 8 ? PP_LIST_PAD / TPI : 8;  // entries per lane per pass
+    constexpr int STEP = UNR * TPI;                       // entries of a particle per pass
+    static_assert(UNR % 2 == 0 && PP_LIST_PAD % STEP == 0, "whole pairs, whole pad blocks");
+    __shared__ double red[32];
+    extern __shared__ __align__(16) float4 ppl_tab[];
+    const int b = blockIdx.x;
+    const int r = find_rep(b, nrep, [&](int k) { return reps[k].pp_blk_off; });
+    const RepDev &R = reps[r];
+    {
+        const float4 *src = tables + (long long)r * PP_TABLE_N;
+        for (int k = threadIdx.x; k < PP_TABLE_N; k += PPL_THREADS) cp_async16(ppl_tab + k, src + k);
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    const int sub = threadIdx.x % TPI;
+    const int s = R.p_off + (b - R.pp_blk_off) * PPB + threadIdx.x / TPI;
+    const bool have = s < R.p_off + R.n;
+    // L / 2^32 as a hi + lo pair (a plain FP32 scale would bias every dx of
+    // the replica by the same relative rounding)
+    const double scd = R.L / 4294967296.0;
+    const float sch = (float)scd;
+    const float2 sc = f2(sch, sch), sc_lo = f2((float)(scd - (double)sch), (float)(scd - (double)sch));
+    const float rc2 = (float)(R.rc * R.rc);
+    const float ih = (float)(PP_TABLE_N / R.rc);
+    const float2 inv_h = f2(ih, ih);
+
+    float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    double u = 0.0;
+    if (have) {
+        const uint4 xi = xq[s];
+        const int nr = (nnb[s] + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1);
+        const int *lp = nlist + list_index(s, sub, maxnb);
+        for (int k0 = 0; k0 < nr; k0 += STEP, lp += STEP * 32) {
+            int j[UNR];
+#pragma unroll
+            for (int v = 0; v < UNR; ++v) j[v] = __ldg(lp + v * TPI * 32);
+            uint4 q[UNR];
+#pragma unroll
+            for (int v = 0; v < UNR; ++v) q[v] = xq[j[v]];
+            float2 px = f2(0.f, 0.f), py = px, pz = px, pu = px;
+#pragma unroll
+            for (int v = 0; v < UNR; v += 2)
+                pair_table2<P>(xi, q[v], q[v + 1], sc, sc_lo, rc2, inv_h, ppl_tab, px, py, pz, pu);
+            const float sx = px.x + px.y, sy = py.x + py.y, sz = pz.x + pz.y;
+            float y = sx - gx, t = fx + y; gx = (t - fx) - y; fx = t;
+            y = sy - gy; t = fy + y; gy = (t - fy) - y; fy = t;
+            y = sz - gz; t = fz + y; gz = (t - fz) - y; fz = t;
+            u += (double)(pu.x + pu.y);
+        }
+    }
+#pragma unroll
+    for (int o = TPI / 2; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (have && sub == 0) acc_out[s] = make_float4(fx, fy, fz, 0.f);
+    const double ut = block_sum(u, red);
+    if (threadIdx.x == 0) u_part[b] = ut;
+}
+
 // Per-replica U_pp = 1/2 sum of the replica's block partials (index order).
 __global__ void k_reduce_pp(const RepDev *__restrict__ reps, int nrep,
                             const double *__restrict__ u_part, int nblk_total,
@@ -403,6 +559,12 @@ template <typename T> void configure_pp_kernels()
     cudaFuncSetAttribute(k_pp_list<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
     cudaFuncSetAttribute(k_pp_list<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
     cudaFuncSetAttribute(k_pp_list<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
+    if constexpr (sizeof(T) == 4) {
+        cudaFuncSetAttribute(k_pp_f32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
+        cudaFuncSetAttribute(k_pp_f32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
+        cudaFuncSetAttribute(k_pp_f32<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
+        cudaFuncSetAttribute(k_pp_f32<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
+    }
 }
 
 template <typename T> void launch_quantize(const DevState &s, cudaStream_t st)
@@ -423,10 +585,16 @@ template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st
 template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cudaStream_t st)
 {
     using Q = typename Coord<T>::Q;
-    const size_t smem = sizeof(T) == 4 ? PP_TABLE_N * sizeof(float4) : 0;
-    k_pp_list<T, TPI><<<s.pp_nblk, PPL_THREADS, smem, st>>>(s.reps, s.nrep, (const Q *)s.xq, s.nnb,
-                                                         s.nlist, s.maxnb, s.pp_tables,
-                                                         (typename V4<T>::t *)s.acc_pp, s.u_pp_part);
+    if constexpr (sizeof(T) == 4) {
+        k_pp_f32<TPI><<<s.pp_nblk, PPL_THREADS, PP_TABLE_N * sizeof(float4), st>>>(
+            s.reps, s.nrep, (const uint4 *)s.xq, s.nnb, s.nlist, s.maxnb, s.pp_tables,
+            (float4 *)s.acc_pp, s.u_pp_part);
+    } else {
+        k_pp_list<T, TPI><<<s.pp_nblk, PPL_THREADS, 0, st>>>(s.reps, s.nrep, (const Q *)s.xq,
+                                                            s.nnb, s.nlist, s.maxnb, s.pp_tables,
+                                                            (typename V4<T>::t *)s.acc_pp,
+                                                            s.u_pp_part);
+    }
 }
 
 template <typename T> void launch_pp(const DevState &s, cudaStream_t st)
