@@ -833,7 +833,10 @@ k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
 // its 216 nodes from there; each thread keeps the weights of up to GPT
 // particles across the three components.
 constexpr int G_THREADS = 256;
-template <typename T> constexpr int GNBUF = sizeof(T) == 4 ? 2 : 1;
+#ifndef P3M_G_NBUF32
+#define P3M_G_NBUF32 2
+#endif
+template <typename T> constexpr int GNBUF = sizeof(T) == 4 ? P3M_G_NBUF32 : 1;
 // Gather tiles keep rows of GTX nodes (TILE padded up) so each row is filled
 // with 16-byte copies: a brick starts on a multiple of 16 nodes and M is a
 // multiple of 16, so every 16-byte chunk -- wrapped ones included -- is
@@ -841,8 +844,12 @@ template <typename T> constexpr int GNBUF = sizeof(T) == 4 ? 2 : 1;
 constexpr int GTX = 24;
 constexpr int GTILE = TILE * TILE * GTX;
 
+#ifndef P3M_G_MINB
+#define P3M_G_MINB 1
+#endif
+
 template <typename T>
-__global__ void __launch_bounds__(G_THREADS)
+__global__ void __launch_bounds__(G_THREADS, P3M_G_MINB)
 k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_start,
          const int *__restrict__ brick_perm, const double *__restrict__ pos,
          const double *__restrict__ charge, const T *__restrict__ efield, long long nmesh,

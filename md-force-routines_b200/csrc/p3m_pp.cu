@@ -380,16 +380,19 @@ k_pp_list(const RepDev *__restrict__ reps, int nrep, const typename Coord<T>::Q 
 }
 
 // ---------------------------------------------------------------------------
-// FP32 forces from the padded lists, two candidates per packed FP32x2 op
+// FP32 forces from the padded lists
 // ---------------------------------------------------------------------------
-// sm_100 issues FP32 multiply-adds on pairs of registers (fma.rn.f32x2 and
-// friends): the pair loop is issue-bound, so each thread evaluates its list
-// entries two at a time with packed operations -- the same rounding, operand
-// by operand, as the scalar evaluation of pair_table. Lists are padded with
-// the particle's own index to whole blocks of PP_LIST_PAD entries, so the
-// loop reads them without a bounds test.
+// Each thread evaluates its list entries two at a time. sm_100 can issue the
+// FP32 arithmetic of such a pair as packed fma.rn.f32x2 / mul / add
+// instructions (P3M_PP_PACK=1, the same rounding operand by operand); on the
+// 20 x 1e4-particle ensemble that measured slower than the scalar form (pair
+// loop 0.199 against 0.181 ms: the kernel is bound by L1 -- the scattered
+// 16-byte coordinate gathers and the table reads -- not by issue, and the
+// packed operands cost register moves), so the scalar form is the default.
+// Lists are padded with the particle's own index to whole blocks of
+// PP_LIST_PAD entries, so the loop reads them without a bounds test.
 #ifndef P3M_PP_PACK
-#define P3M_PP_PACK 1
+#define P3M_PP_PACK 0
 #endif
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
