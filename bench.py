@@ -68,7 +68,7 @@ def parse():
     ap.add_argument("--quench", type=int, default=200,
                     help="thermostat steps at T_desired/100 before --equil (damps the runaway "
                          "particles that random initial positions launch)")
-    ap.add_argument("--no-tune", action="store_true", help="skip the PP autotuner")
+    ap.add_argument("--no-tune", action="store_true", help="skip the kernel-shape autotuner")
     ap.add_argument("--pp-config", default=None, metavar="TPI,SKIN",
                     help="set threads per particle and Verlet skin instead of autotuning")
     ap.add_argument("--no-extras", action="store_true",
@@ -454,6 +454,7 @@ def run_ours(args):
                               f"working set {working_set_mb(reps):.0f} MB fits L2; no flush"),
                        "pp_config": dict(zip(("threads_per_particle", "skin", "list_capacity"),
                                              ctx.pp_config())),
+                       "tuning": ctx.tuning(),
                        "list_rebuilds_per_replica_step": rebuilds / (len(reps) * args.steps),
                        "autotune_ms_per_step": tuned["ms_per_step"] if tuned else None,
                        "autotune_final_ms_per_step": tuned.get("final_ms_per_step") if tuned else None},

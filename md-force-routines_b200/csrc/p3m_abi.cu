@@ -18,6 +18,7 @@ struct p3m_ctx {
     std::vector<p3m_replica_desc> desc;
     std::vector<RepDev> rh;
     std::vector<char> green_ready;
+    double skin_override = -1.0;  // the skin of the last p3m_set_tuning (< 0: per replica)
     DevState s;
     cudaStream_t st = nullptr;
     cudaStream_t st2 = nullptr;   // the mesh branch of a step (joined back into st)
@@ -154,7 +155,39 @@ static void build_pp_table(const p3m_replica_desc &d, float4 *out)
     }
 }
 
-// Cell grid (cells >= (rc + skin) / CELL_DIV, at least 6 per side), list capacity and
+// Work items of the mesh passes of every replica: x-pass items, and either
+// plane items (sides up to s.plane_max: the fused y/z plane kernel) or y and
+// z pencil items. Updates ctx->rh offsets and ctx->s totals; the caller
+// uploads.
+static void plan_mesh_passes(p3m_ctx *ctx)
+{
+    DevState &s = ctx->s;
+    int wa = 0, wb = 0, wc = 0, wp = 0, maxp = 0;
+    for (int r = 0; r < ctx->nrep; ++r) {
+        RepDev &R = ctx->rh[r];
+        R.wa_off = wa;
+        R.wb_off = wb;
+        R.wc_off = wc;
+        R.wp_off = wp;
+        const int M = R.M;
+        if (M == 0) continue;
+        wa += M * (M >> (x_lines_log(R.logM) + 1));
+        if (M <= s.plane_max) {
+            wp += M / 2 + 1;
+            if (M > maxp) maxp = M;
+        } else {
+            wb += (M / 2 + 1) * (M / PENCIL);
+            wc += (M / 2 + 1) * (M / PENCIL);
+        }
+    }
+    s.wa = wa;
+    s.wb = wb;
+    s.wc = wc;
+    s.wp = wp;
+    s.max_plane = maxp;
+}
+
+// Cell grid (cells >= (rc + skin) / cell_div, at least 3 cell_div per side), list capacity and
 // PP block layout of every replica for a given skin and threads-per-particle.
 // Updates ctx->rh and ctx->s counts; the caller uploads and (re)allocates.
 static void plan_lists(p3m_ctx *ctx, double skin_override, int tpi)
@@ -167,13 +200,13 @@ static void plan_lists(p3m_ctx *ctx, double skin_override, int tpi)
         const p3m_replica_desc &d = ctx->desc[r];
         RepDev &R = ctx->rh[r];
         double skin = skin_override >= 0.0 ? skin_override : (d.skin >= 0.0 ? d.skin : kDefaultSkin);
-        // rc + skin <= L/3 keeps >= 3 CELL_DIV cells per side, more than
+        // rc + skin <= L/3 keeps >= 3 cell_div cells per side, more than
         // the stencil spans (no cell is visited twice)
         const double smax = d.box / 3.0 * (1.0 - 1e-12) - d.rc;
         if (skin > smax) skin = smax > 0.0 ? smax : 0.0;
         R.skin = skin;
         R.rcl = d.rc + skin;
-        R.nc = (int)floor(CELL_DIV * d.box / R.rcl);  // >= 6
+        R.nc = (int)floor(s.cell_div * d.box / R.rcl);  // >= 3 cell_div
         R.cellw = d.box / R.nc;
         R.inv_cellw = 1.0 / R.cellw;
         R.cell_off = cell;
@@ -323,7 +356,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     int sort_ch = (int)std::min<long long>(4096, std::max<long long>(256, (ntot_all + 591) / 592));
     sort_ch = (sort_ch + 31) / 32 * 32;
     s.sort_ch = sort_ch;
-    int p = 0, cell = 0, brick = 0, wa = 0, wb = 0, wc = 0, wp = 0, blk = 0, maxm = 0, maxp = 0;
+    int p = 0, cell = 0, brick = 0, wc_cap = 0, blk = 0, maxm = 0;
     for (int r = 0; r < n_reps; ++r) {
         const p3m_replica_desc &d = reps[r];
         RepDev &R = ctx->rh[r];
@@ -354,10 +387,6 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
             R.mesh_off = mesh;
             R.spec_off = spec;
             R.tile_off = tile;
-            R.wa_off = wa;
-            R.wb_off = wb;
-            R.wc_off = wc;
-            R.wp_off = wp;
             R.sc_off = nchunk;
             R.sh_off = hist;
             nchunk += (d.n + sort_ch - 1) / sort_ch;
@@ -367,25 +396,15 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
             mesh += (long long)M * M * M;
             spec += (long long)(M / 2 + 1) * M * M;
             tile += (long long)R.nb * R.nb * R.nb * TILE3;
-            wa += M * (M >> (x_lines_log(R.logM) + 1));
-            if (M <= plane_max_mesh()) {
-                wp += M / 2 + 1;
-                if (M > maxp) maxp = M;
-            } else {
-                wb += (M / 2 + 1) * (M / PENCIL);
-                wc += (M / 2 + 1) * (M / PENCIL);
-            }
+            // U_f partials: one per pencil item, more than per plane item
+            wc_cap += (M / 2 + 1) * (M / PENCIL > 1 ? M / PENCIL : 1);
             if (M > maxm) maxm = M;
         } else {
             R.brick_off = brick;
-            R.wa_off = wa;
-            R.wb_off = wb;
-            R.wc_off = wc;
-            R.wp_off = wp;
         }
         p += d.n;
         {
-            const int ncmax = (int)floor(CELL_DIV * d.box / d.rc);  // the finest grid any skin asks for
+            const int ncmax = (int)floor(CELL_DIV_MAX * d.box / d.rc);  // the finest grid any setting asks for
             cell += ncmax * ncmax * ncmax;
         }
         blk += (d.n + PBLK - 1) / PBLK;
@@ -404,11 +423,9 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     s.nmesh = mesh;
     s.nspec = spec;
     s.ntile = tile;
-    s.wa = wa;
-    s.wb = wb;
-    s.wc = wc;
-    s.wp = wp;
-    s.max_plane = maxp;
+    s.plane_max = plane_max_mesh();
+    s.gather_bufs = precision == P3M_FP32 ? 2 : 1;
+    plan_mesh_passes(ctx);
     s.nblk = blk;
     s.max_mesh = maxm;
     plan_lists(ctx, -1.0, p >= 148 * 256 * 2 ? 1 : (p >= 148 * 64 ? 2 : 4));
@@ -485,7 +502,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
         ctx->pp_nblk_cap = nb8;
         CKC(dalloc(&s.u_pp_part, (size_t)nb8));
     }
-    CKC(dalloc(&s.u_pm_part, (size_t)wc + wp));
+    CKC(dalloc(&s.u_pm_part, (size_t)wc_cap));
     CKC(dalloc(&s.kin_part, (size_t)blk));
     CKC(dalloc(&s.rep_out, (size_t)8 * n_reps));
     CKC(dalloc(&s.status, 1));
@@ -1441,21 +1458,33 @@ extern "C" int p3m_set_priority(p3m_ctx *ctx, int level)
     return P3M_OK;
 }
 
-extern "C" int p3m_set_pp_config(p3m_ctx *ctx, int tpi, double skin)
+extern "C" int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t)
 {
-    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    if (!ctx || !t) return fail(ctx, P3M_EARG, "p3m_set_tuning", "NULL argument");
+    const int tpi = t->pp_tpi;
     if (!(tpi == 1 || tpi == 2 || tpi == 4 || tpi == 8))
-        return fail(ctx, P3M_EARG, "p3m_set_pp_config", "tpi must be 1, 2, 4 or 8");
+        return fail(ctx, P3M_EARG, "p3m_set_tuning", "pp_tpi must be 1, 2, 4 or 8");
+    if (t->cell_div != 1 && t->cell_div != 2)
+        return fail(ctx, P3M_EARG, "p3m_set_tuning", "cell_div must be 1 or 2");
+    if (t->plane_max != 0 && t->plane_max != 32 && t->plane_max != plane_max_mesh())
+        return fail(ctx, P3M_EARG, "p3m_set_tuning", "plane_max must be 0, 32 or 64");
+    if (t->gather_bufs != 1 && t->gather_bufs != 2)
+        return fail(ctx, P3M_EARG, "p3m_set_tuning", "gather_bufs must be 1 or 2");
     for (int r = 0; r < ctx->nrep; ++r)
-        if (skin > 0.5 * ctx->desc[r].rc)
-            return fail(ctx, P3M_EARG, "p3m_set_pp_config", "skin must be <= rc/2 (negative: default)");
+        if (t->skin > 0.5 * ctx->desc[r].rc)
+            return fail(ctx, P3M_EARG, "p3m_set_tuning", "skin must be <= rc/2 (negative: default)");
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->st));
     for (auto &row : ctx->graph)
         for (auto &g : row)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     DevState &s = ctx->s;
-    plan_lists(ctx, skin, tpi);
+    s.cell_div = t->cell_div;
+    s.plane_max = t->plane_max;
+    s.gather_bufs = ctx->prec == P3M_FP32 ? t->gather_bufs : 1;
+    ctx->skin_override = t->skin < 0.0 ? -1.0 : t->skin;
+    plan_lists(ctx, t->skin, tpi);
+    plan_mesh_passes(ctx);
     const long long need = (long long)((s.ntot + 31) / 32) * 32 * s.maxnb;
     if (need > ctx->nlist_cap) {
         cudaFree(s.nlist);
@@ -1466,6 +1495,27 @@ extern "C" int p3m_set_pp_config(p3m_ctx *ctx, int tpi, double skin)
     CK(cudaMemcpy(s.reps, ctx->rh.data(), sizeof(RepDev) * ctx->nrep, cudaMemcpyHostToDevice));
     launch_set_flags(s.rebuild, s.nrep, 1, ctx->st);
     return finish(ctx);
+}
+
+extern "C" int p3m_get_tuning(p3m_ctx *ctx, p3m_tuning *t)
+{
+    if (!ctx || !t) return fail(ctx, P3M_EARG, "p3m_get_tuning", "NULL argument");
+    t->pp_tpi = ctx->s.pp_tpi;
+    t->cell_div = ctx->s.cell_div;
+    t->plane_max = ctx->s.plane_max;
+    t->gather_bufs = ctx->s.gather_bufs;
+    t->skin = ctx->skin_override;
+    return P3M_OK;
+}
+
+extern "C" int p3m_set_pp_config(p3m_ctx *ctx, int tpi, double skin)
+{
+    if (!ctx) return fail(nullptr, P3M_EARG, "context", "NULL");
+    p3m_tuning t;
+    p3m_get_tuning(ctx, &t);
+    t.pp_tpi = tpi;
+    t.skin = skin;
+    return p3m_set_tuning(ctx, &t);
 }
 
 extern "C" int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, double *skin, int *maxnb)

@@ -23,11 +23,11 @@ static_assert(PENCIL == 1 << LOG_PENCIL, "PENCIL is 2^LOG_PENCIL");
 // Complex lines per item of the x passes (two real rows each): 32, or M/2 for
 // M = 32, so each radix pass has a group for every one of 256 threads.
 constexpr int XL_MAX = 32;
-// PP cells are at least (rc + skin) / CELL_DIV wide, so the neighbours of a
-// particle lie in the (2 CELL_DIV + 1)^3 cells around its own.
-constexpr int CELL_DIV = 2;
-constexpr int CELL_SPAN = 2 * CELL_DIV + 1;
-constexpr int CELL_STENCIL = CELL_SPAN * CELL_SPAN * CELL_SPAN;
+// PP cells are at least (rc + skin) / D wide (D, the cell divisor of a
+// context: 1 or 2), so the neighbours of a particle lie in the (2 D + 1)^3
+// cells around its own.
+constexpr int CELL_DIV_MAX = 2;
+__host__ __device__ constexpr int cell_stencil(int d) { return (2 * d + 1) * (2 * d + 1) * (2 * d + 1); }
 __host__ __device__ constexpr int x_lines_log(int logM) { return logM - 1 < 5 ? logM - 1 : 5; }
 constexpr int MAX_LOGM = 8;  // M <= 256
 constexpr int PBLK = 256;      // particles per block in replica-aligned particle kernels

@@ -18,6 +18,9 @@ struct DevState {
     int wp = 0;                  // plane items (fused y/z passes)
     int max_plane = 0;           // largest M among plane replicas
     int pp_tpi = 1;              // threads per particle in the PP force kernel
+    int cell_div = CELL_DIV_MAX; // PP cells are >= (rc + skin) / cell_div wide (1 or 2)
+    int plane_max = 64;          // meshes up to this side take the fused y/z plane kernel
+    int gather_bufs = 2;         // FP32 gather: field-tile buffers per CTA (1 or 2)
     int pp_nblk = 0;             // blocks of the PP force kernel (replica-aligned)
     int maxnb = 0;               // list capacity per particle
     int has_mesh = 0;

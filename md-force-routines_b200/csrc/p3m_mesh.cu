@@ -833,10 +833,7 @@ k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
 // its 216 nodes from there; each thread keeps the weights of up to GPT
 // particles across the three components.
 constexpr int G_THREADS = 256;
-#ifndef P3M_G_NBUF32
-#define P3M_G_NBUF32 2
-#endif
-template <typename T> constexpr int GNBUF = sizeof(T) == 4 ? P3M_G_NBUF32 : 1;
+
 // Gather tiles keep rows of GTX nodes (TILE padded up) so each row is filled
 // with 16-byte copies: a brick starts on a multiple of 16 nodes and M is a
 // multiple of 16, so every 16-byte chunk -- wrapped ones included -- is
@@ -844,12 +841,11 @@ template <typename T> constexpr int GNBUF = sizeof(T) == 4 ? P3M_G_NBUF32 : 1;
 constexpr int GTX = 24;
 constexpr int GTILE = TILE * TILE * GTX;
 
-#ifndef P3M_G_MINB
-#define P3M_G_MINB 1
-#endif
-
-template <typename T>
-__global__ void __launch_bounds__(G_THREADS, P3M_G_MINB)
+// NB field-tile buffers per CTA: with two, the copy of component c+1 is in
+// flight while component c is summed; with one, the CTA is half the size and
+// more of them share an SM (the choice is the context's gather_bufs).
+template <typename T, int NB>
+__global__ void __launch_bounds__(G_THREADS)
 k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_start,
          const int *__restrict__ brick_perm, const double *__restrict__ pos,
          const double *__restrict__ charge, const T *__restrict__ efield, long long nmesh,
@@ -934,8 +930,7 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                 weights6<T>(g_o[1][threadIdx.x], wy);
                 weights6<T>(g_o[2][threadIdx.x], wz);
             }
-            // component tiles through NBUF buffers: with two, the copy of
-            // component c+1 is in flight while component c is summed
+            // component tiles through the NB buffers
             auto issue = [&](int comp) {
                 constexpr int EPC = 16 / sizeof(T);   // elements per 16-byte chunk
                 constexpr int CPR = GTX / EPC;        // chunks per tile row
@@ -947,7 +942,7 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                     const int ch = threadIdx.x % CPR, r0 = threadIdx.x / CPR;
                     const int gx = (bx + ch * EPC) & (M - 1), gy = (by + r0 % TILE) & (M - 1);
                     const T *exy = efield + comp * nmesh + R.mesh_off + (long long)gy * M + gx;
-                    T *d = tile + (comp % GNBUF<T>) * GTILE + r0 * GTX + ch * EPC;
+                    T *d = tile + (comp % NB) * GTILE + r0 * GTX + ch * EPC;
                     for (int tz = r0 / TILE; tz < TILE; tz += RP / TILE, d += RP * GTX)
                         cp_async16(d, exy + (long long)((bz + tz) & (M - 1)) * M * M);
                 }
@@ -955,14 +950,14 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
             };
             issue(0);
             for (int comp = 0; comp < 3; ++comp) {
-                if (GNBUF<T> == 2 && comp + 1 < 3) {
+                if (NB == 2 && comp + 1 < 3) {
                     issue(comp + 1);
                     asm volatile("cp.async.wait_group 1;\n" ::: "memory");
                 } else {
                     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
                 }
                 __syncthreads();
-                const T *tl = tile + (comp % GNBUF<T>) * GTILE;
+                const T *tl = tile + (comp % NB) * GTILE;
                 if (base >= 0) {
                     // separable contraction: sum_g wz sum_a wy sum_c wx E
                     T acc = 0;
@@ -981,7 +976,7 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                     }
                     e[comp] = acc;
                 }
-                if (GNBUF<T> == 1 && comp + 1 < 3) {
+                if (NB == 1 && comp + 1 < 3) {
                     __syncthreads();
                     issue(comp + 1);
                 } else if (comp + 2 < 3) {
@@ -1109,7 +1104,8 @@ template <typename T> void configure_mesh_kernels()
     set_smem(k_fft_y<T>, fft_smem<T>(256, 1));
     set_smem(k_fft_z_green<T>, fft_smem<T>(256, 2));
     set_smem(k_fft_x_c2r<T>, x_smem<T>(256));
-    set_smem(k_gather<T>, GNBUF<T> * GTILE * sizeof(T));
+    set_smem(k_gather<T, 1>, GTILE * sizeof(T));
+    if constexpr (sizeof(T) == 4) set_smem(k_gather<T, 2>, 2 * GTILE * sizeof(T));
     set_smem(k_fft_plane<T>, plane_smem<T>(PLANE_MAX));
 }
 
@@ -1149,7 +1145,7 @@ template <typename T> void launch_fft_forward(const DevState &s, cudaStream_t st
 }
 
 int fft_kernel_count(const DevState &s) { return 2 + (s.wb > 0 ? 3 : 0) + (s.wp > 0 ? 1 : 0); }
-int plane_max_mesh() { return PLANE_MAX; }
+int plane_max_mesh() { return PLANE_MAX; }  // the largest side the plane kernel takes
 
 template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st)
 {
@@ -1165,9 +1161,15 @@ template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st
 
 template <typename T> void launch_gather(const DevState &s, cudaStream_t st)
 {
-    k_gather<T><<<grid_items(s.nbrick, 148 * 16), G_THREADS, GNBUF<T> * GTILE * sizeof(T), st>>>(
-        s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (const T *)s.efield,
-        s.nmesh, (typename V4<T>::t *)s.acc_pm, s.nbrick);
+    const int grid = grid_items(s.nbrick, 148 * 16);
+    if (sizeof(T) == 4 && s.gather_bufs == 2)
+        k_gather<T, 2><<<grid, G_THREADS, 2 * GTILE * sizeof(T), st>>>(
+            s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (const T *)s.efield,
+            s.nmesh, (typename V4<T>::t *)s.acc_pm, s.nbrick);
+    else
+        k_gather<T, 1><<<grid, G_THREADS, GTILE * sizeof(T), st>>>(
+            s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (const T *)s.efield,
+            s.nmesh, (typename V4<T>::t *)s.acc_pm, s.nbrick);
 }
 
 void launch_reduce_pm(const DevState &s, cudaStream_t st)

@@ -101,19 +101,21 @@ __device__ __forceinline__ long long list_index(int s, int k, int maxnb)
 constexpr int LB_THREADS = 256;
 constexpr int LB_TPI = 16;                    // lanes per particle
 constexpr int LB_PPB = LB_THREADS / LB_TPI;   // particles per pass
+constexpr int LB_HC = 256;                    // home particles per chunk
 template <typename T> __host__ __device__ constexpr int lb_scap() { return sizeof(T) == 4 ? 1024 : 512; }
-static_assert(CELL_STENCIL <= LB_THREADS, "one thread per stencil cell");
+static_assert(cell_stencil(CELL_DIV_MAX) <= LB_THREADS, "one thread per stencil cell");
 static_assert(LB_TPI >= PP_LIST_PAD, "one pad entry per lane at most");
 
-// One CTA per cell (about 10 particles: cells are (rc + skin)/2 wide) of the
-// replicas rebuilding this step (the list k_scan wrote). The CELL_STENCIL
-// neighbour cells' coordinates are staged in shared memory in the fixed
-// stencil order (x fastest, offsets -CELL_DIV .. CELL_DIV); the LB_TPI lanes
-// of a particle test LB_TPI consecutive candidates per round, and a warp
-// ballot gives each candidate in range its place: the list holds the
-// in-range candidates in stencil order, as a scan by one thread would, with
-// no padding.
-template <typename T>
+// One CTA per cell of the replicas rebuilding this step (the list k_scan
+// wrote); cells are (rc + skin)/D wide (about 10 particles at D = 2 and unit
+// density 3/(4 pi), 80 at D = 1). The (2D+1)^3 neighbour cells'
+// coordinates are staged in shared memory in the fixed stencil order (x
+// fastest, offsets -D .. D), a window of SCAP candidates at a time; the
+// LB_TPI lanes of a particle test LB_TPI consecutive candidates per round,
+// and a warp ballot gives each candidate in range its place: the list holds
+// the in-range candidates in stencil order, as a scan by one thread would,
+// then the particle's own index up to a whole block of PP_LIST_PAD entries.
+template <typename T, int D>
 __global__ void __launch_bounds__(LB_THREADS)
 k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
               const typename Coord<T>::Q *__restrict__ xq, int *__restrict__ nnb,
@@ -122,11 +124,14 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
 {
     using Q = typename Coord<T>::Q;
     constexpr int SCAP = lb_scap<T>();
+    constexpr int CELL_SPAN = 2 * D + 1;
+    constexpr int CELL_STENCIL = cell_stencil(D);
     extern __shared__ __align__(16) unsigned char lb_smem[];
     Q *stage = reinterpret_cast<Q *>(lb_smem);
     __shared__ int pre[CELL_STENCIL + 1];  // candidates before stencil cell k
     __shared__ int nstart[CELL_STENCIL];   // first sorted index of stencil cell k
     __shared__ int wsum[LB_THREADS / 32];
+    __shared__ int cnt_sm[LB_HC];          // list length so far of each particle of the chunk
     const int tid = threadIdx.x, lane = tid & 31;
     const int sub = tid % LB_TPI;
     const int gshift = lane & ~(LB_TPI - 1);            // first lane of this particle's group
@@ -148,8 +153,8 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
         // stencil cell tid: its start and count; pre = exclusive prefix sum
         int cntc = 0;
         if (tid < CELL_STENCIL) {
-            const int dx = tid % CELL_SPAN - CELL_DIV, dy = (tid / CELL_SPAN) % CELL_SPAN - CELL_DIV,
-                      dz = tid / (CELL_SPAN * CELL_SPAN) - CELL_DIV;
+            const int dx = tid % CELL_SPAN - D, dy = (tid / CELL_SPAN) % CELL_SPAN - D,
+                      dz = tid / (CELL_SPAN * CELL_SPAN) - D;
             const int nx = (cx + dx + nc) % nc, ny = (cy + dy + nc) % nc, nz = (cz + dz + nc) % nc;
             const int nb = R.cell_off + nx + nc * (ny + nc * nz);
             nstart[tid] = cell_start[nb];
@@ -168,16 +173,16 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
         if (tid == 0) pre[0] = 0;
         __syncthreads();
         const int total = pre[CELL_STENCIL];
-        for (int i0 = 0; i0 < nhome; i0 += LB_PPB) {
-            const int i = i0 + tid / LB_TPI;
-            const bool have = i < nhome;
-            const int s = hstart + i;
-            Q xi;
-            if (have) xi = xq[s];
-            int cnt = 0;
+        // home particles in chunks of LB_HC: each window of candidates is
+        // staged once per chunk, and every particle's count so far is kept
+        // in shared memory between windows
+        for (int c0 = 0; c0 < nhome; c0 += LB_HC) {
+            const int nch = min(LB_HC, nhome - c0);
             for (int w0 = 0; w0 < total; w0 += SCAP) {
                 const int wlen = min(SCAP, total - w0);
-                __syncthreads();
+                __syncthreads();  // the previous window's tests (and counts) are done
+                if (w0 == 0)
+                    for (int i = tid; i < nch; i += LB_THREADS) cnt_sm[i] = 0;
                 // candidate g of the window: the stencil cell holding it by
                 // binary search over pre
                 for (int g = tid; g < wlen; g += LB_THREADS) {
@@ -193,29 +198,40 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                     stage[g] = q;
                 }
                 __syncthreads();
-                for (int kb = 0; kb < wlen; kb += LB_TPI) {  // uniform over the block
-                    const int k = kb + sub;
-                    bool in = false;
-                    int j = 0;
-                    if (have && k < wlen) {
-                        const Q q = stage[k];
-                        const float dx = (float)qdiff<T>(xi.x, q.x) * sc;
-                        const float dy = (float)qdiff<T>(xi.y, q.y) * sc;
-                        const float dz = (float)qdiff<T>(xi.z, q.z) * sc;
-                        j = (int)q.w;
-                        in = (dx * dx + dy * dy + dz * dz < rl2) && j != s;
+                for (int i0 = 0; i0 < nch; i0 += LB_PPB) {
+                    const int i = i0 + tid / LB_TPI;
+                    const bool have = i < nch;
+                    const int s = hstart + c0 + i;
+                    Q xi;
+                    if (have) xi = xq[s];
+                    int cnt = have ? cnt_sm[i] : 0;
+                    for (int kb = 0; kb < wlen; kb += LB_TPI) {  // uniform over the block
+                        const int k = kb + sub;
+                        bool in = false;
+                        int j = 0;
+                        if (have && k < wlen) {
+                            const Q q = stage[k];
+                            const float dx = (float)qdiff<T>(xi.x, q.x) * sc;
+                            const float dy = (float)qdiff<T>(xi.y, q.y) * sc;
+                            const float dz = (float)qdiff<T>(xi.z, q.z) * sc;
+                            j = (int)q.w;
+                            in = (dx * dx + dy * dy + dz * dz < rl2) && j != s;
+                        }
+                        const unsigned grp = (__ballot_sync(0xffffffffu, in) >> gshift) &
+                                             ((1u << LB_TPI) - 1u);
+                        if (in) {
+                            const int pos = cnt + __popc(grp & below);
+                            if (pos < maxnb) nlist[list_index(s, pos, maxnb)] = j;
+                        }
+                        cnt += __popc(grp);
                     }
-                    const unsigned grp = (__ballot_sync(0xffffffffu, in) >> gshift) &
-                                         ((1u << LB_TPI) - 1u);
-                    if (in) {
-                        const int pos = cnt + __popc(grp & below);
-                        if (pos < maxnb) nlist[list_index(s, pos, maxnb)] = j;
-                    }
-                    cnt += __popc(grp);
+                    if (have && sub == 0) cnt_sm[i] = cnt;
                 }
             }
-            if (have) {
-                const int nn = min(cnt, maxnb);
+            __syncthreads();  // the chunk's counts are complete
+            for (int i = tid / LB_TPI; i < nch; i += LB_PPB) {
+                const int s = hstart + c0 + i;
+                const int cnt = cnt_sm[i], nn = min(cnt, maxnb);
                 if (sub == 0) {
                     if (cnt > maxnb) raise_status(status, ST_NBOVF);
                     nnb[s] = nn;
@@ -555,7 +571,9 @@ int pp_particles_per_block(int tpi) { return PPL_THREADS / tpi; }
 template <typename T> void configure_pp_kernels()
 {
     using Q = typename Coord<T>::Q;
-    cudaFuncSetAttribute(k_build_lists<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_build_lists<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(lb_scap<T>() * sizeof(Q)));
+    cudaFuncSetAttribute(k_build_lists<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(lb_scap<T>() * sizeof(Q)));
     const int tab = sizeof(T) == 4 ? (int)(PP_TABLE_N * sizeof(float4)) : 0;
     cudaFuncSetAttribute(k_pp_list<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
@@ -580,7 +598,8 @@ template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st
 {
     using Q = typename Coord<T>::Q;
     const int grid = s.ncell < 148 * 16 ? s.ncell : 148 * 16;
-    k_build_lists<T><<<grid, LB_THREADS, lb_scap<T>() * sizeof(Q), st>>>(
+    auto kern = s.cell_div == 1 ? k_build_lists<T, 1> : k_build_lists<T, 2>;
+    kern<<<grid, LB_THREADS, lb_scap<T>() * sizeof(Q), st>>>(
         s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.rb_list, s.nrep,
         s.status);
 }

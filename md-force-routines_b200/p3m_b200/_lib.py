@@ -37,6 +37,21 @@ class P3MError(RuntimeError):
         self.code = code
 
 
+class Tuning(ctypes.Structure):
+    """p3m_tuning of include/p3m_b200.h: the kernel shapes of a context."""
+
+    _fields_ = [
+        ("pp_tpi", ctypes.c_int32),
+        ("cell_div", ctypes.c_int32),
+        ("plane_max", ctypes.c_int32),
+        ("gather_bufs", ctypes.c_int32),
+        ("skin", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ReplicaDesc(ctypes.Structure):
     """p3m_replica_desc of include/p3m_b200.h."""
 
@@ -111,6 +126,8 @@ SIGNATURES = {
     "p3m_set_pp_config": (_I, [_V, _I, ctypes.c_double]),
     "p3m_get_pp_config": (_I, [_V, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double),
                                ctypes.POINTER(_I)]),
+    "p3m_set_tuning": (_I, [_V, ctypes.POINTER(Tuning)]),
+    "p3m_get_tuning": (_I, [_V, ctypes.POINTER(Tuning)]),
     "p3m_profile_stages": (_I, [_V, _I, _D, _I, ctypes.POINTER(_I)]),
     "p3m_stage_name": (ctypes.c_char_p, [_I]),
     "p3m_fp32_peak": (_I, [_I, _D]),

@@ -1,15 +1,31 @@
-"""Autotuner of the PP stage: threads per particle in the force kernel and the
-Verlet-list skin (larger skins rebuild less often but visit more list
-entries). It times short device-resident NVE runs of the caller's own
-context -- so the state should already be equilibrated -- and installs the
-fastest setting. Results are cached per workload signature in a JSON file.
+"""Autotuner of a context's kernel shapes, by timing its own NVE steps.
+
+What it searches (p3m_tuning of the C ABI):
+
+* the PP stage: threads per particle in the pair kernel and the Verlet-list
+  skin (larger skins rebuild less often but visit more list entries) -- a
+  grid of both, since they interact;
+* the list cells: (rc + skin)/2 or (rc + skin) wide (cell_div 2 or 1: a
+  125-cell stencil of small cells, or 27 larger cells whose candidates are
+  staged once for many particles);
+* the FFT tiles of meshes up to 64^3: the fused y/z plane kernel (a whole kx
+  plane per CTA) or the y and z pencil passes (16 lines per CTA);
+* the FP32 gather: one or two field-tile buffers per CTA (copy/compute
+  overlap against CTAs per SM).
+
+The last three are searched one at a time from the best PP setting
+(coordinate descent), then the fastest few settings are timed again over
+twice the steps (list rebuilds come every few tens of steps, so short runs
+rank close candidates by chance) and the fastest is installed. The state
+should already be equilibrated: each timing advances the system. Results are
+cached per workload signature in a JSON file.
 """
 from __future__ import annotations
 
 import json
 import os
 
-from ._lib import MODE_NVE
+from ._lib import FP32, MODE_NVE
 
 CANDIDATES = [(tpi, skin) for tpi in (1, 2, 4) for skin in (0.5, 0.8, 1.1, 1.4)]
 CACHE = os.environ.get("P3M_B200_TUNE_CACHE",
@@ -37,28 +53,39 @@ def _save(d):
         pass
 
 
-def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3):
-    """Time each (threads per particle, skin) candidate over `steps` NVE steps
-    (CUDA events on the context's stream), time the `finalists` fastest again
-    over 2 `steps` (list rebuilds come every few tens of steps, so short runs
-    rank close candidates by chance) and install the fastest of those.
-    Returns {"choice": (tpi, skin), "ms_per_step": {...}, "final_ms_per_step":
-    {...}}. Advances the system by warm + steps per candidate and warm + 2
-    steps per finalist."""
+def _key(t):
+    return f"tpi{t['pp_tpi']},skin{t['skin']:g},div{t['cell_div']},plane{t['plane_max']},gbuf{t['gather_bufs']}"
+
+
+def shape_options(ctx):
+    """The values of each non-PP shape worth trying on this context."""
+    opts = {"cell_div": (2, 1)}
+    if any(0 < r.M <= 64 for r in ctx.replicas):
+        opts["plane_max"] = (64, 0)
+    if ctx.precision == FP32 and any(r.M > 0 for r in ctx.replicas):
+        opts["gather_bufs"] = (2, 1)
+    return opts
+
+
+def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, shapes=True):
+    """Search the kernel shapes (see the module docstring) and install the
+    fastest. Returns {"choice": {tuning}, "ms_per_step": {setting: ms},
+    "final_ms_per_step": {setting: ms}}."""
     import torch
 
     sig = signature(ctx)
     cache = _load() if use_cache else {}
-    if use_cache and sig in cache:
-        tpi, skin = cache[sig]["choice"]
-        max_skin = min(0.5 * r.rc for r in ctx.replicas)
-        ctx.set_pp_config(tpi, min(skin, max_skin))
+    max_skin = min(0.5 * r.rc for r in ctx.replicas)
+    if use_cache and sig in cache and isinstance(cache[sig].get("choice"), dict):
+        choice = dict(cache[sig]["choice"])
+        choice["skin"] = min(choice["skin"], max_skin)
+        ctx.set_tuning(**choice)
         return cache[sig]
     stream = torch.cuda.ExternalStream(ctx.stream())
-    max_skin = min(0.5 * r.rc for r in ctx.replicas)
+    base = ctx.tuning()
 
-    def timed(tpi, skin, n):
-        ctx.set_pp_config(tpi, skin)
+    def timed(t, n):
+        ctx.set_tuning(**t)
         ctx.run(warm, MODE_NVE, graph=True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -67,18 +94,30 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3):
         e1.synchronize()
         return e0.elapsed_time(e1) / n
 
-    times = {}
+    times, settings = {}, {}
+
+    def trial(t):
+        k = _key(t)
+        if k not in times:
+            times[k] = timed(t, steps)
+            settings[k] = dict(t)
+        return times[k]
+
     for tpi, skin in (candidates or CANDIDATES):
         if skin <= max_skin:
-            times[f"{tpi},{skin}"] = timed(tpi, skin, steps)
+            trial(dict(base, pp_tpi=tpi, skin=skin))
+    best = dict(settings[min(times, key=times.get)])
+    if shapes:
+        for name, values in shape_options(ctx).items():
+            for v in values:
+                trial(dict(best, **{name: v}))
+            best = dict(settings[min(times, key=times.get)])
     final = {}
-    for key in sorted(times, key=times.get)[:max(1, finalists)]:
-        tpi, skin = key.split(",")
-        final[key] = timed(int(tpi), float(skin), 2 * steps)
-    best = min(final, key=final.get)
-    tpi, skin = best.split(",")
-    choice = (int(tpi), float(skin))
-    ctx.set_pp_config(*choice)
+    for k in sorted(times, key=times.get)[:max(1, finalists)]:
+        final[k] = timed(settings[k], 2 * steps)
+    win = min(final, key=final.get)
+    choice = settings[win]
+    ctx.set_tuning(**choice)
     result = {"choice": choice, "ms_per_step": times, "final_ms_per_step": final}
     if use_cache:
         cache[sig] = result

@@ -8,7 +8,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._lib import FP32, FP64, MODE_NVE, MODE_THERMOSTAT, P3MError, ReplicaDesc, check, dptr, lib
+from ._lib import (FP32, FP64, MODE_NVE, MODE_THERMOSTAT, P3MError, ReplicaDesc, Tuning, check,
+                   dptr, lib)
 
 
 @dataclass
@@ -384,6 +385,25 @@ class Context:
     def set_pp_config(self, tpi, skin=-1.0):
         """Threads per particle of the PP force kernel and the list skin."""
         self._ck(lib().p3m_set_pp_config(self.handle, int(tpi), float(skin)))
+
+    def tuning(self):
+        """{pp_tpi, cell_div, plane_max, gather_bufs, skin}: the kernel shapes."""
+        t = Tuning()
+        self._ck(lib().p3m_get_tuning(self.handle, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        """Change some of the kernel shapes (the others keep their values):
+        pp_tpi (1, 2, 4, 8), cell_div (1, 2), plane_max (0, 32, 64),
+        gather_bufs (1, 2), skin."""
+        cur = self.tuning()
+        unknown = set(kw) - set(cur)
+        if unknown:
+            raise ValueError(f"unknown tuning keys {sorted(unknown)}")
+        cur.update(kw)
+        t = Tuning(int(cur["pp_tpi"]), int(cur["cell_div"]), int(cur["plane_max"]),
+                   int(cur["gather_bufs"]), float(cur["skin"]))
+        self._ck(lib().p3m_set_tuning(self.handle, ctypes.byref(t)))
 
     def pp_config(self):
         """-> (threads per particle, skin, list capacity)."""

@@ -365,10 +365,11 @@ def test_async_state_copies_on_two_contexts():
 
 
 def test_autotune_installs_a_finalist():
-    """The PP autotuner times the candidates, re-times the fastest and
-    installs the best finalist."""
+    """The autotuner times the PP candidates, then each other kernel shape
+    from the best of them, re-times the fastest settings and installs the
+    best finalist."""
     from p3m_b200 import FP32, Context, Replica
-    from p3m_b200.autotune import tune
+    from p3m_b200.autotune import shape_options, tune
 
     N = 3000
     L = (4 * np.pi * N / 3) ** (1 / 3)
@@ -377,13 +378,61 @@ def test_autotune_installs_a_finalist():
     with Context([r, r], precision=FP32) as c:
         c.set_state_all(np.concatenate([pos, pos]), np.concatenate([vel, vel]))
         c.init_forces()
+        assert set(shape_options(c)) == {"cell_div", "plane_max", "gather_bufs"}
         res = tune(c, steps=10, use_cache=False, candidates=[(1, 0.5), (2, 0.8), (4, 1.1)],
                    finalists=2)
-        assert len(res["ms_per_step"]) == 3 and len(res["final_ms_per_step"]) == 2
+        # 3 PP settings, then one new setting per other shape value
+        assert len(res["ms_per_step"]) == 3 + 3 and len(res["final_ms_per_step"]) == 2
         best = min(res["final_ms_per_step"], key=res["final_ms_per_step"].get)
-        assert tuple(res["choice"]) == (int(best.split(",")[0]), float(best.split(",")[1]))
-        tpi, skin, _ = c.pp_config()
-        assert (tpi, skin) == tuple(res["choice"])
+        assert best in res["ms_per_step"]
+        assert c.tuning() == res["choice"]
+
+
+@pytest.mark.parametrize("prec_name", ["fp32", "fp64"])
+def test_kernel_shapes_agree(prec_name):
+    """Every kernel shape computes the same forces and energies: cell divisor
+    1 or 2, the fused plane FFT or the pencil passes for a 32^3 and a 64^3
+    replica, one or two gather buffers -- to rounding (FP64: 1e-12; FP32:
+    1e-6 of the RMS force) -- and the pencil FFT path matches the oracle."""
+    from p3m_b200 import FP32, FP64, Context, Replica, gf_opt_device
+
+    prec = {"fp32": FP32, "fp64": FP64}[prec_name]
+    reps = []
+    for N, M in ((2500, 32), (4000, 64)):
+        L = (4 * np.pi * N / 3) ** (1 / 3)
+        reps.append(Replica(N=N, L=L, kappa=1.0, alpha=0.8, rc=L / 3.4, M=M))
+    states = [_init_state(r, 30 + i)[0] for i, r in enumerate(reps)]
+    pos = np.concatenate(states)
+    out = {}
+    for shape in ({}, {"cell_div": 1}, {"plane_max": 0}, {"plane_max": 32}, {"gather_bufs": 1}):
+        with Context(reps, precision=prec) as c:
+            c.set_tuning(**shape)
+            assert all(c.tuning()[k] == v for k, v in shape.items()) or prec_name == "fp64"
+            c.set_state_all(pos, np.zeros_like(pos))
+            c.init_forces()
+            acc = c.get_state_all()[2]
+            st = [c.replica_stats(i) for i in range(2)]
+        out[str(shape)] = (acc, st)
+    acc0, st0 = out["{}"]
+    tol = 1e-12 if prec_name == "fp64" else 1e-6
+    for k, (acc, st) in out.items():
+        assert rel_rms(acc, acc0) < tol, k
+        for a, b in zip(st, st0):  # U = U_short + U_fft + U_self cancels: judge on U_short
+            assert abs(a["U"] - b["U"]) <= tol * abs(b["U_short"]), k
+    if prec_name == "fp64":
+        # the pencil passes on the 64^3 replica against the oracle's chain
+        r, p = reps[1], states[1]
+        G, _ = gf_opt_device(r.kappa, r.alpha, 6, 3, r.M, r.L)
+        with Context(r, precision=FP64) as c:
+            c.set_tuning(plane_max=0)
+            c.set_green(G)
+            U, acc, _, _ = c.pm(p)
+        kv = 2 * np.pi * (np.arange(r.M) - r.M // 2) / r.L
+        h = r.L / r.M
+        Uo, ao, _ = O.pm(p, np.ones(r.N), G, kv.reshape(1, r.M), kv.reshape(r.M, 1),
+                         kv.reshape(r.M, 1, 1), r.M, r.M, r.M, h, h, h, r.L, r.L, r.L)
+        assert U == pytest.approx(Uo, rel=1e-10)
+        assert rel_rms(acc, ao) < 1e-10
 
 
 def test_get_step_async_matches_sync_reads():
