@@ -312,7 +312,7 @@ int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, double *skin, int *maxnb);
 /* Kernel shapes of a context (no counterpart in the reference, whose PP and
  * PM stages have no GPU path): what the autotuner of the Python package
  * searches. p3m_create picks pp_tpi from the particle count, cell_div 2,
- * plane_max 64 and gather_bufs 2 (FP32; FP64 always uses 1). Setting waits
+ * plane_max 64 and gather_bufs 1 (FP64 always uses 1). Setting waits
  * for the context's work, drops its captured step graphs and forces a list
  * rebuild. Every setting computes the same sums; they differ only in the
  * order of additions (pair order in the lists, lanes per particle, FFT

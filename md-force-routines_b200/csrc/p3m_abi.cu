@@ -424,7 +424,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     s.nspec = spec;
     s.ntile = tile;
     s.plane_max = plane_max_mesh();
-    s.gather_bufs = precision == P3M_FP32 ? 2 : 1;
+    s.gather_bufs = 1;
     plan_mesh_passes(ctx);
     s.nblk = blk;
     s.max_mesh = maxm;

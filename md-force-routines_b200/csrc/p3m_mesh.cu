@@ -842,10 +842,11 @@ constexpr int GTX = 24;
 constexpr int GTILE = TILE * TILE * GTX;
 
 // NB field-tile buffers per CTA: with two, the copy of component c+1 is in
-// flight while component c is summed; with one, the CTA is half the size and
-// more of them share an SM (the choice is the context's gather_bufs).
+// flight while component c is summed; with one, the CTA is half the size and,
+// held to 64 registers, four of them share an SM (FP32: 57 against 63 us on
+// the 20 x 64^3 ensemble). The choice is the context's gather_bufs.
 template <typename T, int NB>
-__global__ void __launch_bounds__(G_THREADS)
+__global__ void __launch_bounds__(G_THREADS, (sizeof(T) == 4 && NB == 1) ? 4 : 1)
 k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_start,
          const int *__restrict__ brick_perm, const double *__restrict__ pos,
          const double *__restrict__ charge, const T *__restrict__ efield, long long nmesh,

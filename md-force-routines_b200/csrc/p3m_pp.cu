@@ -268,65 +268,34 @@ __device__ __forceinline__ void pair_direct(double r2, const RepDev &R, double &
     f_over_r = fr * rinv;
 }
 
-// FP32: tab holds the cubic coefficients of psi in the interval coordinate
-// u in [0,1), one float4 per interval; t = r / h, g = psi - t dpsi/du.
-__device__ __forceinline__ void pair_table(float r2, const float4 *__restrict__ tab, float inv_h,
-                                           float &f_over_r, float &phi)
-{
-    const float rinv = rsqrtf(r2);
-    const float r = r2 * rinv;
-    const float t = r * inv_h;  // in [0, PP_TABLE_N) inside the cutoff
-    // i = round(t - 1/2) and float(i) by the 1.5 * 2^23 rounding constant
-    // (exact for |t| < 2^22), without float <-> int conversions
-    const float tb = (t - 0.5f) + 12582912.0f;
-    const int i = min(__float_as_int(tb) - 0x4B400000, PP_TABLE_N - 1);
-    const float u = t - (tb - 12582912.0f);
-    const float4 c = tab[i];
-    const float ps = fmaf(fmaf(fmaf(c.w, u, c.z), u, c.y), u, c.x);
-    const float dps = fmaf(fmaf(3.0f * c.w, u, 2.0f * c.z), u, c.y);
-    const float g = fmaf(-t, dps, ps);
-    f_over_r = g * (rinv * rinv) * rinv;
-    phi = ps * rinv;
-}
-
 // ---------------------------------------------------------------------------
 // forces from the lists
 // ---------------------------------------------------------------------------
 constexpr int PPL_THREADS = 256;
 
-template <typename T, int TPI>
+// FP64 forces from the lists: the reference's pair terms (pair_direct) per
+// entry, TPI threads per particle, Kahan-compensated sums.
+template <int TPI>
 __global__ void __launch_bounds__(PPL_THREADS)
-k_pp_list(const RepDev *__restrict__ reps, int nrep, const typename Coord<T>::Q *__restrict__ xq,
-          const int *__restrict__ nnb, const int *__restrict__ nlist, int maxnb,
-          const float4 *__restrict__ tables, typename V4<T>::t *__restrict__ acc_out,
-          double *__restrict__ u_part)
+k_pp_f64(const RepDev *__restrict__ reps, int nrep, const ulonglong4 *__restrict__ xq,
+         const int *__restrict__ nnb, const int *__restrict__ nlist, int maxnb,
+         double4 *__restrict__ acc_out, double *__restrict__ u_part)
 {
-    using Q = typename Coord<T>::Q;
-    constexpr bool F32 = sizeof(T) == 4;
+    using T = double;
+    using Q = ulonglong4;
     constexpr int PPB = PPL_THREADS / TPI;  // particles per block
     constexpr int CH = 32;                  // entries per Kahan flush
     __shared__ double red[32];
-    extern __shared__ __align__(16) float4 ppl_tab[];  // FP32: this replica's table
     const int b = blockIdx.x;
     const int r = find_rep(b, nrep, [&](int k) { return reps[k].pp_blk_off; });
     const RepDev &R = reps[r];
-    if constexpr (F32) {
-        // every block works on one replica: stage its pair-function table
-        const float4 *src = tables + (long long)r * PP_TABLE_N;
-        for (int k = threadIdx.x; k < PP_TABLE_N; k += PPL_THREADS) cp_async16(ppl_tab + k, src + k);
-        cp_async_wait_all();
-        __syncthreads();
-    }
     const int sub = threadIdx.x % TPI;
     const int s = R.p_off + (b - R.pp_blk_off) * PPB + threadIdx.x / TPI;
     const bool have = s < R.p_off + R.n;
-    // L / 2^B as a hi + lo pair: a plain FP32 scale would bias every dx of
-    // the replica by the same relative rounding, which adds up coherently
+    // L / 2^64 as a hi + lo pair
     const double scd = R.L / Coord<T>::scale;
     const T sc = (T)scd, sc_lo = (T)(scd - (double)sc);
     const T rc2 = (T)(R.rc * R.rc);
-    const float4 *tab = ppl_tab;
-    const float inv_h = (float)(PP_TABLE_N / R.rc);
 
     T fx = 0, fy = 0, fz = 0, gx = 0, gy = 0, gz = 0;
     double u = 0.0;
@@ -359,11 +328,7 @@ k_pp_list(const RepDev *__restrict__ reps, int nrep, const typename Coord<T>::Q 
                     const T r2 = dx * dx + dy * dy + dz * dz;
                     if (r2 < rc2 && r2 > (T)0) {
                         T fr, ph;
-                        if constexpr (F32) {
-                            pair_table(r2, tab, inv_h, fr, ph);
-                        } else {
-                            pair_direct(r2, R, fr, ph);
-                        }
+                        pair_direct(r2, R, fr, ph);
                         px += fr * dx;
                         py += fr * dy;
                         pz += fr * dz;
@@ -383,14 +348,7 @@ k_pp_list(const RepDev *__restrict__ reps, int nrep, const typename Coord<T>::Q 
         fy += __shfl_xor_sync(0xffffffffu, fy, o);
         fz += __shfl_xor_sync(0xffffffffu, fz, o);
     }
-    if (have && sub == 0) {
-        typename V4<T>::t a;
-        a.x = fx;
-        a.y = fy;
-        a.z = fz;
-        a.w = (T)0;
-        acc_out[s] = a;
-    }
+    if (have && sub == 0) acc_out[s] = make_double4(fx, fy, fz, 0.0);
     const double ut = block_sum(u, red);
     if (threadIdx.x == 0) u_part[b] = ut;
 }
@@ -410,6 +368,17 @@ k_pp_list(const RepDev *__restrict__ reps, int nrep, const typename Coord<T>::Q 
 #ifndef P3M_PP_PACK
 #define P3M_PP_PACK 0
 #endif
+// Copies of the pair table in shared memory. A warp's 128-bit table reads go
+// through the banks eight lanes at a time; with random intervals two of
+// those lanes often hit the same bank group (8.4 wavefronts per read measured
+// on the ensemble, against 4 without conflicts). With 8 copies, copy c held
+// in bank group c only (entry i at float4 index 8 i + c) and read by the
+// lanes l with l mod 8 = c, no two lanes of a phase can conflict.
+#ifndef P3M_PP_TABLE_COPIES
+#define P3M_PP_TABLE_COPIES 1
+#endif
+constexpr int PP_TABLE_COPIES = P3M_PP_TABLE_COPIES;
+static_assert(PP_TABLE_COPIES == 1 || PP_TABLE_COPIES == 8, "1 or 8 table copies");
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
@@ -430,7 +399,12 @@ template <bool P> __device__ __forceinline__ float2 v_add(float2 a, float2 b)
 }
 
 // Two candidates a, b of particle xi: adds F/r * (dx, dy, dz) and phi of the
-// ones closer than rc (and not the particle itself) to p*.
+// ones closer than rc (and not the particle itself) to p*. tab holds the
+// cubic coefficients of psi = phi r in the interval coordinate u in [0,1),
+// one float4 per interval of h = rc / PP_TABLE_N; with t = r / h, the
+// interval i = round(t - 1/2) and float(i) come from the 1.5 * 2^23 rounding
+// constant (exact for t < 2^22, no float <-> int conversions), and the force
+// from the same cubic: g = F r^2 = psi - t dpsi/du, F/r = g / r^3, phi = psi / r.
 template <bool P>
 __device__ __forceinline__ void pair_table2(const uint4 &xi, const uint4 &qa, const uint4 &qb,
                                             float2 sc, float2 sc_lo, float rc2, float2 inv_h,
@@ -457,7 +431,7 @@ __device__ __forceinline__ void pair_table2(const uint4 &xi, const uint4 &qa, co
     const int ib = min(__float_as_int(tb.y) - 0x4B400000, PP_TABLE_N - 1);
     const float2 fl = v_add<P>(tb, f2(-kMagic, -kMagic));       // the interval index, exact
     const float2 u = v_fma<P>(fl, f2(-1.f, -1.f), t);            // t - fl, exact
-    const float4 ca = tab[ia], cb = tab[ib];
+    const float4 ca = tab[ia * PP_TABLE_COPIES], cb = tab[ib * PP_TABLE_COPIES];
     const float2 c0 = f2(ca.x, cb.x), c1 = f2(ca.y, cb.y), c2 = f2(ca.z, cb.z), c3 = f2(ca.w, cb.w);
     const float2 ps = v_fma<P>(v_fma<P>(v_fma<P>(c3, u, c2), u, c1), u, c0);
     const float2 dps = v_fma<P>(v_fma<P>(v_mul<P>(c3, f2(3.f, 3.f)), u, v_add<P>(c2, c2)), u, c1);
@@ -493,10 +467,12 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
     const RepDev &R = reps[r];
     {
         const float4 *src = tables + (long long)r * PP_TABLE_N;
-        for (int k = threadIdx.x; k < PP_TABLE_N; k += PPL_THREADS) cp_async16(ppl_tab + k, src + k);
+        for (int k = threadIdx.x; k < PP_TABLE_N * PP_TABLE_COPIES; k += PPL_THREADS)
+            cp_async16(ppl_tab + k, src + k / PP_TABLE_COPIES);
         cp_async_wait_all();
         __syncthreads();
     }
+    const float4 *tab = ppl_tab + (threadIdx.x & (PP_TABLE_COPIES - 1));  // this lane's copy
     const int sub = threadIdx.x % TPI;
     const int s = R.p_off + (b - R.pp_blk_off) * PPB + threadIdx.x / TPI;
     const bool have = s < R.p_off + R.n;
@@ -525,7 +501,7 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
             float2 px = f2(0.f, 0.f), py = px, pz = px, pu = px;
 #pragma unroll
             for (int v = 0; v < UNR; v += 2)
-                pair_table2<P>(xi, q[v], q[v + 1], sc, sc_lo, rc2, inv_h, ppl_tab, px, py, pz, pu);
+                pair_table2<P>(xi, q[v], q[v + 1], sc, sc_lo, rc2, inv_h, tab, px, py, pz, pu);
             const float sx = px.x + px.y, sy = py.x + py.y, sz = pz.x + pz.y;
             float y = sx - gx, t = fx + y; gx = (t - fx) - y; fx = t;
             y = sy - gy; t = fy + y; gy = (t - fy) - y; fy = t;
@@ -575,12 +551,8 @@ template <typename T> void configure_pp_kernels()
                          (int)(lb_scap<T>() * sizeof(Q)));
     cudaFuncSetAttribute(k_build_lists<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(lb_scap<T>() * sizeof(Q)));
-    const int tab = sizeof(T) == 4 ? (int)(PP_TABLE_N * sizeof(float4)) : 0;
-    cudaFuncSetAttribute(k_pp_list<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
-    cudaFuncSetAttribute(k_pp_list<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
-    cudaFuncSetAttribute(k_pp_list<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
-    cudaFuncSetAttribute(k_pp_list<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
     if constexpr (sizeof(T) == 4) {
+        const int tab = (int)(PP_TABLE_N * PP_TABLE_COPIES * sizeof(float4));
         cudaFuncSetAttribute(k_pp_f32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
         cudaFuncSetAttribute(k_pp_f32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
         cudaFuncSetAttribute(k_pp_f32<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
@@ -608,14 +580,13 @@ template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cuda
 {
     using Q = typename Coord<T>::Q;
     if constexpr (sizeof(T) == 4) {
-        k_pp_f32<TPI><<<s.pp_nblk, PPL_THREADS, PP_TABLE_N * sizeof(float4), st>>>(
+        k_pp_f32<TPI><<<s.pp_nblk, PPL_THREADS, PP_TABLE_N * PP_TABLE_COPIES * sizeof(float4), st>>>(
             s.reps, s.nrep, (const uint4 *)s.xq, s.nnb, s.nlist, s.maxnb, s.pp_tables,
             (float4 *)s.acc_pp, s.u_pp_part);
     } else {
-        k_pp_list<T, TPI><<<s.pp_nblk, PPL_THREADS, 0, st>>>(s.reps, s.nrep, (const Q *)s.xq,
-                                                            s.nnb, s.nlist, s.maxnb, s.pp_tables,
-                                                            (typename V4<T>::t *)s.acc_pp,
-                                                            s.u_pp_part);
+        k_pp_f64<TPI><<<s.pp_nblk, PPL_THREADS, 0, st>>>(s.reps, s.nrep, (const Q *)s.xq, s.nnb,
+                                                         s.nlist, s.maxnb, (double4 *)s.acc_pp,
+                                                         s.u_pp_part);
     }
 }
 
