@@ -444,23 +444,38 @@ k_nqt_partial(const RepDev *__restrict__ reps, int nrep, const double *__restric
 }
 
 // Per replica: sum the block partials into out[r][nq][3] complex (re, im).
-__global__ void k_nqt_reduce(const RepDev *__restrict__ reps, int nrep, int nblk,
-                             const double *__restrict__ part, int nq, double *__restrict__ out,
-                             const int *__restrict__ counters, int ring_cap)
+// Block (r, c) sums values 32 c .. 32 c + 31 of replica r: warp w adds the
+// partials of blocks b0 + w, b0 + w + 8, ... (lane = value), then the eight
+// warp sums are added in warp order -- a fixed order, so the result does not
+// depend on timing; a large replica's thousand partial blocks are summed by
+// eight warps instead of one thread per value.
+constexpr int NQR_WARPS = 8;
+
+__global__ void __launch_bounds__(NQR_WARPS * 32)
+k_nqt_reduce(const RepDev *__restrict__ reps, int nrep, int nblk,
+             const double *__restrict__ part, int nq, double *__restrict__ out,
+             const int *__restrict__ counters, int ring_cap)
 {
-    const int r = blockIdx.x;
+    __shared__ double wsum[NQR_WARPS][32];
+    const int r = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nv = nq * 6, k = blockIdx.y * 32 + lane;
     const RepDev &R = reps[r];
     const int b0 = R.nq_blk_off, b1 = (r + 1 < nrep) ? reps[r + 1].nq_blk_off : nblk;
-    double *o = out;
-    if (counters) {
-        // ring layout [row][replica][nq][3][2]; this step's row
-        const int step = counters[3] % ring_cap;
-        o = out + (long long)step * nrep * nq * 6;
-    }
-    for (int k = threadIdx.x; k < nq * 6; k += blockDim.x) {
-        double s = 0.0;
-        for (int bb = b0; bb < b1; ++bb) s += part[(long long)bb * nq * 6 + k];
-        o[(long long)r * nq * 6 + k] = s;
+    double s = 0.0;
+    if (k < nv)
+        for (int bb = b0 + w; bb < b1; bb += NQR_WARPS) s += part[(long long)bb * nv + k];
+    wsum[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && k < nv) {
+        double t = 0.0;
+        for (int j = 0; j < NQR_WARPS; ++j) t += wsum[j][lane];
+        double *o = out;
+        if (counters) {
+            // ring layout [row][replica][nq][3][2]; this step's row
+            const int step = counters[3] % ring_cap;
+            o = out + (long long)step * nrep * nv;
+        }
+        o[(long long)r * nv + k] = t;
     }
 }
 
@@ -597,8 +612,9 @@ void launch_nqt(const DevState &s, const double *pos, const double *qmult, int n
         k_nqt_partial<T, true><<<s.nq_nblk, PBLK, smem, st>>>(s.reps, s.nrep, pos, qmult, nq, part);
     else
         k_nqt_partial<T, false><<<s.nq_nblk, PBLK, smem, st>>>(s.reps, s.nrep, pos, qmult, nq, part);
-    k_nqt_reduce<<<s.nrep, 256, 0, st>>>(s.reps, s.nrep, s.nq_nblk, part, nq, out, counters,
-                                         ring_cap);
+    const dim3 rgrid(s.nrep, (nq * 6 + 31) / 32);
+    k_nqt_reduce<<<rgrid, NQR_WARPS * 32, 0, st>>>(s.reps, s.nrep, s.nq_nblk, part, nq, out,
+                                                   counters, ring_cap);
 }
 
 int nqt_particles_per_block() { return PBLK * NQ_PPT; }
