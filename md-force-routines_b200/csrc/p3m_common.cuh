@@ -41,7 +41,7 @@ enum : int {
 
 // Intervals of the tabulated FP32 pair functions on [0, rc].
 #ifndef P3M_PP_TABLE_N
-#define P3M_PP_TABLE_N 2048
+#define P3M_PP_TABLE_N 512
 #endif
 constexpr int PP_TABLE_N = P3M_PP_TABLE_N;  // FP32 pair table: cubic intervals on [0, rc]
 // Neighbour lists are padded with the particle's own index to a multiple of
