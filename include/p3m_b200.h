@@ -312,7 +312,7 @@ int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, double *skin, int *maxnb);
 /* Kernel shapes of a context (no counterpart in the reference, whose PP and
  * PM stages have no GPU path): what the autotuner of the Python package
  * searches. p3m_create picks pp_tpi from the particle count, cell_div 2,
- * plane_max 64 and gather_bufs 1 (FP64 always uses 1). Setting waits
+ * plane_max 64 and gather_mode 1. Setting waits
  * for the context's work, drops its captured step graphs and forces a list
  * rebuild. Every setting computes the same sums; they differ only in the
  * order of additions (pair order in the lists, lanes per particle, FFT
@@ -322,7 +322,9 @@ typedef struct {
     int32_t cell_div;     /* list cells are >= (rc + skin)/cell_div wide: 1 or 2          */
     int32_t plane_max;    /* meshes with sides up to this (0, 32 or 64) take the fused
                              y/z plane FFT kernel, larger ones the y and z pencil passes */
-    int32_t gather_bufs;  /* FP32 force gather: field-tile buffers per CTA, 1 or 2         */
+    int32_t gather_mode;  /* force gather: 0 = a CTA per mesh brick and field component,
+                             1 = a CTA per brick (one tile buffer), 2 = a CTA per brick
+                             with two buffers (FP32; FP64 takes 1 for 2)              */
     double skin;          /* Verlet skin for every replica (< 0: each replica's own /
                              the default); get returns the last value set              */
 } p3m_tuning;

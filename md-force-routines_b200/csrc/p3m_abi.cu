@@ -424,7 +424,7 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     s.nspec = spec;
     s.ntile = tile;
     s.plane_max = plane_max_mesh();
-    s.gather_bufs = 1;
+    s.gather_mode = 1;
     plan_mesh_passes(ctx);
     s.nblk = blk;
     s.max_mesh = maxm;
@@ -1468,8 +1468,8 @@ extern "C" int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t)
         return fail(ctx, P3M_EARG, "p3m_set_tuning", "cell_div must be 1 or 2");
     if (t->plane_max != 0 && t->plane_max != 32 && t->plane_max != plane_max_mesh())
         return fail(ctx, P3M_EARG, "p3m_set_tuning", "plane_max must be 0, 32 or 64");
-    if (t->gather_bufs != 1 && t->gather_bufs != 2)
-        return fail(ctx, P3M_EARG, "p3m_set_tuning", "gather_bufs must be 1 or 2");
+    if (t->gather_mode < 0 || t->gather_mode > 2)
+        return fail(ctx, P3M_EARG, "p3m_set_tuning", "gather_mode must be 0, 1 or 2");
     for (int r = 0; r < ctx->nrep; ++r)
         if (t->skin > 0.5 * ctx->desc[r].rc)
             return fail(ctx, P3M_EARG, "p3m_set_tuning", "skin must be <= rc/2 (negative: default)");
@@ -1481,7 +1481,7 @@ extern "C" int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t)
     DevState &s = ctx->s;
     s.cell_div = t->cell_div;
     s.plane_max = t->plane_max;
-    s.gather_bufs = ctx->prec == P3M_FP32 ? t->gather_bufs : 1;
+    s.gather_mode = (ctx->prec == P3M_FP64 && t->gather_mode == 2) ? 1 : t->gather_mode;
     ctx->skin_override = t->skin < 0.0 ? -1.0 : t->skin;
     plan_lists(ctx, t->skin, tpi);
     plan_mesh_passes(ctx);
@@ -1503,7 +1503,7 @@ extern "C" int p3m_get_tuning(p3m_ctx *ctx, p3m_tuning *t)
     t->pp_tpi = ctx->s.pp_tpi;
     t->cell_div = ctx->s.cell_div;
     t->plane_max = ctx->s.plane_max;
-    t->gather_bufs = ctx->s.gather_bufs;
+    t->gather_mode = ctx->s.gather_mode;
     t->skin = ctx->skin_override;
     return P3M_OK;
 }

@@ -20,7 +20,8 @@ struct DevState {
     int pp_tpi = 1;              // threads per particle in the PP force kernel
     int cell_div = CELL_DIV_MAX; // PP cells are >= (rc + skin) / cell_div wide (1 or 2)
     int plane_max = 64;          // meshes up to this side take the fused y/z plane kernel
-    int gather_bufs = 2;         // FP32 gather: field-tile buffers per CTA (1 or 2)
+    int gather_mode = 1;         // gather: 0 a CTA per brick and component, 1 / 2 a CTA per
+                                 // brick with one / two tile buffers (2: FP32 only)
     int pp_nblk = 0;             // blocks of the PP force kernel (replica-aligned)
     int maxnb = 0;               // list capacity per particle
     int has_mesh = 0;

@@ -844,9 +844,14 @@ constexpr int GTILE = TILE * TILE * GTX;
 // NB field-tile buffers per CTA: with two, the copy of component c+1 is in
 // flight while component c is summed; with one, the CTA is half the size and,
 // held to 64 registers, four of them share an SM (FP32: 57 against 63 us on
-// the 20 x 64^3 ensemble). The choice is the context's gather_bufs.
-template <typename T, int NB>
-__global__ void __launch_bounds__(G_THREADS, (sizeof(T) == 4 && NB == 1) ? 4 : 1)
+// the 20 x 64^3 ensemble). The choice is the context's gather_mode.
+//
+// NC field components per CTA: 3 (a CTA per brick), or 1 (a CTA per brick and
+// component: three times the work items, each staging one tile and repeating
+// the weights, so the SMs' last wave is shorter and no CTA waits for its own
+// next copy).
+template <typename T, int NB, int NC>
+__global__ void __launch_bounds__(G_THREADS, sizeof(T) == 4 ? (NB == 1 ? 4 : 1) : 2)
 k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ brick_start,
          const int *__restrict__ brick_perm, const double *__restrict__ pos,
          const double *__restrict__ charge, const T *__restrict__ efield, long long nmesh,
@@ -861,7 +866,10 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
     __shared__ int g_base[G_THREADS];
     __shared__ int g_cnt[32];
     const int lane = threadIdx.x & 31;
-    for (int b = blockIdx.x; b < nbrick; b += gridDim.x) {
+    static_assert(NC == 3 || NC == 1, "a whole brick or one component per CTA");
+    constexpr int IPB = 3 / NC;  // work items per brick
+    for (int it = blockIdx.x; it < nbrick * IPB; it += gridDim.x) {
+        const int b = it / IPB, cfirst = (it % IPB) * NC, cend = cfirst + NC;
         const int r = find_rep(b, nrep, [&](int k) { return reps[k].brick_off; });
         const RepDev &R = reps[r];
         const int nb = R.nb, M = R.M, local = b - R.brick_off;
@@ -949,9 +957,9 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                 }
                 asm volatile("cp.async.commit_group;\n" ::: "memory");
             };
-            issue(0);
-            for (int comp = 0; comp < 3; ++comp) {
-                if (NB == 2 && comp + 1 < 3) {
+            issue(cfirst);
+            for (int comp = cfirst; comp < cend; ++comp) {
+                if (NB == 2 && comp + 1 < cend) {
                     issue(comp + 1);
                     asm volatile("cp.async.wait_group 1;\n" ::: "memory");
                 } else {
@@ -977,20 +985,26 @@ k_gather(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
                     }
                     e[comp] = acc;
                 }
-                if (NB == 1 && comp + 1 < 3) {
+                if (NB == 1 && comp + 1 < cend) {
                     __syncthreads();
                     issue(comp + 1);
-                } else if (comp + 2 < 3) {
+                } else if (comp + 2 < cend) {
                     __syncthreads();  // buffer (comp % 2) is refilled next
                 }
             }
             if (p >= 0) {
-                typename V4<T>::t out;
-                out.x = e[0];
-                out.y = e[1];
-                out.z = e[2];
-                out.w = (T)charge[brick_perm[p]];
-                acc_pm[p] = out;
+                if constexpr (NC == 3) {
+                    typename V4<T>::t out;
+                    out.x = e[0];
+                    out.y = e[1];
+                    out.z = e[2];
+                    out.w = (T)charge[brick_perm[p]];
+                    acc_pm[p] = out;
+                } else {
+                    T *o = reinterpret_cast<T *>(acc_pm + p);  // (Ex, Ey, Ez, Z)
+                    o[cfirst] = e[cfirst];
+                    if (cfirst == 0) o[3] = (T)charge[brick_perm[p]];
+                }
             }
         }
     }
@@ -1105,8 +1119,9 @@ template <typename T> void configure_mesh_kernels()
     set_smem(k_fft_y<T>, fft_smem<T>(256, 1));
     set_smem(k_fft_z_green<T>, fft_smem<T>(256, 2));
     set_smem(k_fft_x_c2r<T>, x_smem<T>(256));
-    set_smem(k_gather<T, 1>, GTILE * sizeof(T));
-    if constexpr (sizeof(T) == 4) set_smem(k_gather<T, 2>, 2 * GTILE * sizeof(T));
+    set_smem(k_gather<T, 1, 3>, GTILE * sizeof(T));
+    set_smem(k_gather<T, 1, 1>, GTILE * sizeof(T));
+    if constexpr (sizeof(T) == 4) set_smem(k_gather<T, 2, 3>, 2 * GTILE * sizeof(T));
     set_smem(k_fft_plane<T>, plane_smem<T>(PLANE_MAX));
 }
 
@@ -1162,15 +1177,19 @@ template <typename T> void launch_fft_inverse(const DevState &s, cudaStream_t st
 
 template <typename T> void launch_gather(const DevState &s, cudaStream_t st)
 {
-    const int grid = grid_items(s.nbrick, 148 * 16);
-    if (sizeof(T) == 4 && s.gather_bufs == 2)
-        k_gather<T, 2><<<grid, G_THREADS, 2 * GTILE * sizeof(T), st>>>(
+    using A = typename V4<T>::t;
+    if (sizeof(T) == 4 && s.gather_mode == 2)
+        k_gather<T, 2, 3><<<grid_items(s.nbrick, 148 * 16), G_THREADS, 2 * GTILE * sizeof(T), st>>>(
             s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (const T *)s.efield,
-            s.nmesh, (typename V4<T>::t *)s.acc_pm, s.nbrick);
+            s.nmesh, (A *)s.acc_pm, s.nbrick);
+    else if (s.gather_mode == 0)
+        k_gather<T, 1, 1><<<grid_items(3 * s.nbrick, 148 * 16), G_THREADS, GTILE * sizeof(T), st>>>(
+            s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (const T *)s.efield,
+            s.nmesh, (A *)s.acc_pm, s.nbrick);
     else
-        k_gather<T, 1><<<grid, G_THREADS, GTILE * sizeof(T), st>>>(
+        k_gather<T, 1, 3><<<grid_items(s.nbrick, 148 * 16), G_THREADS, GTILE * sizeof(T), st>>>(
             s.reps, s.nrep, s.brick_start, s.brick_perm, s.pos, s.charge, (const T *)s.efield,
-            s.nmesh, (typename V4<T>::t *)s.acc_pm, s.nbrick);
+            s.nmesh, (A *)s.acc_pm, s.nbrick);
 }
 
 void launch_reduce_pm(const DevState &s, cudaStream_t st)

@@ -44,7 +44,7 @@ class Tuning(ctypes.Structure):
         ("pp_tpi", ctypes.c_int32),
         ("cell_div", ctypes.c_int32),
         ("plane_max", ctypes.c_int32),
-        ("gather_bufs", ctypes.c_int32),
+        ("gather_mode", ctypes.c_int32),
         ("skin", ctypes.c_double),
     ]
 

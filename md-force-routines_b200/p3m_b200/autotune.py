@@ -10,8 +10,9 @@ What it searches (p3m_tuning of the C ABI):
   staged once for many particles);
 * the FFT tiles of meshes up to 64^3: the fused y/z plane kernel (a whole kx
   plane per CTA) or the y and z pencil passes (16 lines per CTA);
-* the FP32 gather: one or two field-tile buffers per CTA (copy/compute
-  overlap against CTAs per SM).
+* the force gather: a CTA per mesh brick with one or two field-tile buffers
+  (copy/compute overlap against CTAs per SM), or a CTA per brick and field
+  component (three times the work items).
 
 The last three are searched one at a time from the best PP setting
 (coordinate descent), then the fastest few settings are timed again over
@@ -54,7 +55,7 @@ def _save(d):
 
 
 def _key(t):
-    return f"tpi{t['pp_tpi']},skin{t['skin']:g},div{t['cell_div']},plane{t['plane_max']},gbuf{t['gather_bufs']}"
+    return f"tpi{t['pp_tpi']},skin{t['skin']:g},div{t['cell_div']},plane{t['plane_max']},gather{t['gather_mode']}"
 
 
 def shape_options(ctx):
@@ -62,8 +63,8 @@ def shape_options(ctx):
     opts = {"cell_div": (2, 1)}
     if any(0 < r.M <= 64 for r in ctx.replicas):
         opts["plane_max"] = (64, 0)
-    if ctx.precision == FP32 and any(r.M > 0 for r in ctx.replicas):
-        opts["gather_bufs"] = (2, 1)
+    if any(r.M > 0 for r in ctx.replicas):
+        opts["gather_mode"] = (1, 0, 2) if ctx.precision == FP32 else (1, 0)
     return opts
 
 

@@ -387,7 +387,7 @@ class Context:
         self._ck(lib().p3m_set_pp_config(self.handle, int(tpi), float(skin)))
 
     def tuning(self):
-        """{pp_tpi, cell_div, plane_max, gather_bufs, skin}: the kernel shapes."""
+        """{pp_tpi, cell_div, plane_max, gather_mode, skin}: the kernel shapes."""
         t = Tuning()
         self._ck(lib().p3m_get_tuning(self.handle, ctypes.byref(t)))
         return t.as_dict()
@@ -395,14 +395,14 @@ class Context:
     def set_tuning(self, **kw):
         """Change some of the kernel shapes (the others keep their values):
         pp_tpi (1, 2, 4, 8), cell_div (1, 2), plane_max (0, 32, 64),
-        gather_bufs (1, 2), skin."""
+        gather_mode (0, 1, 2), skin."""
         cur = self.tuning()
         unknown = set(kw) - set(cur)
         if unknown:
             raise ValueError(f"unknown tuning keys {sorted(unknown)}")
         cur.update(kw)
         t = Tuning(int(cur["pp_tpi"]), int(cur["cell_div"]), int(cur["plane_max"]),
-                   int(cur["gather_bufs"]), float(cur["skin"]))
+                   int(cur["gather_mode"]), float(cur["skin"]))
         self._ck(lib().p3m_set_tuning(self.handle, ctypes.byref(t)))
 
     def pp_config(self):

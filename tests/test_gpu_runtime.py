@@ -378,11 +378,11 @@ def test_autotune_installs_a_finalist():
     with Context([r, r], precision=FP32) as c:
         c.set_state_all(np.concatenate([pos, pos]), np.concatenate([vel, vel]))
         c.init_forces()
-        assert set(shape_options(c)) == {"cell_div", "plane_max", "gather_bufs"}
+        assert set(shape_options(c)) == {"cell_div", "plane_max", "gather_mode"}
         res = tune(c, steps=10, use_cache=False, candidates=[(1, 0.5), (2, 0.8), (4, 1.1)],
                    finalists=2)
         # 3 PP settings, then one new setting per other shape value
-        assert len(res["ms_per_step"]) == 3 + 3 and len(res["final_ms_per_step"]) == 2
+        assert len(res["ms_per_step"]) == 3 + 1 + 1 + 2 and len(res["final_ms_per_step"]) == 2
         best = min(res["final_ms_per_step"], key=res["final_ms_per_step"].get)
         assert best in res["ms_per_step"]
         assert c.tuning() == res["choice"]
@@ -392,7 +392,7 @@ def test_autotune_installs_a_finalist():
 def test_kernel_shapes_agree(prec_name):
     """Every kernel shape computes the same forces and energies: cell divisor
     1 or 2, the fused plane FFT or the pencil passes for a 32^3 and a 64^3
-    replica, one or two gather buffers -- to rounding (FP64: 1e-12; FP32:
+    replica, every gather mode -- to rounding (FP64: 1e-12; FP32:
     1e-6 of the RMS force) -- and the pencil FFT path matches the oracle."""
     from p3m_b200 import FP32, FP64, Context, Replica, gf_opt_device
 
@@ -404,7 +404,8 @@ def test_kernel_shapes_agree(prec_name):
     states = [_init_state(r, 30 + i)[0] for i, r in enumerate(reps)]
     pos = np.concatenate(states)
     out = {}
-    for shape in ({}, {"cell_div": 1}, {"plane_max": 0}, {"plane_max": 32}, {"gather_bufs": 1}):
+    for shape in ({}, {"cell_div": 1}, {"plane_max": 0}, {"plane_max": 32}, {"gather_mode": 0},
+                  {"gather_mode": 2}):
         with Context(reps, precision=prec) as c:
             c.set_tuning(**shape)
             assert all(c.tuning()[k] == v for k, v in shape.items()) or prec_name == "fp64"
