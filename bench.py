@@ -21,7 +21,8 @@ oracle port on one host core).
 
 --impl reference: the reference's CPU path for the same workload, run as the
 oracle port (the reference's own code is Python/numba that does not travel
-to the GPU box) over all host cores, one replica per process.
+to the GPU box) over all host cores, each process owning a fixed set of
+replicas that it sets up and warms up before the timed region.
 """
 import argparse
 import json
@@ -592,14 +593,20 @@ def extras(args, line, ctx, reps, states, device):
         s = torch.cuda.ExternalStream(ctxs[0].stream())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        for _ in range(n_e2e):
+        # each context's step k+1 starts from the host arrays its step k
+        # wrote back: wait for that context only (the host reads its result,
+        # then hands it in again), so while one context's copies run the
+        # others compute and no step waits for the whole ensemble
+        for k in range(n_e2e):
             for c, hb, eb in zip(ctxs, host, ebuf):
+                if k:
+                    c.sync()  # this context's previous step is in hb, eb
                 c.set_state_all(*hb, keep_lists=True, sync=False)
                 c.run(1, MODE_NVE, graph=True, sync=False)
                 c.get_step_async(*hb, eb)
-            for c in ctxs:
-                c.sync()
-        e1.record(s)  # after both contexts' work: the host synchronised on both
+        for c in ctxs:
+            c.sync()
+        e1.record(s)  # after every context's work: the host synchronised on all
         e1.synchronize()
         t = e0.elapsed_time(e1) * 1e-3
     finally:
@@ -611,7 +618,9 @@ def extras(args, line, ctx, reps, states, device):
                    "how": ("p3m_set_state_all_async (pinned host -> device, lists kept), "
                            "p3m_run(1, sync=0), p3m_get_step_async (state and energies back) "
                            f"per step on each of {len(halves)} contexts (its own streams, "
-                           "priority levels 0, 1, ...), then p3m_sync")}
+                           "priority levels 0, 1, ...); a context's next step is queued after "
+                           "p3m_sync on that context alone (its result back in the host "
+                           "arrays it hands in again)")}
 
     # -- CPU baseline: the oracle port on one host core ------------------------------
     G, _ = gf_opt_device(r0.kappa, r0.alpha, 6, 3, r0.M, r0.L, device=device)
