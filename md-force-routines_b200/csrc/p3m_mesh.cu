@@ -515,7 +515,47 @@ __device__ __forceinline__ T rho_at(const RepDev &R, const T *__restrict__ tiles
 
 // Pass A: rows of the charge mesh (reduced from the tiles) -> R2C along x,
 // written transposed into spec[kx][z][y]. Item = (replica, z, tile of
-// 2 x_lines rows); two real rows share one complex line.
+// 2 x_lines rows); two real rows share one complex line. The item body is
+// instantiated per mesh side, so its loop bounds, masks and shifts are
+// compile-time constants.
+template <typename T, int LOGM>
+__device__ __forceinline__ void x_r2c_item(const RepDev &R, int w, const T *__restrict__ tiles,
+                                           cplx<T> *__restrict__ spec, cplx<T> *buf,
+                                           const cplx<T> *tw)
+{
+    constexpr int M = 1 << LOGM;
+    constexpr int LNL = x_lines_log(LOGM), NROW = 2 << LNL;  // complex lines, real rows
+    constexpr int NYT = M >> (LNL + 1), NK = (M >> 1) + 1;
+    static_assert(FFT_THREADS % M == 0, "each thread keeps one x");
+    const int z = w / NYT, y0 = (w % NYT) * NROW;
+    const int x = threadIdx.x & (M - 1);
+    const AxisOff ax = axis_x(x, R.nb), az = axis_z(z, R.nb);
+    const T *t = tiles + R.tile_off;
+    T *dst = reinterpret_cast<T *>(&buf[brev(x, LOGM) * LSX]);
+    __syncthreads();
+    for (int j = threadIdx.x >> LOGM; j < NROW; j += FFT_THREADS >> LOGM)
+        dst[j] = rho_sum<T>(t, ax, axis_y(y0 + j, R.nb), az);  // line j/2, part j%2
+    __syncthreads();
+    fft_lines_t<T, LOGM>(buf, 1, LSX, LNL, tw, false);
+    // split the two real rows: Xa = (Z[k] + conj Z[M-k])/2, Xb = (Z[k] - conj Z[M-k])/2i
+    cplx<T> *out = spec + R.spec_off + (long long)z * M + y0;
+    for (int e = threadIdx.x; e < NROW * NK; e += FFT_THREADS) {
+        const int j = e & (NROW - 1), k = e >> (LNL + 1);
+        const int l = j >> 1;
+        const cplx<T> Z = buf[k * LSX + l];
+        const cplx<T> Zm = buf[((M - k) & (M - 1)) * LSX + l];
+        cplx<T> X;
+        if ((j & 1) == 0) {
+            X.x = (T)0.5 * (Z.x + Zm.x);
+            X.y = (T)0.5 * (Z.y - Zm.y);
+        } else {
+            X.x = (T)0.5 * (Z.y + Zm.y);
+            X.y = (T)0.5 * (Zm.x - Z.x);
+        }
+        out[(long long)k * M * M + j] = X;
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS)
 k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const T *__restrict__ tiles,
@@ -528,37 +568,12 @@ k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const T *__restrict__ til
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int r = find_rep(item, nrep, [&](int k) { return reps[k].wa_off; });
         const RepDev &R = reps[r];
-        const int M = R.M, logM = R.logM, w = item - R.wa_off;
-        const int lnl = x_lines_log(logM), nrow = 2 << lnl;  // complex lines, real rows
-        const int nyt = M >> (lnl + 1);
-        const int z = w / nyt, y0 = (w % nyt) * nrow;
-        // blockDim.x is a multiple of M: each thread keeps one x
-        const int x = threadIdx.x & (M - 1);
-        const AxisOff ax = axis_x(x, R.nb), az = axis_z(z, R.nb);
-        const T *t = tiles + R.tile_off;
-        T *dst = reinterpret_cast<T *>(&buf[brev(x, logM) * LSX]);
-        __syncthreads();
-        for (int j = threadIdx.x >> logM; j < nrow; j += blockDim.x >> logM)
-            dst[j] = rho_sum<T>(t, ax, axis_y(y0 + j, R.nb), az);  // line j/2, part j%2
-        __syncthreads();
-        fft_lines<T>(buf, logM, 1, LSX, lnl, tw, false);
-        // split the two real rows: Xa = (Z[k] + conj Z[M-k])/2, Xb = (Z[k] - conj Z[M-k])/2i
-        const int nk = (M >> 1) + 1;
-        cplx<T> *out = spec + R.spec_off;
-        for (int e = threadIdx.x; e < nrow * nk; e += blockDim.x) {
-            const int j = e & (nrow - 1), k = e >> (lnl + 1);
-            const int l = j >> 1;
-            const cplx<T> Z = buf[k * LSX + l];
-            const cplx<T> Zm = buf[((M - k) & (M - 1)) * LSX + l];
-            cplx<T> X;
-            if ((j & 1) == 0) {
-                X.x = (T)0.5 * (Z.x + Zm.x);
-                X.y = (T)0.5 * (Z.y - Zm.y);
-            } else {
-                X.x = (T)0.5 * (Z.y + Zm.y);
-                X.y = (T)0.5 * (Zm.x - Z.x);
-            }
-            out[((long long)k * M + z) * M + y0 + j] = X;
+        const int w = item - R.wa_off;
+        switch (R.logM) {  // block-uniform: one replica per item
+        case 5: x_r2c_item<T, 5>(R, w, tiles, spec, buf, tw); break;
+        case 6: x_r2c_item<T, 6>(R, w, tiles, spec, buf, tw); break;
+        case 7: x_r2c_item<T, 7>(R, w, tiles, spec, buf, tw); break;
+        default: x_r2c_item<T, 8>(R, w, tiles, spec, buf, tw); break;
         }
     }
 }
@@ -676,6 +691,85 @@ k_fft_z_green(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restri
 // load and the multiplies write bit-reversed positions.
 constexpr int PLANE_MAX = 64;
 
+template <typename T, int LOGM>
+__device__ __forceinline__ void plane_item(const RepDev &R, int kx, const cplx<T> *__restrict__ spec,
+                                           const T *__restrict__ green, cplx<T> *__restrict__ ek,
+                                           long long nspec, double *__restrict__ u_out,
+                                           cplx<T> *A, cplx<T> *B, const cplx<T> *tw,
+                                           double *red)
+{
+    constexpr int M = 1 << LOGM, LD = M + 1, MM = M * M;
+    const long long lbase = R.spec_off + (long long)kx * M * M;
+    __syncthreads();
+    for (int e = threadIdx.x; e < MM; e += FFT_THREADS) {
+        const int z = e >> LOGM, y = e & (M - 1);
+        A[brev(z, LOGM) * LD + brev(y, LOGM)] = spec[lbase + e];
+    }
+    // this thread's influence-function values, in flight during the sweeps
+    constexpr int GPT = (MM + FFT_THREADS - 1) / FFT_THREADS;
+    T gr[GPT];
+#pragma unroll
+    for (int i = 0; i < GPT; ++i) {
+        const int e = threadIdx.x + i * FFT_THREADS;
+        gr[i] = e < MM ? __ldg(green + lbase + e) : (T)0;
+    }
+    __syncthreads();
+    fft_lines_t<T, LOGM>(A, LD, 1, LOGM, tw, false);  // along y
+    fft_lines_t<T, LOGM>(A, 1, LD, LOGM, tw, false);  // along z
+    const double wkx = (kx == 0 || kx == (M >> 1)) ? 1.0 : 2.0;
+    double u = 0.0;
+#pragma unroll
+    for (int i = 0; i < GPT; ++i) {
+        const int e = threadIdx.x + i * FFT_THREADS;
+        if (e >= MM) break;
+        const int z = e >> LOGM, y = e & (M - 1);
+        const cplx<T> rk = A[z * LD + y];
+        const T g = gr[i];
+        u += wkx * (double)g * ((double)rk.x * rk.x + (double)rk.y * rk.y);
+        B[brev(z, LOGM) * LD + brev(y, LOGM)] = make_c<T>(g * rk.x, g * rk.y);
+    }
+    __syncthreads();
+    const T twopi_L = (T)(6.283185307179586477 * R.inv_L);
+    for (int e = threadIdx.x; e < MM; e += FFT_THREADS) {
+        const int zb = e >> LOGM, yb = e & (M - 1);
+        const int z = brev(zb, LOGM);
+        const T kz = (z == (M >> 1)) ? (T)0 : twopi_L * (T)freq(z, M);
+        const cplx<T> ph = B[zb * LD + yb];
+        A[zb * LD + yb] = make_c<T>(kz * ph.y, -kz * ph.x);  // -i kz phi
+    }
+    __syncthreads();
+    fft_lines_t<T, LOGM>(A, 1, LD, LOGM, tw, true);  // z, of -i kz phi
+    fft_lines_t<T, LOGM>(B, 1, LD, LOGM, tw, true);  // z, of phi: psi
+    fft_lines_t<T, LOGM>(A, LD, 1, LOGM, tw, true);  // y: E_z
+    cplx<T> *Ez = ek + 2 * nspec + lbase;
+    for (int e = threadIdx.x; e < MM; e += FFT_THREADS) {
+        const int z = e >> LOGM, y = e & (M - 1);
+        Ez[e] = A[z * LD + y];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < MM; e += FFT_THREADS) {
+        const int z = e >> LOGM, yb = e & (M - 1);
+        const int y = brev(yb, LOGM);
+        const T ky = (y == (M >> 1)) ? (T)0 : twopi_L * (T)freq(y, M);
+        const cplx<T> ps = B[z * LD + yb];
+        A[z * LD + yb] = make_c<T>(ky * ps.y, -ky * ps.x);  // -i ky psi
+    }
+    __syncthreads();
+    fft_lines_t<T, LOGM>(A, LD, 1, LOGM, tw, true);  // y: E_y
+    fft_lines_t<T, LOGM>(B, LD, 1, LOGM, tw, true);  // y: IFFT(psi)
+    const T kxv = (kx == (M >> 1)) ? (T)0 : twopi_L * (T)kx;
+    cplx<T> *Ey = ek + nspec + lbase;
+    cplx<T> *Ex = ek + lbase;
+    for (int e = threadIdx.x; e < MM; e += FFT_THREADS) {
+        const int z = e >> LOGM, y = e & (M - 1);
+        Ey[e] = A[z * LD + y];
+        const cplx<T> ps = B[z * LD + y];
+        Ex[e] = make_c<T>(kxv * ps.y, -kxv * ps.x);
+    }
+    const double ut = block_sum(u, red);
+    if (threadIdx.x == 0) *u_out = ut;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS)
 k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict__ spec,
@@ -689,80 +783,13 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int r = find_rep(item, nrep, [&](int k) { return reps[k].wp_off; });
         const RepDev &R = reps[r];
-        const int M = R.M, logM = R.logM, kx = item - R.wp_off;
-        const int LD = M + 1;
+        const int kx = item - R.wp_off;
         cplx<T> *A = tw + 128;
-        cplx<T> *B = A + M * LD;
-        const long long lbase = R.spec_off + (long long)kx * M * M;
-        const int MM = M * M;
-        __syncthreads();
-        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
-            const int z = e >> logM, y = e & (M - 1);
-            A[brev(z, logM) * LD + brev(y, logM)] = spec[lbase + e];
-        }
-        // this thread's influence-function values, in flight during the sweeps
-        constexpr int GPT = PLANE_MAX * PLANE_MAX / FFT_THREADS;
-        T gr[GPT];
-#pragma unroll
-        for (int i = 0; i < GPT; ++i) {
-            const int e = threadIdx.x + i * FFT_THREADS;
-            gr[i] = e < MM ? __ldg(green + lbase + e) : (T)0;
-        }
-        __syncthreads();
-        fft_lines<T>(A, logM, LD, 1, logM, tw, false);  // along y
-        fft_lines<T>(A, logM, 1, LD, logM, tw, false);  // along z
-        const double wkx = (kx == 0 || kx == (M >> 1)) ? 1.0 : 2.0;
-        double u = 0.0;
-#pragma unroll
-        for (int i = 0; i < GPT; ++i) {
-            const int e = threadIdx.x + i * FFT_THREADS;
-            if (e >= MM) break;
-            const int z = e >> logM, y = e & (M - 1);
-            const cplx<T> rk = A[z * LD + y];
-            const T g = gr[i];
-            u += wkx * (double)g * ((double)rk.x * rk.x + (double)rk.y * rk.y);
-            B[brev(z, logM) * LD + brev(y, logM)] = make_c<T>(g * rk.x, g * rk.y);
-        }
-        __syncthreads();
-        const T twopi_L = (T)(6.283185307179586477 * R.inv_L);
-        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
-            const int zb = e >> logM, yb = e & (M - 1);
-            const int z = brev(zb, logM);
-            const T kz = (z == (M >> 1)) ? (T)0 : twopi_L * (T)freq(z, M);
-            const cplx<T> ph = B[zb * LD + yb];
-            A[zb * LD + yb] = make_c<T>(kz * ph.y, -kz * ph.x);  // -i kz phi
-        }
-        __syncthreads();
-        fft_lines<T>(A, logM, 1, LD, logM, tw, true);  // z, of -i kz phi
-        fft_lines<T>(B, logM, 1, LD, logM, tw, true);  // z, of phi: psi
-        fft_lines<T>(A, logM, LD, 1, logM, tw, true);  // y: E_z
-        cplx<T> *Ez = ek + 2 * nspec + lbase;
-        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
-            const int z = e >> logM, y = e & (M - 1);
-            Ez[e] = A[z * LD + y];
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
-            const int z = e >> logM, yb = e & (M - 1);
-            const int y = brev(yb, logM);
-            const T ky = (y == (M >> 1)) ? (T)0 : twopi_L * (T)freq(y, M);
-            const cplx<T> ps = B[z * LD + yb];
-            A[z * LD + yb] = make_c<T>(ky * ps.y, -ky * ps.x);  // -i ky psi
-        }
-        __syncthreads();
-        fft_lines<T>(A, logM, LD, 1, logM, tw, true);  // y: E_y
-        fft_lines<T>(B, logM, LD, 1, logM, tw, true);  // y: IFFT(psi)
-        const T kxv = (kx == (M >> 1)) ? (T)0 : twopi_L * (T)kx;
-        cplx<T> *Ey = ek + nspec + lbase;
-        cplx<T> *Ex = ek + lbase;
-        for (int e = threadIdx.x; e < MM; e += blockDim.x) {
-            const int z = e >> logM, y = e & (M - 1);
-            Ey[e] = A[z * LD + y];
-            const cplx<T> ps = B[z * LD + y];
-            Ex[e] = make_c<T>(kxv * ps.y, -kxv * ps.x);
-        }
-        const double ut = block_sum(u, red);
-        if (threadIdx.x == 0) u_part[item] = ut;
+        cplx<T> *B = A + R.M * (R.M + 1);
+        if (R.logM == 5)
+            plane_item<T, 5>(R, kx, spec, green, ek, nspec, u_part + item, A, B, tw, red);
+        else
+            plane_item<T, 6>(R, kx, spec, green, ek, nspec, u_part + item, A, B, tw, red);
     }
 }
 
@@ -770,6 +797,48 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
 // efield[c][z][y][x]. Item = (replica, component, z, tile of 2 x_lines rows); rows
 // 2l and 2l+1 share complex line l: Z[k] = Xa[k] + i Xb[k] over the
 // Hermitian extension, with the imaginary parts at k = 0 and M/2 dropped.
+// Instantiated per mesh side like pass A.
+template <typename T, int LOGM>
+__device__ __forceinline__ void x_c2r_item(const RepDev &R, int comp, int w,
+                                           const cplx<T> *__restrict__ ek, long long nspec,
+                                           T *__restrict__ efield, long long nmesh, cplx<T> *buf,
+                                           const cplx<T> *tw)
+{
+    constexpr int M = 1 << LOGM;
+    constexpr int LNL = x_lines_log(LOGM), NROW = 2 << LNL;  // complex lines, real rows
+    constexpr int NYT = M >> (LNL + 1), NK = (M >> 1) + 1;
+    const int z = w / NYT, y0 = (w % NYT) * NROW;
+    const cplx<T> *src = ek + comp * nspec + R.spec_off + (long long)z * M + y0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < (NK << LNL); e += FFT_THREADS) {
+        const int l = e & ((1 << LNL) - 1), k = e >> LNL;
+        const long long o = (long long)k * M * M + 2 * l;
+        cplx<T> a, b;  // o is even: one 16-byte load in FP32
+        if constexpr (sizeof(T) == 4) {
+            const float4 ab = __ldg(reinterpret_cast<const float4 *>(src + o));
+            a = make_c<T>(ab.x, ab.y);
+            b = make_c<T>(ab.z, ab.w);
+        } else {
+            a = src[o];
+            b = src[o + 1];
+        }
+        if (k == 0 || k == (M >> 1)) {
+            buf[brev(k, LOGM) * LSX + l] = make_c<T>(a.x, b.x);
+        } else {
+            buf[brev(k, LOGM) * LSX + l] = make_c<T>(a.x - b.y, a.y + b.x);
+            buf[brev(M - k, LOGM) * LSX + l] = make_c<T>(a.x + b.y, b.x - a.y);
+        }
+    }
+    __syncthreads();
+    fft_lines_t<T, LOGM>(buf, 1, LSX, LNL, tw, true);
+    T *dst = efield + comp * nmesh + R.mesh_off + ((long long)z * M + y0) * M;
+    for (int e = threadIdx.x; e < NROW * M; e += FFT_THREADS) {
+        const int x = e & (M - 1), j = e >> LOGM;
+        const cplx<T> v = buf[x * LSX + (j >> 1)];
+        dst[j * M + x] = (j & 1) ? v.y : v.x;
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS)
 k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict__ ek,
@@ -784,39 +853,12 @@ k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
         const int comp = item / nitems_per_comp, it = item % nitems_per_comp;
         const int r = find_rep(it, nrep, [&](int k) { return reps[k].wa_off; });
         const RepDev &R = reps[r];
-        const int M = R.M, logM = R.logM, w = it - R.wa_off;
-        const int lnl = x_lines_log(logM), nrow = 2 << lnl;  // complex lines, real rows
-        const int nyt = M >> (lnl + 1);
-        const int z = w / nyt, y0 = (w % nyt) * nrow;
-        const cplx<T> *src = ek + comp * nspec + R.spec_off;
-        const int nk = (M >> 1) + 1;
-        __syncthreads();
-        for (int e = threadIdx.x; e < (nk << lnl); e += blockDim.x) {
-            const int l = e & ((1 << lnl) - 1), k = e >> lnl;
-            const long long o = ((long long)k * M + z) * M + y0 + 2 * l;
-            cplx<T> a, b;  // o is even: one 16-byte load in FP32
-            if constexpr (sizeof(T) == 4) {
-                const float4 ab = __ldg(reinterpret_cast<const float4 *>(src + o));
-                a = make_c<T>(ab.x, ab.y);
-                b = make_c<T>(ab.z, ab.w);
-            } else {
-                a = src[o];
-                b = src[o + 1];
-            }
-            if (k == 0 || k == (M >> 1)) {
-                buf[brev(k, logM) * LSX + l] = make_c<T>(a.x, b.x);
-            } else {
-                buf[brev(k, logM) * LSX + l] = make_c<T>(a.x - b.y, a.y + b.x);
-                buf[brev(M - k, logM) * LSX + l] = make_c<T>(a.x + b.y, b.x - a.y);
-            }
-        }
-        __syncthreads();
-        fft_lines<T>(buf, logM, 1, LSX, lnl, tw, true);
-        T *dst = efield + comp * nmesh + R.mesh_off + ((long long)z * M + y0) * M;
-        for (int e = threadIdx.x; e < nrow * M; e += blockDim.x) {
-            const int x = e & (M - 1), j = e >> logM;
-            const cplx<T> v = buf[x * LSX + (j >> 1)];
-            dst[(long long)j * M + x] = (j & 1) ? v.y : v.x;
+        const int w = it - R.wa_off;
+        switch (R.logM) {  // block-uniform: one replica per item
+        case 5: x_c2r_item<T, 5>(R, comp, w, ek, nspec, efield, nmesh, buf, tw); break;
+        case 6: x_c2r_item<T, 6>(R, comp, w, ek, nspec, efield, nmesh, buf, tw); break;
+        case 7: x_c2r_item<T, 7>(R, comp, w, ek, nspec, efield, nmesh, buf, tw); break;
+        default: x_c2r_item<T, 8>(R, comp, w, ek, nspec, efield, nmesh, buf, tw); break;
         }
     }
 }
