@@ -172,31 +172,6 @@ __device__ __forceinline__ void fft_lines_t(cplx<T> *buf, int ls, int es, int lo
     }
 }
 
-template <typename T>
-__device__ __forceinline__ void fft_lines(cplx<T> *buf, int logM, int ls, int es, int lognl,
-                                          const cplx<T> *tw, bool inverse)
-{
-    switch (logM) {  // the mesh sides a context accepts: 32 .. 256
-    case 5: fft_lines_t<T, 5>(buf, ls, es, lognl, tw, inverse); break;
-    case 6: fft_lines_t<T, 6>(buf, ls, es, lognl, tw, inverse); break;
-    case 7: fft_lines_t<T, 7>(buf, ls, es, lognl, tw, inverse); break;
-    case 8: fft_lines_t<T, 8>(buf, ls, es, lognl, tw, inverse); break;
-    default: {
-        int s = 0;
-        for (; s + 3 <= logM; s += 3) fft_group_pass<T, 3>(buf, logM, ls, es, lognl, tw, inverse, s);
-        if (logM - s == 2) fft_group_pass<T, 2>(buf, logM, ls, es, lognl, tw, inverse, s);
-        else if (logM - s == 1) fft_group_pass<T, 1>(buf, logM, ls, es, lognl, tw, inverse, s);
-    }
-    }
-}
-
-// PENCIL lines, element n of line l at buf[n * LS + l]
-template <typename T>
-__device__ __forceinline__ void fft_pencil(cplx<T> *buf, int logM, const cplx<T> *tw, bool inverse)
-{
-    fft_lines<T>(buf, logM, 1, LS, LOG_PENCIL, tw, inverse);
-}
-
 // ---------------------------------------------------------------------------
 // Charge assignment
 // ---------------------------------------------------------------------------
@@ -557,7 +532,7 @@ __device__ __forceinline__ void x_r2c_item(const RepDev &R, int w, const T *__re
 }
 
 template <typename T>
-__global__ void __launch_bounds__(FFT_THREADS)
+__global__ void __launch_bounds__(FFT_THREADS, sizeof(T) == 4 ? 4 : 1)
 k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const T *__restrict__ tiles,
             cplx<T> *__restrict__ spec, const cplx<T> *__restrict__ twg, int nitems)
 {
@@ -580,7 +555,30 @@ k_fft_x_r2c(const RepDev *__restrict__ reps, int nrep, const T *__restrict__ til
 
 // Passes B / D: FFT along y of contiguous lines spec[kx][z][:]. Item =
 // (replica, [component,] kx, 16-line z tile). `ncomp` arrays of `stride`
-// elements are processed (1 forward, 3 inverse).
+// elements are processed (1 forward, 3 inverse). The item body is
+// instantiated per mesh side.
+template <typename T, int LOGM>
+__device__ __forceinline__ void y_item(const RepDev &R, int w, cplx<T> *__restrict__ data,
+                                       long long off, cplx<T> *buf, const cplx<T> *tw,
+                                       bool inverse)
+{
+    constexpr int M = 1 << LOGM, NZT = M / PENCIL;
+    const int kx = w / NZT, z0 = (w % NZT) * PENCIL;
+    cplx<T> *base = data + off + R.spec_off + ((long long)kx * M + z0) * M;
+    __syncthreads();
+    for (int e = threadIdx.x; e < PENCIL * M; e += FFT_THREADS) {
+        const int y = e & (M - 1), l = e >> LOGM;
+        buf[brev(y, LOGM) * LS + l] = base[l * M + y];
+    }
+    __syncthreads();
+    if (inverse) fft_lines_t<T, LOGM>(buf, 1, LS, LOG_PENCIL, tw, true);
+    else fft_lines_t<T, LOGM>(buf, 1, LS, LOG_PENCIL, tw, false);
+    for (int e = threadIdx.x; e < PENCIL * M; e += FFT_THREADS) {
+        const int y = e & (M - 1), l = e >> LOGM;
+        base[l * M + y] = buf[y * LS + l];
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS)
 k_fft_y(const RepDev *__restrict__ reps, int nrep, cplx<T> *__restrict__ data, long long stride,
@@ -594,20 +592,13 @@ k_fft_y(const RepDev *__restrict__ reps, int nrep, cplx<T> *__restrict__ data, l
         const int comp = item / nitems_per_comp, it = item % nitems_per_comp;
         const int r = find_rep(it, nrep, [&](int k) { return reps[k].wb_off; });
         const RepDev &R = reps[r];
-        const int M = R.M, logM = R.logM, w = it - R.wb_off;
-        const int nzt = M / PENCIL;
-        const int kx = w / nzt, z0 = (w % nzt) * PENCIL;
-        cplx<T> *base = data + comp * stride + R.spec_off + ((long long)kx * M + z0) * M;
-        __syncthreads();
-        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
-            const int y = e & (M - 1), l = e >> logM;
-            buf[brev(y, logM) * LS + l] = base[(long long)l * M + y];
-        }
-        __syncthreads();
-        fft_pencil<T>(buf, logM, tw, inverse);
-        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
-            const int y = e & (M - 1), l = e >> logM;
-            base[(long long)l * M + y] = buf[y * LS + l];
+        const int w = it - R.wb_off;
+        const long long off = comp * stride;
+        switch (R.logM) {  // block-uniform: one replica per item
+        case 5: y_item<T, 5>(R, w, data, off, buf, tw, inverse); break;
+        case 6: y_item<T, 6>(R, w, data, off, buf, tw, inverse); break;
+        case 7: y_item<T, 7>(R, w, data, off, buf, tw, inverse); break;
+        default: y_item<T, 8>(R, w, data, off, buf, tw, inverse); break;
         }
     }
 }
@@ -616,7 +607,63 @@ k_fft_y(const RepDev *__restrict__ reps, int nrep, cplx<T> *__restrict__ data, l
 // field spectra with their inverse z transforms. E_z = IFFT_z(-i kz phi);
 // E_x and E_y use psi = IFFT_z(phi) since their multipliers are constant
 // along z: E_x = -i kx psi, E_y = -i ky psi. Item = (replica, kx, 16-wide y
-// tile).
+// tile); the item body is instantiated per mesh side.
+template <typename T, int LOGM>
+__device__ __forceinline__ void z_green_item(const RepDev &R, int w,
+                                             const cplx<T> *__restrict__ spec,
+                                             const T *__restrict__ green,
+                                             cplx<T> *__restrict__ ek, long long nspec,
+                                             double *__restrict__ u_out, cplx<T> *buf,
+                                             const cplx<T> *tw, double *red)
+{
+    constexpr int M = 1 << LOGM, NYT = M / PENCIL;
+    cplx<T> *buf2 = buf + M * LS;
+    const int kx = w / NYT, y0 = (w % NYT) * PENCIL;
+    const long long lbase = R.spec_off + (long long)kx * M * M + y0;  // + z*M + l
+    __syncthreads();
+    for (int e = threadIdx.x; e < PENCIL * M; e += FFT_THREADS) {
+        const int l = e & (PENCIL - 1), z = e >> LOG_PENCIL;
+        buf[brev(z, LOGM) * LS + l] = spec[lbase + z * M + l];
+    }
+    __syncthreads();
+    fft_lines_t<T, LOGM>(buf, 1, LS, LOG_PENCIL, tw, false);
+    const double wkx = (kx == 0 || kx == (M >> 1)) ? 1.0 : 2.0;
+    double u = 0.0;
+    for (int e = threadIdx.x; e < PENCIL * M; e += FFT_THREADS) {
+        const int l = e & (PENCIL - 1), n = e >> LOG_PENCIL;
+        const cplx<T> rk = buf[n * LS + l];
+        const T g = green[lbase + n * M + l];
+        u += wkx * (double)g * ((double)rk.x * rk.x + (double)rk.y * rk.y);
+        buf2[brev(n, LOGM) * LS + l] = make_c<T>(g * rk.x, g * rk.y);
+    }
+    __syncthreads();
+    const T twopi_L = (T)(6.283185307179586477 * R.inv_L);
+    for (int e = threadIdx.x; e < PENCIL * M; e += FFT_THREADS) {
+        const int l = e & (PENCIL - 1), n = e >> LOG_PENCIL;
+        const int br = brev(n, LOGM);
+        const cplx<T> ph = buf2[br * LS + l];
+        const T kz = (n == (M >> 1)) ? (T)0 : twopi_L * (T)freq(n, M);
+        // -i kz phi = (kz phi.y, -kz phi.x)
+        buf[br * LS + l] = make_c<T>(kz * ph.y, -kz * ph.x);
+    }
+    __syncthreads();
+    fft_lines_t<T, LOGM>(buf, 1, LS, LOG_PENCIL, tw, true);   // E_z
+    fft_lines_t<T, LOGM>(buf2, 1, LS, LOG_PENCIL, tw, true);  // psi
+    const T kxv = (kx == (M >> 1)) ? (T)0 : twopi_L * (T)kx;
+    for (int e = threadIdx.x; e < PENCIL * M; e += FFT_THREADS) {
+        const int l = e & (PENCIL - 1), z = e >> LOG_PENCIL;
+        const int yy = y0 + l;
+        const T kyv = (yy == (M >> 1)) ? (T)0 : twopi_L * (T)freq(yy, M);
+        const cplx<T> ps = buf2[z * LS + l];
+        const long long o = lbase + z * M + l;
+        ek[o] = make_c<T>(kxv * ps.y, -kxv * ps.x);
+        ek[nspec + o] = make_c<T>(kyv * ps.y, -kyv * ps.x);
+        ek[2 * nspec + o] = buf[z * LS + l];
+    }
+    const double ut = block_sum(u, red);
+    if (threadIdx.x == 0) *u_out = ut;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(FFT_THREADS)
 k_fft_z_green(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict__ spec,
@@ -630,54 +677,15 @@ k_fft_z_green(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restri
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int r = find_rep(item, nrep, [&](int k) { return reps[k].wc_off; });
         const RepDev &R = reps[r];
-        const int M = R.M, logM = R.logM, w = item - R.wc_off;
+        const int w = item - R.wc_off;
         cplx<T> *buf = tw + 128;
-        cplx<T> *buf2 = buf + M * LS;
-        const int nyt = M / PENCIL;
-        const int kx = w / nyt, y0 = (w % nyt) * PENCIL;
-        const long long lbase = R.spec_off + (long long)kx * M * M + y0;  // + z*M + l
-        __syncthreads();
-        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
-            const int l = e & (PENCIL - 1), z = e >> 4;
-            buf[brev(z, logM) * LS + l] = spec[lbase + (long long)z * M + l];
+        double *u_out = u_part + item;
+        switch (R.logM) {  // block-uniform: one replica per item
+        case 5: z_green_item<T, 5>(R, w, spec, green, ek, nspec, u_out, buf, tw, red); break;
+        case 6: z_green_item<T, 6>(R, w, spec, green, ek, nspec, u_out, buf, tw, red); break;
+        case 7: z_green_item<T, 7>(R, w, spec, green, ek, nspec, u_out, buf, tw, red); break;
+        default: z_green_item<T, 8>(R, w, spec, green, ek, nspec, u_out, buf, tw, red); break;
         }
-        __syncthreads();
-        fft_pencil<T>(buf, logM, tw, false);
-        const double wkx = (kx == 0 || kx == (M >> 1)) ? 1.0 : 2.0;
-        double u = 0.0;
-        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
-            const int l = e & (PENCIL - 1), n = e >> 4;
-            const cplx<T> rk = buf[n * LS + l];
-            const T g = green[lbase + (long long)n * M + l];
-            u += wkx * (double)g * ((double)rk.x * rk.x + (double)rk.y * rk.y);
-            buf2[brev(n, logM) * LS + l] = make_c<T>(g * rk.x, g * rk.y);
-        }
-        __syncthreads();
-        const T twopi_L = (T)(6.283185307179586477 * R.inv_L);
-        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
-            const int l = e & (PENCIL - 1), n = e >> 4;
-            const int br = brev(n, logM);
-            const cplx<T> ph = buf2[br * LS + l];
-            const T kz = (n == (M >> 1)) ? (T)0 : twopi_L * (T)freq(n, M);
-            // -i kz phi = (kz phi.y, -kz phi.x)
-            buf[br * LS + l] = make_c<T>(kz * ph.y, -kz * ph.x);
-        }
-        __syncthreads();
-        fft_pencil<T>(buf, logM, tw, true);   // E_z
-        fft_pencil<T>(buf2, logM, tw, true);  // psi
-        const T kxv = (kx == (M >> 1)) ? (T)0 : twopi_L * (T)kx;
-        for (int e = threadIdx.x; e < PENCIL * M; e += blockDim.x) {
-            const int l = e & (PENCIL - 1), z = e >> 4;
-            const int yy = y0 + l;
-            const T kyv = (yy == (M >> 1)) ? (T)0 : twopi_L * (T)freq(yy, M);
-            const cplx<T> ps = buf2[z * LS + l];
-            const long long o = lbase + (long long)z * M + l;
-            ek[o] = make_c<T>(kxv * ps.y, -kxv * ps.x);
-            ek[nspec + o] = make_c<T>(kyv * ps.y, -kyv * ps.x);
-            ek[2 * nspec + o] = buf[z * LS + l];
-        }
-        const double ut = block_sum(u, red);
-        if (threadIdx.x == 0) u_part[item] = ut;
     }
 }
 
