@@ -1479,19 +1479,28 @@ extern "C" int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t)
         for (auto &g : row)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     DevState &s = ctx->s;
+    // the new plan replaces the old one only once its list storage exists
+    const DevState saved = s;
+    const std::vector<RepDev> saved_rh = ctx->rh;
     s.cell_div = t->cell_div;
     s.plane_max = t->plane_max;
     s.gather_mode = (ctx->prec == P3M_FP64 && t->gather_mode == 2) ? 1 : t->gather_mode;
-    ctx->skin_override = t->skin < 0.0 ? -1.0 : t->skin;
     plan_lists(ctx, t->skin, tpi);
     plan_mesh_passes(ctx);
     const long long need = (long long)((s.ntot + 31) / 32) * 32 * s.maxnb;
     if (need > ctx->nlist_cap) {
+        int *fresh = nullptr;
+        const cudaError_t e = dalloc(&fresh, (size_t)need);
+        if (e != cudaSuccess) {
+            s = saved;
+            ctx->rh = saved_rh;
+            return fail(ctx, P3M_ECUDA, "p3m_set_tuning: list storage", cudaGetErrorString(e));
+        }
         cudaFree(s.nlist);
-        s.nlist = nullptr;
-        CK(dalloc(&s.nlist, (size_t)need));
+        s.nlist = fresh;
         ctx->nlist_cap = need;
     }
+    ctx->skin_override = t->skin < 0.0 ? -1.0 : t->skin;
     CK(cudaMemcpy(s.reps, ctx->rh.data(), sizeof(RepDev) * ctx->nrep, cudaMemcpyHostToDevice));
     launch_set_flags(s.rebuild, s.nrep, 1, ctx->st);
     return finish(ctx);
