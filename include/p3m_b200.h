@@ -301,7 +301,7 @@ int p3m_set_priority(p3m_ctx *ctx, int level);
  * raised by that work. */
 int p3m_sync(p3m_ctx *ctx);
 
-/* PP configuration: threads per particle in the force kernel (1, 2, 4, 8; 32 on FP32)
+/* PP configuration: threads per particle in the force kernel (1, 2, 4, 8)
  * and the Verlet-list skin for every replica (< 0: each replica's own /
  * default). p3m_create picks tpi from the particle count; the autotuner of
  * the Python package times candidates and installs the fastest. Forces a
@@ -318,8 +318,7 @@ int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, double *skin, int *maxnb);
  * order of additions (pair order in the lists, lanes per particle, FFT
  * passes), so results agree to rounding. */
 typedef struct {
-    int32_t pp_tpi;       /* threads per particle in the pair kernel: 1, 2, 4 or 8, or
-                             32 (FP32: a warp per particle over contiguous lists)      */
+    int32_t pp_tpi;       /* threads per particle in the pair kernel: 1, 2, 4 or 8       */
     int32_t cell_div;     /* list cells are >= (rc + skin)/cell_div wide: 1 or 2          */
     int32_t plane_max;    /* meshes with sides up to this (0, 32 or 64) take the fused
                              y/z plane FFT kernel, larger ones the y and z pencil passes */

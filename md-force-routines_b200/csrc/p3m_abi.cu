@@ -1462,9 +1462,8 @@ extern "C" int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t)
 {
     if (!ctx || !t) return fail(ctx, P3M_EARG, "p3m_set_tuning", "NULL argument");
     const int tpi = t->pp_tpi;
-    if (!(tpi == 1 || tpi == 2 || tpi == 4 || tpi == 8 || (tpi == PP_WARP_TPI && ctx->prec == P3M_FP32)))
-        return fail(ctx, P3M_EARG, "p3m_set_tuning",
-                    "pp_tpi must be 1, 2, 4 or 8 (or 32 on the FP32 path: a warp per particle)");
+    if (!(tpi == 1 || tpi == 2 || tpi == 4 || tpi == 8))
+        return fail(ctx, P3M_EARG, "p3m_set_tuning", "pp_tpi must be 1, 2, 4 or 8");
     if (t->cell_div != 1 && t->cell_div != 2)
         return fail(ctx, P3M_EARG, "p3m_set_tuning", "cell_div must be 1 or 2");
     if (t->plane_max != 0 && t->plane_max != 32 && t->plane_max != plane_max_mesh())

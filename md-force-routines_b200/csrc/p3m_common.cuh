@@ -48,9 +48,6 @@ constexpr int PP_TABLE_N = P3M_PP_TABLE_N;  // FP32 pair table: cubic intervals 
 // this many entries (a padded entry has r = 0 and adds nothing), so the FP32
 // pair loop reads whole blocks of entries without a bounds test.
 constexpr int PP_LIST_PAD = 16;
-// pp_tpi value of the FP32 pair kernel that gives each particle a whole warp
-// (contiguous lists instead of warp-interleaved ones)
-constexpr int PP_WARP_TPI = 32;
 
 // Per-replica constants. Offsets index the concatenated device arrays.
 struct RepDev {

@@ -88,14 +88,11 @@ __device__ __forceinline__ typename Coord<T>::I qdiff(typename Coord<T>::U a, ty
     return (typename Coord<T>::I)(a - b);
 }
 
-// Index of list entry k of sorted particle s. Interleaved (the pair kernels
-// with a few threads per particle): by warps of 32 consecutive particles, so
-// a warp's k-th entries are contiguous. Contiguous (the warp-per-particle
-// kernel): a particle's entries one after another, so a warp reads 32
-// consecutive entries of one list.
-__device__ __forceinline__ long long list_index(int s, int k, int maxnb, bool contig = false)
+// Index of list entry k of sorted particle s: lists are interleaved by warps
+// of 32 consecutive particles so a warp's k-th entries are contiguous.
+__device__ __forceinline__ long long list_index(int s, int k, int maxnb)
 {
-    return contig ? (long long)s * maxnb + k : ((long long)(s >> 5) * maxnb + k) * 32 + (s & 31);
+    return ((long long)(s >> 5) * maxnb + k) * 32 + (s & 31);
 }
 
 // ---------------------------------------------------------------------------
@@ -123,7 +120,7 @@ __global__ void __launch_bounds__(LB_THREADS)
 k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
               const typename Coord<T>::Q *__restrict__ xq, int *__restrict__ nnb,
               int *__restrict__ nlist, int maxnb, const int *__restrict__ rb_list, int nrep_all,
-              int *status, int contig)
+              int *status)
 {
     using Q = typename Coord<T>::Q;
     constexpr int SCAP = lb_scap<T>();
@@ -224,7 +221,7 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                                              ((1u << LB_TPI) - 1u);
                         if (in) {
                             const int pos = cnt + __popc(grp & below);
-                            if (pos < maxnb) nlist[list_index(s, pos, maxnb, contig)] = j;
+                            if (pos < maxnb) nlist[list_index(s, pos, maxnb)] = j;
                         }
                         cnt += __popc(grp);
                     }
@@ -244,7 +241,7 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                 // multiple of PP_LIST_PAD, so the pad stays in the list
                 const int pe = nn + sub;
                 if (pe < ((nn + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1)))
-                    nlist[list_index(s, pe, maxnb, contig)] = s;
+                    nlist[list_index(s, pe, maxnb)] = s;
             }
         }
     }
@@ -523,80 +520,6 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
     if (threadIdx.x == 0) u_part[b] = ut;
 }
 
-// FP32 forces, one warp per particle (pp_tpi = PP_WARP_TPI): the 32 lanes
-// read 32 consecutive entries of one contiguous list -- neighbours in
-// stencil-cell order, so most of them are runs of consecutive sorted
-// particles and their coordinates share sectors -- two entries per lane per
-// round (pairs as in k_pp_f32), Kahan-compensated per lane, then summed over
-// the warp by a butterfly. Each warp takes PP_WARP_PPW particles in turn.
-constexpr int PP_WARP_PPW = 16;
-constexpr int PP_WARP_PPB = (PPL_THREADS / 32) * PP_WARP_PPW;  // particles per block
-
-__global__ void __launch_bounds__(PPL_THREADS)
-k_pp_f32_warp(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq,
-              const int *__restrict__ nnb, const int *__restrict__ nlist, int maxnb,
-              const float4 *__restrict__ tables, float4 *__restrict__ acc_out,
-              double *__restrict__ u_part)
-{
-    constexpr bool P = P3M_PP_PACK != 0;
-    __shared__ double red[32];
-    extern __shared__ __align__(16) float4 ppl_tab[];
-    const int b = blockIdx.x;
-    const int r = find_rep(b, nrep, [&](int k) { return reps[k].pp_blk_off; });
-    const RepDev &R = reps[r];
-    {
-        const float4 *src = tables + (long long)r * PP_TABLE_N;
-        for (int k = threadIdx.x; k < PP_TABLE_N * PP_TABLE_COPIES; k += PPL_THREADS)
-            cp_async16(ppl_tab + k, src + k / PP_TABLE_COPIES);
-        cp_async_wait_all();
-        __syncthreads();
-    }
-    const float4 *tab = ppl_tab + (threadIdx.x & (PP_TABLE_COPIES - 1));
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const double scd = R.L / 4294967296.0;
-    const float sch = (float)scd;
-    const float2 sc = f2(sch, sch), sc_lo = f2((float)(scd - (double)sch), (float)(scd - (double)sch));
-    const float rc2 = (float)(R.rc * R.rc);
-    const float ih = (float)(PP_TABLE_N / R.rc);
-    const float2 inv_h = f2(ih, ih);
-    double u = 0.0;
-    const int first = R.p_off + (b - R.pp_blk_off) * PP_WARP_PPB + warp * PP_WARP_PPW;
-    const int end = R.p_off + R.n;
-    for (int p = 0; p < PP_WARP_PPW; ++p) {
-        const int s = first + p;
-        if (s >= end) break;  // warp-uniform
-        const uint4 xi = xq[s];
-        const int nr = (nnb[s] + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1);
-        const int *lp = nlist + list_index(s, 0, maxnb, true);
-        float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-        for (int k0 = 0; k0 < nr; k0 += 64) {
-            const int ka = k0 + lane, kb = k0 + 32 + lane;
-            const int ja = ka < nr ? __ldg(lp + ka) : s;
-            const int jb = kb < nr ? __ldg(lp + kb) : s;
-            const uint4 qa = xq[ja], qb = xq[jb];
-            float2 px = f2(0.f, 0.f), py = px, pz = px, pu = px;
-            pair_table2<P>(xi, qa, qb, sc, sc_lo, rc2, inv_h, tab, px, py, pz, pu);
-            const float sx = px.x + px.y, sy = py.x + py.y, sz = pz.x + pz.y;
-            float y = sx - gx, t = fx + y; gx = (t - fx) - y; fx = t;
-            y = sy - gy; t = fy + y; gy = (t - fy) - y; fy = t;
-            y = sz - gz; t = fz + y; gz = (t - fz) - y; fz = t;
-            u += (double)(pu.x + pu.y);
-        }
-        fx -= gx;
-        fy -= gy;
-        fz -= gz;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            fx += __shfl_xor_sync(0xffffffffu, fx, o);
-            fy += __shfl_xor_sync(0xffffffffu, fy, o);
-            fz += __shfl_xor_sync(0xffffffffu, fz, o);
-        }
-        if (lane == 0) acc_out[s] = make_float4(fx, fy, fz, 0.f);
-    }
-    const double ut = block_sum(u, red);
-    if (threadIdx.x == 0) u_part[b] = ut;
-}
-
 // Per-replica U_pp = 1/2 sum of the replica's block partials (index order).
 __global__ void k_reduce_pp(const RepDev *__restrict__ reps, int nrep,
                             const double *__restrict__ u_part, int nblk_total,
@@ -619,7 +542,7 @@ __global__ void k_reduce_pp(const RepDev *__restrict__ reps, int nrep,
 // ---------------------------------------------------------------------------
 static int qgrid(int n) { int g = (n + 255) / 256; return g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g); }
 
-int pp_particles_per_block(int tpi) { return tpi == PP_WARP_TPI ? PP_WARP_PPB : PPL_THREADS / tpi; }
+int pp_particles_per_block(int tpi) { return PPL_THREADS / tpi; }
 
 template <typename T> void configure_pp_kernels()
 {
@@ -634,7 +557,6 @@ template <typename T> void configure_pp_kernels()
         cudaFuncSetAttribute(k_pp_f32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
         cudaFuncSetAttribute(k_pp_f32<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
         cudaFuncSetAttribute(k_pp_f32<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
-        cudaFuncSetAttribute(k_pp_f32_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
     }
 }
 
@@ -651,7 +573,7 @@ template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st
     auto kern = s.cell_div == 1 ? k_build_lists<T, 1> : k_build_lists<T, 2>;
     kern<<<grid, LB_THREADS, lb_scap<T>() * sizeof(Q), st>>>(
         s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.rb_list, s.nrep,
-        s.status, s.pp_tpi == PP_WARP_TPI ? 1 : 0);
+        s.status);
 }
 
 template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cudaStream_t st)
@@ -670,14 +592,6 @@ template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cuda
 
 template <typename T> void launch_pp(const DevState &s, cudaStream_t st)
 {
-    if constexpr (sizeof(T) == 4) {
-        if (s.pp_tpi == PP_WARP_TPI) {
-            k_pp_f32_warp<<<s.pp_nblk, PPL_THREADS, PP_TABLE_N * PP_TABLE_COPIES * sizeof(float4),
-                            st>>>(s.reps, s.nrep, (const uint4 *)s.xq, s.nnb, s.nlist, s.maxnb,
-                                  s.pp_tables, (float4 *)s.acc_pp, s.u_pp_part);
-            return;
-        }
-    }
     switch (s.pp_tpi) {
     case 2: launch_pp_tpi<T, 2>(s, st); break;
     case 4: launch_pp_tpi<T, 4>(s, st); break;

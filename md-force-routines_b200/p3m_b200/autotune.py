@@ -2,10 +2,9 @@
 
 What it searches (p3m_tuning of the C ABI):
 
-* the PP stage: threads per particle in the pair kernel (1, 2 or 4, or on
-  the FP32 path a whole warp per particle) and the Verlet-list skin (larger
-  skins rebuild less often but visit more list entries) -- a grid of both,
-  since they interact;
+* the PP stage: threads per particle in the pair kernel and the Verlet-list
+  skin (larger skins rebuild less often but visit more list entries) -- a
+  grid of both, since they interact;
 * the list cells: (rc + skin)/2 or (rc + skin) wide (cell_div 2 or 1: a
   125-cell stencil of small cells, or 27 larger cells whose candidates are
   staged once for many particles);
@@ -30,8 +29,6 @@ import os
 from ._lib import FP32, MODE_NVE
 
 CANDIDATES = [(tpi, skin) for tpi in (1, 2, 4) for skin in (0.5, 0.8, 1.1, 1.4)]
-#: FP32 only: a warp per particle over contiguous lists
-WARP_CANDIDATES = [(32, skin) for skin in (0.5, 0.8, 1.1)]
 CACHE = os.environ.get("P3M_B200_TUNE_CACHE",
                        os.path.join(os.path.expanduser("~"), ".cache", "p3m_b200", "autotune.json"))
 
@@ -107,8 +104,7 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
             settings[k] = dict(t)
         return times[k]
 
-    cands = candidates or (CANDIDATES + (WARP_CANDIDATES if ctx.precision == FP32 else []))
-    for tpi, skin in cands:
+    for tpi, skin in (candidates or CANDIDATES):
         if skin <= max_skin:
             trial(dict(base, pp_tpi=tpi, skin=skin))
     best = dict(settings[min(times, key=times.get)])

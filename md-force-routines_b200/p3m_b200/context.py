@@ -394,7 +394,7 @@ class Context:
 
     def set_tuning(self, **kw):
         """Change some of the kernel shapes (the others keep their values):
-        pp_tpi (1, 2, 4, 8; 32 on FP32), cell_div (1, 2), plane_max (0, 32, 64),
+        pp_tpi (1, 2, 4, 8), cell_div (1, 2), plane_max (0, 32, 64),
         gather_mode (0, 1, 2), skin."""
         cur = self.tuning()
         unknown = set(kw) - set(cur)

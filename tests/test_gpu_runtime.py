@@ -392,7 +392,7 @@ def test_autotune_installs_a_finalist():
 def test_kernel_shapes_agree(prec_name):
     """Every kernel shape computes the same forces and energies: cell divisor
     1 or 2, the fused plane FFT or the pencil passes for a 32^3 and a 64^3
-    replica, every gather mode, the warp-per-particle pair kernel -- to rounding (FP64: 1e-12; FP32:
+    replica, every gather mode -- to rounding (FP64: 1e-12; FP32:
     1e-6 of the RMS force) -- and the pencil FFT path matches the oracle."""
     from p3m_b200 import FP32, FP64, Context, Replica, gf_opt_device
 
@@ -404,11 +404,8 @@ def test_kernel_shapes_agree(prec_name):
     states = [_init_state(r, 30 + i)[0] for i, r in enumerate(reps)]
     pos = np.concatenate(states)
     out = {}
-    shapes = [{}, {"cell_div": 1}, {"plane_max": 0}, {"plane_max": 32}, {"gather_mode": 0},
-              {"gather_mode": 2}]
-    if prec_name == "fp32":
-        shapes += [{"pp_tpi": 32}, {"pp_tpi": 32, "cell_div": 1}]  # a warp per particle
-    for shape in shapes:
+    for shape in ({}, {"cell_div": 1}, {"plane_max": 0}, {"plane_max": 32}, {"gather_mode": 0},
+                  {"gather_mode": 2}):
         with Context(reps, precision=prec) as c:
             c.set_tuning(**shape)
             assert all(c.tuning()[k] == v for k, v in shape.items()) or prec_name == "fp64"
