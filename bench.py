@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="skip the kernel-shape autotuner")
     ap.add_argument("--pp-config", default=None, metavar="TPI,SKIN",
                     help="set threads per particle and Verlet skin instead of autotuning")
+    ap.add_argument("--prune-buf", type=float, default=0.0,
+                    help="with --pp-config: FP32 inner-list buffer beyond rc (0: none)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the FP64, e2e, roofline and CPU-baseline legs")
     return ap.parse_args()
@@ -406,13 +408,14 @@ def run_ours(args):
     tuned = None
     if args.pp_config:
         tpi, skin = args.pp_config.split(",")
-        ctx.set_pp_config(int(tpi), float(skin))
+        ctx.set_tuning(pp_tpi=int(tpi), skin=float(skin), prune_buf=args.prune_buf)
     elif not args.no_tune:
         from p3m_b200.autotune import tune
 
         tuned = tune(ctx, use_cache=False)
     ctx.run(max(args.warmup, 3), MODE_NVE, record_nqt=True, graph=True)
     rb0 = sum(ctx.replica_stats(i)["rebuilds"] for i in range(len(reps)))
+    ib0 = sum(ctx.inner_builds(i) for i in range(len(reps)))
 
     def barrier():
         if world > 1:
@@ -435,6 +438,7 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     launches = ctx.launch_count() - n0
     rebuilds = sum(ctx.replica_stats(i)["rebuilds"] for i in range(len(reps))) - rb0
+    inner_builds = sum(ctx.inner_builds(i) for i in range(len(reps))) - ib0
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
@@ -457,6 +461,7 @@ def run_ours(args):
                                              ctx.pp_config())),
                        "tuning": ctx.tuning(),
                        "list_rebuilds_per_replica_step": rebuilds / (len(reps) * args.steps),
+                       "inner_list_builds_per_replica_step": inner_builds / (len(reps) * args.steps),
                        "autotune_ms_per_step": tuned["ms_per_step"] if tuned else None,
                        "autotune_final_ms_per_step": tuned.get("final_ms_per_step") if tuned else None},
             "gpu_launches": launches, "clocks": clocks}

@@ -312,11 +312,12 @@ int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, double *skin, int *maxnb);
 /* Kernel shapes of a context (no counterpart in the reference, whose PP and
  * PM stages have no GPU path): what the autotuner of the Python package
  * searches. p3m_create picks pp_tpi from the particle count, cell_div 2,
- * plane_max 64 and gather_mode 1. Setting waits
+ * plane_max 64, gather_mode 1 and prune_buf 0. Setting waits
  * for the context's work, drops its captured step graphs and forces a list
  * rebuild. Every setting computes the same sums; they differ only in the
  * order of additions (pair order in the lists, lanes per particle, FFT
- * passes), so results agree to rounding. */
+ * passes, entries beyond rc left out of the inner lists), so results agree
+ * to rounding. */
 typedef struct {
     int32_t pp_tpi;       /* threads per particle in the pair kernel: 1, 2, 4 or 8       */
     int32_t cell_div;     /* list cells are >= (rc + skin)/cell_div wide: 1 or 2          */
@@ -327,9 +328,18 @@ typedef struct {
                              with two buffers (FP32; FP64 takes 1 for 2)              */
     double skin;          /* Verlet skin for every replica (< 0: each replica's own /
                              the default); get returns the last value set              */
+    double prune_buf;     /* FP32 path: 0 = the pair kernel reads the Verlet lists
+                             (rc + skin); > 0 (below every skin) = it reads inner lists,
+                             the Verlet-list entries closer than rc + prune_buf, which
+                             it rebuilds itself whenever a particle of the replica has
+                             moved prune_buf/2 since their last build (dynamic pruning)  */
 } p3m_tuning;
 int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t);
 int p3m_get_tuning(p3m_ctx *ctx, p3m_tuning *t);
+
+/* Number of inner-list builds of one replica that came without a Verlet-list
+ * rebuild (steps with prune_buf > 0), as a double. */
+int p3m_get_inner_builds(p3m_ctx *ctx, int replica, double *out);
 
 /* Measurement: average device time (ms) of each step stage over `iters`
  * back-to-back launches, timed with CUDA events on the context's stream.

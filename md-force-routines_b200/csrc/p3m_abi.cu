@@ -56,6 +56,7 @@ struct p3m_ctx {
     long long graph_kernels[2][2] = {{0, 0}, {0, 0}};  // kernels each graph launches
     int ncell_cap = 0;            // cells allocated (grid with skin 0)
     long long nlist_cap = 0;      // list entries allocated
+    long long nlist_in_cap = 0;   // inner-list entries allocated
     int pp_nblk_cap = 0;          // PP blocks allocated (tpi = 8)
     long long launches = 0;
     std::string err;
@@ -194,7 +195,7 @@ static void plan_lists(p3m_ctx *ctx, double skin_override, int tpi)
 {
     DevState &s = ctx->s;
     int cell = 0, blk = 0;
-    double maxmean = 0.0;
+    double maxmean = 0.0, maxmean_in = 0.0;
     const int ppb = pp_particles_per_block(tpi);
     for (int r = 0; r < ctx->nrep; ++r) {
         const p3m_replica_desc &d = ctx->desc[r];
@@ -213,14 +214,22 @@ static void plan_lists(p3m_ctx *ctx, double skin_override, int tpi)
         cell += R.nc * R.nc * R.nc;
         R.pp_blk_off = blk;
         blk += (d.n + ppb - 1) / ppb;
-        const double mean = 4.0 / 3.0 * M_PI * d.n / (d.box * d.box * d.box) * R.rcl * R.rcl * R.rcl;
+        const double dens = 4.0 / 3.0 * M_PI * d.n / (d.box * d.box * d.box);
+        const double mean = dens * R.rcl * R.rcl * R.rcl;
         if (mean > maxmean) maxmean = mean;
+        R.pbuf = s.prune_buf;
+        const double rin = d.rc + R.pbuf;
+        if (dens * rin * rin * rin > maxmean_in) maxmean_in = dens * rin * rin * rin;
     }
     s.ncell = cell;
     s.pp_tpi = tpi;
     s.pp_nblk = blk;
     // a multiple of PP_LIST_PAD: the builder pads every list to one
     s.maxnb = ((int)ceil(1.5 * maxmean + 64.0) + PP_LIST_PAD - 1) / PP_LIST_PAD * PP_LIST_PAD;
+    s.maxnb_in = s.prune_buf > 0.0
+                     ? ((int)ceil(1.5 * maxmean_in + 64.0) + PP_LIST_PAD - 1) / PP_LIST_PAD * PP_LIST_PAD
+                     : 0;
+    if (s.maxnb_in > s.maxnb) s.maxnb_in = s.maxnb;  // a subset of the outer list
 }
 
 extern "C" int p3m_version(void) { return P3M_VERSION; }
@@ -244,6 +253,7 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
                     s.cell_start, s.cell_cursor, s.cell_tmp, s.cell_perm, s.cell_slot, s.xq, s.nnb,
                     s.cell_sub,
                     s.nlist, s.rebuild, s.rb_list, s.pos_ref, s.pp_tables,
+                    s.nnb_in, s.nlist_in, s.prune, s.pos_pref, s.prune_count,
                     s.acc_pp, s.brick_key, s.brick_count, s.brick_start, s.brick_cursor,
                     s.brick_perm, s.brick_slot, s.brick_hist, s.tiles, s.spec, s.ek, s.green, s.efield,
                     s.acc_pm, s.twiddle, s.u_pp_part, s.u_pm_part, s.kin_part, s.rep_out,
@@ -482,6 +492,10 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(dalloc(&s.rebuild, (size_t)n_reps));
     CKC(dalloc(&s.rb_list, (size_t)2 * n_reps + 2));
     CKC(dalloc(&s.pos_ref, (size_t)3 * p));
+    CKC(dalloc(&s.prune, (size_t)n_reps));
+    CKC(dalloc(&s.nnb_in, (size_t)p));
+    CKC(dalloc(&s.pos_pref, (size_t)3 * p));
+    CKC(dalloc(&s.prune_count, (size_t)n_reps));
     CKC(dalloc(&s.cell_tmp, (size_t)p));
     CKC(dalloc(&s.cell_perm, (size_t)p));
     CKC(dalloc(&s.cell_slot, (size_t)p));
@@ -561,7 +575,7 @@ template <typename T> static void seq_pp(p3m_ctx *ctx, bool reduce = true, cudaS
 {
     if (!st) st = ctx->st;
     launch_pp<T>(ctx->s, st);
-    ctx->launches++;
+    ctx->launches += pp_kernel_count(ctx->s);
     if (reduce) {
         launch_reduce_pp(ctx->s, st);
         ctx->launches++;
@@ -1473,6 +1487,10 @@ extern "C" int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t)
     for (int r = 0; r < ctx->nrep; ++r)
         if (t->skin > 0.5 * ctx->desc[r].rc)
             return fail(ctx, P3M_EARG, "p3m_set_tuning", "skin must be <= rc/2 (negative: default)");
+    if (!(t->prune_buf >= 0.0 && t->prune_buf <= 1e3))
+        return fail(ctx, P3M_EARG, "p3m_set_tuning", "prune_buf must be >= 0");
+    if (t->prune_buf > 0.0 && ctx->prec != P3M_FP32)
+        return fail(ctx, P3M_EARG, "p3m_set_tuning", "inner lists (prune_buf > 0) are an FP32-path option");
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->st));
     for (auto &row : ctx->graph)
@@ -1485,24 +1503,42 @@ extern "C" int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t)
     s.cell_div = t->cell_div;
     s.plane_max = t->plane_max;
     s.gather_mode = (ctx->prec == P3M_FP64 && t->gather_mode == 2) ? 1 : t->gather_mode;
+    s.prune_buf = t->prune_buf;
     plan_lists(ctx, t->skin, tpi);
     plan_mesh_passes(ctx);
-    const long long need = (long long)((s.ntot + 31) / 32) * 32 * s.maxnb;
-    if (need > ctx->nlist_cap) {
-        int *fresh = nullptr;
-        const cudaError_t e = dalloc(&fresh, (size_t)need);
-        if (e != cudaSuccess) {
+    for (int r = 0; r < ctx->nrep; ++r)
+        if (s.prune_buf > 0.0 && s.prune_buf >= ctx->rh[r].skin) {
             s = saved;
             ctx->rh = saved_rh;
-            return fail(ctx, P3M_ECUDA, "p3m_set_tuning: list storage", cudaGetErrorString(e));
+            return fail(ctx, P3M_EARG, "p3m_set_tuning", "prune_buf must be below every replica's skin");
         }
+    // list storage: the outer lists, then the inner ones (both keep their
+    // old storage when it is large enough)
+    const long long need = (long long)((s.ntot + 31) / 32) * 32 * s.maxnb;
+    const long long need_in = (long long)((s.ntot + 31) / 32) * 32 * s.maxnb_in;
+    int *fresh = nullptr, *fresh_in = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (need > ctx->nlist_cap) e = dalloc(&fresh, (size_t)need);
+    if (e == cudaSuccess && need_in > ctx->nlist_in_cap) e = dalloc(&fresh_in, (size_t)need_in);
+    if (e != cudaSuccess) {
+        cudaFree(fresh);
+        s = saved;
+        ctx->rh = saved_rh;
+        return fail(ctx, P3M_ECUDA, "p3m_set_tuning: list storage", cudaGetErrorString(e));
+    }
+    if (fresh) {
         cudaFree(s.nlist);
         s.nlist = fresh;
         ctx->nlist_cap = need;
     }
+    if (fresh_in) {
+        cudaFree(s.nlist_in);
+        s.nlist_in = fresh_in;
+        ctx->nlist_in_cap = need_in;
+    }
     ctx->skin_override = t->skin < 0.0 ? -1.0 : t->skin;
     CK(cudaMemcpy(s.reps, ctx->rh.data(), sizeof(RepDev) * ctx->nrep, cudaMemcpyHostToDevice));
-    launch_set_flags(s.rebuild, s.nrep, 1, ctx->st);
+    launch_set_flags(s.rebuild, s.nrep, 1, ctx->st);  // the next force evaluation builds both lists
     return finish(ctx);
 }
 
@@ -1514,6 +1550,17 @@ extern "C" int p3m_get_tuning(p3m_ctx *ctx, p3m_tuning *t)
     t->plane_max = ctx->s.plane_max;
     t->gather_mode = ctx->s.gather_mode;
     t->skin = ctx->skin_override;
+    t->prune_buf = ctx->s.prune_buf;
+    return P3M_OK;
+}
+
+extern "C" int p3m_get_inner_builds(p3m_ctx *ctx, int replica, double *out)
+{
+    if (!ctx || !out) return fail(ctx, P3M_EARG, "p3m_get_inner_builds", "NULL argument");
+    if (replica < 0 || replica >= ctx->nrep) return fail(ctx, P3M_EARG, "p3m_get_inner_builds", "replica");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaMemcpy(out, ctx->s.prune_count + replica, sizeof(double), cudaMemcpyDeviceToHost));
     return P3M_OK;
 }
 
@@ -1542,10 +1589,12 @@ extern "C" int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, double *skin, int *maxn
 
 // Each stage is idempotent when repeated (the inverse FFT works in place on
 // the field spectra, so it is timed together with the forward pass that
-// rebuilds them: fft_inverse = fft_both - fft_forward).
+// rebuilds them: fft_inverse = fft_both - fft_forward). With inner lists,
+// "pp" is the pair kernel of a step without list work (inner lists) and
+// "pp_prune" that of a step where every replica builds its inner lists.
 static const char *kStageNames[] = {"drift_sort", "keys_sort", "pp", "assign", "fft_forward",
-                                    "fft_both", "gather", "finish", "nqt", "step"};
-static const int kNumStages = 10;
+                                    "fft_both", "gather", "finish", "nqt", "step", "pp_prune"};
+static const int kNumStages = 11;
 
 extern "C" const char *p3m_stage_name(int i)
 {
@@ -1577,6 +1626,11 @@ template <typename T> static void enqueue_stage(p3m_ctx *ctx, int k)
         launch_kick_finish<T>(s, 0, nullptr, ctx->st);
         launch_step_reduce(s, 2, ctx->counters, nullptr, 0, ctx->st);
         ctx->launches += 2;
+        break;
+    case 10:
+        launch_set_flags(s.rebuild, s.nrep, 1, ctx->st);
+        seq_pp<T>(ctx);
+        ctx->launches++;
         break;
     case 8:
         if (ctx->nq > 0) {
@@ -1625,6 +1679,12 @@ template <typename T> static int do_profile(p3m_ctx *ctx, int iters, double *ms,
             CK(cudaEventRecord(e1, ctx->st));
         } else {
             enqueue_stage<T>(ctx, k);
+            if (k == 2 && s.prune_buf > 0.0) {
+                // that launch built the inner lists: time the steps that read them
+                launch_set_flags(s.rebuild, s.nrep, 0, ctx->st);
+                launch_set_flags(s.prune, s.nrep, 0, ctx->st);
+                ctx->launches += 2;
+            }
             CK(cudaEventRecord(e0, ctx->st));
             for (int i = 0; i < iters; ++i) enqueue_stage<T>(ctx, k);
             CK(cudaEventRecord(e1, ctx->st));

@@ -70,6 +70,8 @@ struct RepDev {
     long long sh_off;      // offset into the brick-sort count table (chunks x nb^3)
     double L, kappa, alpha, rc, cellw, h, dt, t_desired, af, uf, kf;
     double skin, rcl;      // Verlet skin and list cutoff rc + skin
+    double pbuf;           // inner-list buffer: the pair kernel reads the outer-list entries
+                           // closer than rc + pbuf (0: it reads the outer list itself)
     double qmax;           // largest |charge| of the replica
     double inv_cellw, inv_h, inv_L, inv_V;
 };

@@ -36,13 +36,14 @@ __global__ void k_kick_drift(const RepDev *__restrict__ reps, const int *__restr
                              double *__restrict__ pos, double *__restrict__ vel,
                              const double *__restrict__ acc, const double *__restrict__ pos_ref,
                              int ntot, int *__restrict__ brick_key, int *__restrict__ brick_count,
-                             int has_mesh, int *rebuild, int *status)
+                             int has_mesh, int *rebuild, int *status,
+                             const double *__restrict__ pos_pref, int *prune)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
         const int r = prep[i];
         const RepDev &R = reps[r];
         double x[3];
-        double d2 = 0.0;
+        double d2 = 0.0, d2p = 0.0;
         bool vfin = true;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -55,11 +56,17 @@ __global__ void k_kick_drift(const RepDev *__restrict__ reps, const int *__restr
             double dd = x[d] - pos_ref[3 * i + d];
             dd -= R.L * rint(dd * R.inv_L);
             d2 += dd * dd;
+            if (pos_pref) {  // and since the last inner-list build
+                double dp = x[d] - pos_pref[3 * i + d];
+                dp -= R.L * rint(dp * R.inv_L);
+                d2p += dp * dp;
+            }
         }
         // a non-finite velocity (or acceleration) is reported as such; the
         // position it makes is also flagged by particle_keys below
         if (!vfin) raise_status(status, ST_NONFINITE);
         if (d2 > 0.25 * R.skin * R.skin && !rebuild[r]) atomicOr(rebuild + r, 1);
+        if (pos_pref && d2p > 0.25 * R.pbuf * R.pbuf && !prune[r]) atomicOr(prune + r, 1);
         int b;
         particle_keys(R, x[0], x[1], x[2], has_mesh, nullptr, &b, status);
         if (b >= 0) {
@@ -132,7 +139,8 @@ __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nbl
                               const double *__restrict__ kin_part, double *__restrict__ rep_out,
                               int mode, int *__restrict__ counters, double *__restrict__ ring,
                               int ring_cap, int recorded, int snap_interval, int snap_cap,
-                              int *rebuild, int *status, StepSums sums)
+                              int *rebuild, int *status, StepSums sums, int *prune,
+                              double *prune_count)
 {
     // counters: [0] steps since the run started, [1] energy-ring position,
     // [2] step index of the run's first step (thermostat_p3m_ord6.py:15 tests
@@ -213,6 +221,10 @@ __global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nbl
     // this step's lists are built (count them); the next drift decides again
     for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
         if (rebuild[r] && mode != 2) rep_out[8 * r + RO_REBUILDS] += 1.0;
+        if (prune) {  // inner lists: count the builds that came without an outer rebuild
+            if (prune[r] && !rebuild[r] && mode != 2) prune_count[r] += 1.0;
+            prune[r] = 0;
+        }
         rebuild[r] = 0;
     }
 }
@@ -547,9 +559,11 @@ static int pgrid(int n) { int g = (n + 255) / 256; return g < 1 ? 1 : (g > 148 *
 
 void launch_kick_drift(const DevState &s, cudaStream_t st)
 {
+    const bool inner = s.prune_buf > 0.0;
     k_kick_drift<<<pgrid(s.ntot), 256, 0, st>>>(s.reps, s.prep, s.pos, s.vel, s.acc, s.pos_ref,
                                                 s.ntot, s.brick_key, s.brick_count, s.has_mesh,
-                                                s.rebuild, s.status);
+                                                s.rebuild, s.status, inner ? s.pos_pref : nullptr,
+                                                s.prune);
 }
 
 void launch_set_flags(int *flag, int n, int value, cudaStream_t st)
@@ -573,7 +587,8 @@ void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring
 {
     k_step_reduce<<<1, 1024, 0, st>>>(s.reps, s.nrep, s.nblk, s.kin_part, s.rep_out, mode,
                                       counters, ring, ring_cap, recorded, snap_interval, snap_cap,
-                                      s.rebuild, s.status, sums);
+                                      s.rebuild, s.status, sums,
+                                      s.prune_buf > 0.0 ? s.prune : nullptr, s.prune_count);
 }
 
 void launch_snapshot(const DevState &s, const int *counters, double *snap, int *steps,

@@ -24,6 +24,8 @@ struct DevState {
                                  // brick with one / two tile buffers (2: FP32 only)
     int pp_nblk = 0;             // blocks of the PP force kernel (replica-aligned)
     int maxnb = 0;               // list capacity per particle
+    double prune_buf = 0.0;      // inner-list buffer beyond rc (FP32; 0: no inner lists)
+    int maxnb_in = 0;            // inner-list capacity per particle
     int has_mesh = 0;
     int max_mesh = 0;            // largest M over replicas
     int nblk = 0;                // replica-aligned particle blocks (PBLK each)
@@ -44,6 +46,13 @@ struct DevState {
     // [1 .. k] replica indices, [nrep + 1 + j] = cells of the first j of them
     int *rb_list = nullptr;
     double *pos_ref = nullptr;   // positions at the last rebuild (ntot,3)
+    // inner lists (prune_buf > 0): the outer entries closer than rc + prune_buf,
+    // in outer-list order and the same layout, rebuilt by the pair kernel on the
+    // steps a replica's flag is set
+    int *nnb_in = nullptr, *nlist_in = nullptr;
+    int *prune = nullptr;        // per-replica flags: rebuild the inner lists this step
+    double *pos_pref = nullptr;  // positions at the last inner-list build (ntot,3)
+    double *prune_count = nullptr;  // per replica: inner-list builds between outer rebuilds
     float4 *pp_tables = nullptr; // FP32 pair tables: cubic of psi = phi r, [nrep][PP_TABLE_N]
     void *acc_pp = nullptr;      // V4<T> PP acceleration, cell-sorted order
     // brick sort
@@ -83,6 +92,7 @@ template <typename T> void launch_quantize(const DevState &s, cudaStream_t st);
 template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st);
 template <typename T> void launch_pp(const DevState &s, cudaStream_t st);
 int pp_particles_per_block(int tpi);
+int pp_kernel_count(const DevState &s);  // 2 with inner lists (prune and inner launches)
 void launch_reduce_pp(const DevState &s, cudaStream_t st);
 
 template <typename T> void launch_assign(const DevState &s, cudaStream_t st);

@@ -405,11 +405,14 @@ template <bool P> __device__ __forceinline__ float2 v_add(float2 a, float2 b)
 // interval i = round(t - 1/2) and float(i) come from the 1.5 * 2^23 rounding
 // constant (exact for t < 2^22, no float <-> int conversions), and the force
 // from the same cubic: g = F r^2 = psi - t dpsi/du, F/r = g / r^3, phi = psi / r.
-template <bool P>
+// With KEEP, bits 0 / 1 of `keep` are set for a / b closer than sqrt(rin2)
+// (self entries included; the caller masks them by index).
+template <bool P, bool KEEP = false>
 __device__ __forceinline__ void pair_table2(const uint4 &xi, const uint4 &qa, const uint4 &qb,
                                             float2 sc, float2 sc_lo, float rc2, float2 inv_h,
                                             const float4 *__restrict__ tab, float2 &px,
-                                            float2 &py, float2 &pz, float2 &pu)
+                                            float2 &py, float2 &pz, float2 &pu,
+                                            float rin2 = 0.f, unsigned *keep = nullptr)
 {
     constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: round-to-integer constant
     const float2 ix = f2((float)(int)(xi.x - qa.x), (float)(int)(xi.x - qb.x));
@@ -419,6 +422,7 @@ __device__ __forceinline__ void pair_table2(const uint4 &xi, const uint4 &qa, co
     const float2 dy = v_fma<P>(iy, sc_lo, v_mul<P>(iy, sc));
     const float2 dz = v_fma<P>(iz, sc_lo, v_mul<P>(iz, sc));
     const float2 r2 = v_fma<P>(dz, dz, v_fma<P>(dy, dy, v_mul<P>(dx, dx)));
+    if constexpr (KEEP) *keep = (r2.x < rin2 ? 1u : 0u) | (r2.y < rin2 ? 2u : 0u);
     // r = 0 (the particle itself: list padding) would make r = 0 * inf: take
     // rc^2 there (a valid table interval) and mask the result; beyond rc the
     // last interval's cubic is extrapolated, finite, and masked as well
@@ -448,22 +452,48 @@ __device__ __forceinline__ void pair_table2(const uint4 &xi, const uint4 &qa, co
 #define P3M_PP_MINB 3
 #endif
 
-template <int TPI>
+// List modes of the FP32 pair kernel. Without inner lists (prune buffer 0)
+// it reads the outer lists (PP_OUTER). With them a step launches it twice:
+// PP_PRUNE for the replicas whose flag (outer rebuild or inner prune) is set
+// -- the outer lists, writing each particle's inner list on the way: the
+// entries closer than rc + pbuf, in outer-list order, padded like the outer
+// ones, and the positions they were taken at -- and PP_INNER for the others,
+// which reads the inner lists. The two touch disjoint replicas and blocks.
+enum PpMode { PP_OUTER = 0, PP_INNER = 1, PP_PRUNE = 2 };
+
+struct PruneArgs {
+    const int *rebuild = nullptr, *prune = nullptr;  // per-replica flags
+    int *nnb_in = nullptr, *nlist_in = nullptr;      // inner lists (written by PP_PRUNE)
+    int maxnb_in = 0;
+    const int *cell_perm = nullptr;                  // sorted -> original particle
+    const double *pos = nullptr;
+    double *pos_pref = nullptr;                      // positions of the inner-list build
+    int *status = nullptr;
+};
+
+template <int TPI, int PM>
 __global__ void __launch_bounds__(PPL_THREADS, P3M_PP_MINB)
 k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq,
          const int *__restrict__ nnb, const int *__restrict__ nlist, int maxnb,
          const float4 *__restrict__ tables, float4 *__restrict__ acc_out,
-         double *__restrict__ u_part)
+         double *__restrict__ u_part, PruneArgs pa)
 {
     constexpr bool P = P3M_PP_PACK != 0;
+    constexpr bool PRUNE = PM == PP_PRUNE;
     constexpr int PPB = PPL_THREADS / TPI;               // particles per block
     constexpr int UNR = PP_LIST_PAD / TPI < 8 ? PP_LIST_PAD / TPI : 8;  // entries per lane per pass
     constexpr int STEP = UNR * TPI;                       // entries of a particle per pass
     static_assert(UNR % 2 == 0 && PP_LIST_PAD % STEP == 0, "whole pairs, whole pad blocks");
+    static_assert(STEP <= 32, "a pass's keep bits fit one word");
     __shared__ double red[32];
     extern __shared__ __align__(16) float4 ppl_tab[];
     const int b = blockIdx.x;
     const int r = find_rep(b, nrep, [&](int k) { return reps[k].pp_blk_off; });
+    if constexpr (PM != PP_OUTER) {
+        // block-uniform: this block's replica belongs to the other launch
+        const bool flagged = (pa.rebuild[r] | pa.prune[r]) != 0;
+        if (flagged != PRUNE) return;
+    }
     const RepDev &R = reps[r];
     {
         const float4 *src = tables + (long long)r * PP_TABLE_N;
@@ -484,6 +514,8 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
     const float rc2 = (float)(R.rc * R.rc);
     const float ih = (float)(PP_TABLE_N / R.rc);
     const float2 inv_h = f2(ih, ih);
+    const float rin2 = PRUNE ? (float)((R.rc + R.pbuf) * (R.rc + R.pbuf)) : 0.f;
+    const int gbase = (threadIdx.x & 31) & ~(TPI - 1);   // first lane of this particle's group
 
     float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     double u = 0.0;
@@ -491,6 +523,7 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
         const uint4 xi = xq[s];
         const int nr = (nnb[s] + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1);
         const int *lp = nlist + list_index(s, sub, maxnb);
+        int cin = 0;  // PP_PRUNE: inner entries so far
         for (int k0 = 0; k0 < nr; k0 += STEP, lp += STEP * 32) {
             int j[UNR];
 #pragma unroll
@@ -499,14 +532,59 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
 #pragma unroll
             for (int v = 0; v < UNR; ++v) q[v] = xq[j[v]];
             float2 px = f2(0.f, 0.f), py = px, pz = px, pu = px;
+            unsigned keep = 0;  // PP_PRUNE: bit v = entry v of this lane goes to the inner list
 #pragma unroll
-            for (int v = 0; v < UNR; v += 2)
-                pair_table2<P>(xi, q[v], q[v + 1], sc, sc_lo, rc2, inv_h, tab, px, py, pz, pu);
+            for (int v = 0; v < UNR; v += 2) {
+                unsigned k2 = 0;
+                pair_table2<P, PRUNE>(xi, q[v], q[v + 1], sc, sc_lo, rc2, inv_h, tab, px, py, pz,
+                                      pu, rin2, &k2);
+                if constexpr (PRUNE) keep |= k2 << v;
+            }
             const float sx = px.x + px.y, sy = py.x + py.y, sz = pz.x + pz.y;
             float y = sx - gx, t = fx + y; gx = (t - fx) - y; fx = t;
             y = sy - gy; t = fy + y; gy = (t - fy) - y; fy = t;
             y = sz - gz; t = fz + y; gz = (t - fz) - y; fz = t;
             u += (double)(pu.x + pu.y);
+            if constexpr (PRUNE) {
+#pragma unroll
+                for (int v = 0; v < UNR; ++v)
+                    if (j[v] == s) keep &= ~(1u << v);  // list padding
+                // entry v of lane `sub` is entry v * TPI + sub of the pass:
+                // the group's keep bits in entry order give each its place
+                unsigned mask = 0;
+                if constexpr (TPI == 1) {
+                    mask = keep;
+                } else {
+                    const unsigned gm = ((1u << TPI) - 1u) << gbase;
+#pragma unroll
+                    for (int v = 0; v < UNR; ++v) {
+                        const unsigned bal = __ballot_sync(gm, (keep >> v) & 1u);
+                        mask |= ((bal >> gbase) & ((1u << TPI) - 1u)) << (v * TPI);
+                    }
+                }
+#pragma unroll
+                for (int v = 0; v < UNR; ++v)
+                    if ((keep >> v) & 1u) {
+                        const int e = v * TPI + sub;
+                        const int pos = cin + __popc(mask & ((1u << e) - 1u));
+                        if (pos < pa.maxnb_in) pa.nlist_in[list_index(s, pos, pa.maxnb_in)] = j[v];
+                    }
+                cin += __popc(mask);
+            }
+        }
+        if constexpr (PRUNE) {
+            const int nn = min(cin, pa.maxnb_in);
+            if (sub == 0) {
+                if (cin > pa.maxnb_in) raise_status(pa.status, ST_NBOVF);
+                pa.nnb_in[s] = nn;
+                const int o = pa.cell_perm[s];
+                pa.pos_pref[3 * o + 0] = pa.pos[3 * o + 0];
+                pa.pos_pref[3 * o + 1] = pa.pos[3 * o + 1];
+                pa.pos_pref[3 * o + 2] = pa.pos[3 * o + 2];
+            }
+            // pad like the outer lists (maxnb_in is a multiple of PP_LIST_PAD)
+            const int pend = (nn + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1);
+            for (int e = nn + sub; e < pend; e += TPI) pa.nlist_in[list_index(s, e, pa.maxnb_in)] = s;
         }
     }
 #pragma unroll
@@ -553,10 +631,13 @@ template <typename T> void configure_pp_kernels()
                          (int)(lb_scap<T>() * sizeof(Q)));
     if constexpr (sizeof(T) == 4) {
         const int tab = (int)(PP_TABLE_N * PP_TABLE_COPIES * sizeof(float4));
-        cudaFuncSetAttribute(k_pp_f32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
-        cudaFuncSetAttribute(k_pp_f32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
-        cudaFuncSetAttribute(k_pp_f32<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
-        cudaFuncSetAttribute(k_pp_f32<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, tab);
+        auto set = [&](auto k) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tab); };
+        set(k_pp_f32<1, PP_OUTER>); set(k_pp_f32<2, PP_OUTER>);
+        set(k_pp_f32<4, PP_OUTER>); set(k_pp_f32<8, PP_OUTER>);
+        set(k_pp_f32<1, PP_INNER>); set(k_pp_f32<2, PP_INNER>);
+        set(k_pp_f32<4, PP_INNER>); set(k_pp_f32<8, PP_INNER>);
+        set(k_pp_f32<1, PP_PRUNE>); set(k_pp_f32<2, PP_PRUNE>);
+        set(k_pp_f32<4, PP_PRUNE>); set(k_pp_f32<8, PP_PRUNE>);
     }
 }
 
@@ -580,9 +661,29 @@ template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cuda
 {
     using Q = typename Coord<T>::Q;
     if constexpr (sizeof(T) == 4) {
-        k_pp_f32<TPI><<<s.pp_nblk, PPL_THREADS, PP_TABLE_N * PP_TABLE_COPIES * sizeof(float4), st>>>(
+        const size_t tab = PP_TABLE_N * PP_TABLE_COPIES * sizeof(float4);
+        PruneArgs pa;
+        if (s.prune_buf <= 0.0) {
+            k_pp_f32<TPI, PP_OUTER><<<s.pp_nblk, PPL_THREADS, tab, st>>>(
+                s.reps, s.nrep, (const uint4 *)s.xq, s.nnb, s.nlist, s.maxnb, s.pp_tables,
+                (float4 *)s.acc_pp, s.u_pp_part, pa);
+            return;
+        }
+        pa.rebuild = s.rebuild;
+        pa.prune = s.prune;
+        pa.nnb_in = s.nnb_in;
+        pa.nlist_in = s.nlist_in;
+        pa.maxnb_in = s.maxnb_in;
+        pa.cell_perm = s.cell_perm;
+        pa.pos = s.pos;
+        pa.pos_pref = s.pos_pref;
+        pa.status = s.status;
+        k_pp_f32<TPI, PP_PRUNE><<<s.pp_nblk, PPL_THREADS, tab, st>>>(
             s.reps, s.nrep, (const uint4 *)s.xq, s.nnb, s.nlist, s.maxnb, s.pp_tables,
-            (float4 *)s.acc_pp, s.u_pp_part);
+            (float4 *)s.acc_pp, s.u_pp_part, pa);
+        k_pp_f32<TPI, PP_INNER><<<s.pp_nblk, PPL_THREADS, tab, st>>>(
+            s.reps, s.nrep, (const uint4 *)s.xq, s.nnb_in, s.nlist_in, s.maxnb_in, s.pp_tables,
+            (float4 *)s.acc_pp, s.u_pp_part, pa);
     } else {
         k_pp_f64<TPI><<<s.pp_nblk, PPL_THREADS, 0, st>>>(s.reps, s.nrep, (const Q *)s.xq, s.nnb,
                                                          s.nlist, s.maxnb, (double4 *)s.acc_pp,
@@ -599,6 +700,8 @@ template <typename T> void launch_pp(const DevState &s, cudaStream_t st)
     default: launch_pp_tpi<T, 1>(s, st);
     }
 }
+
+int pp_kernel_count(const DevState &s) { return s.prune_buf > 0.0 ? 2 : 1; }
 
 void launch_reduce_pp(const DevState &s, cudaStream_t st)
 {

@@ -46,6 +46,7 @@ class Tuning(ctypes.Structure):
         ("plane_max", ctypes.c_int32),
         ("gather_mode", ctypes.c_int32),
         ("skin", ctypes.c_double),
+        ("prune_buf", ctypes.c_double),
     ]
 
     def as_dict(self):
@@ -128,6 +129,7 @@ SIGNATURES = {
                                ctypes.POINTER(_I)]),
     "p3m_set_tuning": (_I, [_V, ctypes.POINTER(Tuning)]),
     "p3m_get_tuning": (_I, [_V, ctypes.POINTER(Tuning)]),
+    "p3m_get_inner_builds": (_I, [_V, _I, _D]),
     "p3m_profile_stages": (_I, [_V, _I, _D, _I, ctypes.POINTER(_I)]),
     "p3m_stage_name": (ctypes.c_char_p, [_I]),
     "p3m_fp32_peak": (_I, [_I, _D]),

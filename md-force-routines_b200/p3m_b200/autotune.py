@@ -12,10 +12,14 @@ What it searches (p3m_tuning of the C ABI):
   plane per CTA) or the y and z pencil passes (16 lines per CTA);
 * the force gather: a CTA per mesh brick with one or two field-tile buffers
   (copy/compute overlap against CTAs per SM), or a CTA per brick and field
-  component (three times the work items).
+  component (three times the work items);
+* on the FP32 path, inner lists (dynamic pruning): the pair kernel reads the
+  Verlet entries closer than rc + prune_buf and rebuilds those lists itself
+  every few steps, which makes larger skins (rarer Verlet rebuilds) cheap.
 
-The last three are searched one at a time from the best PP setting
-(coordinate descent), then the fastest few settings are timed again over
+The list cells, FFT tiles and gather are searched one at a time from the
+best PP setting (coordinate descent), then inner-list buffers with a few
+skins from the best of those; then the fastest few settings are timed again over
 twice the steps (list rebuilds come every few tens of steps, so short runs
 rank close candidates by chance) and the fastest is installed. The state
 should already be equilibrated: each timing advances the system. Results are
@@ -26,9 +30,12 @@ from __future__ import annotations
 import json
 import os
 
-from ._lib import FP32, MODE_NVE
+from ._lib import FP32, MODE_NVE, P3MError
 
 CANDIDATES = [(tpi, skin) for tpi in (1, 2, 4) for skin in (0.5, 0.8, 1.1, 1.4)]
+#: FP32 inner-list buffers, each tried with the best skin so far and larger ones
+PRUNE_BUFS = (0.15, 0.25)
+PRUNE_SKINS = (1.1, 1.4)
 CACHE = os.environ.get("P3M_B200_TUNE_CACHE",
                        os.path.join(os.path.expanduser("~"), ".cache", "p3m_b200", "autotune.json"))
 
@@ -55,7 +62,8 @@ def _save(d):
 
 
 def _key(t):
-    return f"tpi{t['pp_tpi']},skin{t['skin']:g},div{t['cell_div']},plane{t['plane_max']},gather{t['gather_mode']}"
+    return (f"tpi{t['pp_tpi']},skin{t['skin']:g},div{t['cell_div']},plane{t['plane_max']},"
+            f"gather{t['gather_mode']},prune{t.get('prune_buf', 0.0):g}")
 
 
 def shape_options(ctx):
@@ -68,10 +76,20 @@ def shape_options(ctx):
     return opts
 
 
-def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, shapes=True):
+def prune_options(ctx, skin, max_skin):
+    """(skin, prune_buf) pairs worth trying from a best skin so far: FP32
+    only, each buffer below the skin."""
+    if ctx.precision != FP32:
+        return []
+    skins = sorted({skin, *(x for x in PRUNE_SKINS if x <= max_skin)})
+    return [(sk, pb) for pb in PRUNE_BUFS for sk in skins if pb < sk]
+
+
+def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, shapes=True,
+         prune=True):
     """Search the kernel shapes (see the module docstring) and install the
     fastest. Returns {"choice": {tuning}, "ms_per_step": {setting: ms},
-    "final_ms_per_step": {setting: ms}}."""
+    "final_ms_per_step": {setting: ms}, "prune_trials": n}."""
     import torch
 
     sig = signature(ctx)
@@ -86,7 +104,10 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
     base = ctx.tuning()
 
     def timed(t, n):
-        ctx.set_tuning(**t)
+        try:
+            ctx.set_tuning(**t)
+        except P3MError:  # e.g. an inner-list buffer not below a box-clamped skin
+            return float("inf")
         ctx.run(warm, MODE_NVE, graph=True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -104,6 +125,7 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
             settings[k] = dict(t)
         return times[k]
 
+    base["prune_buf"] = 0.0
     for tpi, skin in (candidates or CANDIDATES):
         if skin <= max_skin:
             trial(dict(base, pp_tpi=tpi, skin=skin))
@@ -113,13 +135,19 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
             for v in values:
                 trial(dict(best, **{name: v}))
             best = dict(settings[min(times, key=times.get)])
+    n_prune = 0
+    if prune:
+        for skin, pb in prune_options(ctx, best["skin"], max_skin):
+            trial(dict(best, skin=skin, prune_buf=pb))
+            n_prune += 1
     final = {}
     for k in sorted(times, key=times.get)[:max(1, finalists)]:
         final[k] = timed(settings[k], 2 * steps)
     win = min(final, key=final.get)
     choice = settings[win]
     ctx.set_tuning(**choice)
-    result = {"choice": choice, "ms_per_step": times, "final_ms_per_step": final}
+    result = {"choice": choice, "ms_per_step": times, "final_ms_per_step": final,
+              "prune_trials": n_prune}
     if use_cache:
         cache[sig] = result
         _save(cache)

@@ -355,6 +355,13 @@ class Context:
         keys = ("U_short", "U_fft", "U_self", "U", "K", "T", "factor", "rebuilds")
         return dict(zip(keys, (float(x) for x in out)))
 
+    def inner_builds(self, replica=0):
+        """Inner-list builds of one replica between Verlet-list rebuilds
+        (prune_buf > 0)."""
+        out = np.zeros(1)
+        self._ck(lib().p3m_get_inner_builds(self.handle, int(replica), dptr(out)))
+        return float(out[0])
+
     def check(self):
         self._ck(lib().p3m_check(self.handle))
 
@@ -387,7 +394,7 @@ class Context:
         self._ck(lib().p3m_set_pp_config(self.handle, int(tpi), float(skin)))
 
     def tuning(self):
-        """{pp_tpi, cell_div, plane_max, gather_mode, skin}: the kernel shapes."""
+        """{pp_tpi, cell_div, plane_max, gather_mode, skin, prune_buf}: the kernel shapes."""
         t = Tuning()
         self._ck(lib().p3m_get_tuning(self.handle, ctypes.byref(t)))
         return t.as_dict()
@@ -395,14 +402,15 @@ class Context:
     def set_tuning(self, **kw):
         """Change some of the kernel shapes (the others keep their values):
         pp_tpi (1, 2, 4, 8), cell_div (1, 2), plane_max (0, 32, 64),
-        gather_mode (0, 1, 2), skin."""
+        gather_mode (0, 1, 2), skin, prune_buf (FP32: 0, or the inner-list
+        buffer beyond rc, below the skin)."""
         cur = self.tuning()
         unknown = set(kw) - set(cur)
         if unknown:
             raise ValueError(f"unknown tuning keys {sorted(unknown)}")
         cur.update(kw)
         t = Tuning(int(cur["pp_tpi"]), int(cur["cell_div"]), int(cur["plane_max"]),
-                   int(cur["gather_mode"]), float(cur["skin"]))
+                   int(cur["gather_mode"]), float(cur["skin"]), float(cur["prune_buf"]))
         self._ck(lib().p3m_set_tuning(self.handle, ctypes.byref(t)))
 
     def pp_config(self):

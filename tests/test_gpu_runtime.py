@@ -381,8 +381,12 @@ def test_autotune_installs_a_finalist():
         assert set(shape_options(c)) == {"cell_div", "plane_max", "gather_mode"}
         res = tune(c, steps=10, use_cache=False, candidates=[(1, 0.5), (2, 0.8), (4, 1.1)],
                    finalists=2)
-        # 3 PP settings, then one new setting per other shape value
-        assert len(res["ms_per_step"]) == 3 + 1 + 1 + 2 and len(res["final_ms_per_step"]) == 2
+        # 3 PP settings, then one new setting per other shape value, then
+        # the inner-list buffers
+        assert res["prune_trials"] >= 2
+        assert len(res["ms_per_step"]) == 3 + 1 + 1 + 2 + res["prune_trials"]
+        assert len(res["final_ms_per_step"]) == 2
+        assert any(k.endswith("prune0.15") for k in res["ms_per_step"])
         best = min(res["final_ms_per_step"], key=res["final_ms_per_step"].get)
         assert best in res["ms_per_step"]
         assert c.tuning() == res["choice"]
@@ -392,7 +396,7 @@ def test_autotune_installs_a_finalist():
 def test_kernel_shapes_agree(prec_name):
     """Every kernel shape computes the same forces and energies: cell divisor
     1 or 2, the fused plane FFT or the pencil passes for a 32^3 and a 64^3
-    replica, every gather mode -- to rounding (FP64: 1e-12; FP32:
+    replica, every gather mode, FP32 inner lists -- to rounding (FP64: 1e-12; FP32:
     1e-6 of the RMS force) -- and the pencil FFT path matches the oracle."""
     from p3m_b200 import FP32, FP64, Context, Replica, gf_opt_device
 
@@ -404,8 +408,11 @@ def test_kernel_shapes_agree(prec_name):
     states = [_init_state(r, 30 + i)[0] for i, r in enumerate(reps)]
     pos = np.concatenate(states)
     out = {}
-    for shape in ({}, {"cell_div": 1}, {"plane_max": 0}, {"plane_max": 32}, {"gather_mode": 0},
-                  {"gather_mode": 2}):
+    shapes = [{}, {"cell_div": 1}, {"plane_max": 0}, {"plane_max": 32}, {"gather_mode": 0},
+              {"gather_mode": 2}]
+    if prec_name == "fp32":
+        shapes.append({"prune_buf": 0.2})  # inner lists, built by this force evaluation
+    for shape in shapes:
         with Context(reps, precision=prec) as c:
             c.set_tuning(**shape)
             assert all(c.tuning()[k] == v for k, v in shape.items()) or prec_name == "fp64"
@@ -434,6 +441,79 @@ def test_kernel_shapes_agree(prec_name):
                          kv.reshape(r.M, 1, 1), r.M, r.M, r.M, h, h, h, r.L, r.L, r.L)
         assert U == pytest.approx(Uo, rel=1e-10)
         assert rel_rms(acc, ao) < 1e-10
+
+
+def test_inner_lists_follow_the_trajectory():
+    """With inner lists (prune_buf > 0) the steps read lists of the Verlet
+    entries closer than rc + prune_buf, rebuilt whenever a particle moved
+    prune_buf/2: over a trajectory with several such builds between Verlet
+    rebuilds, the last step's forces equal a fresh evaluation at the same
+    positions, and graph and eager runs stay bit-identical."""
+    from p3m_b200 import FP32, MODE_NVE, Context, Replica
+
+    reps = []
+    for N, kappa, M in [(3000, 2.0, 32), (5000, 1.0, 64)]:
+        L = (4 * np.pi * N / 3) ** (1 / 3)
+        reps.append(Replica(N=N, L=L, kappa=kappa, alpha=0.7, rc=min(5.0, L / 3.6), M=M, dt=0.1,
+                            T_desired=0.02))
+    states = [_init_state(r, 41 + i) for i, r in enumerate(reps)]
+    with Context(reps, precision=FP32) as c:
+        for i, (p, v) in enumerate(states):
+            c.set_state(i, p, v)
+        c.init_forces()
+        c.equilibrate(100, quench_steps=100)
+        eq = c.get_state_all()
+    outs = []
+    for graph in (True, False):
+        with Context(reps, precision=FP32) as c:
+            skin = min(0.9, min(r.L / 3 - r.rc for r in reps) * 0.99)
+            c.set_tuning(pp_tpi=2, skin=skin, prune_buf=0.15)
+            assert c.tuning()["prune_buf"] == pytest.approx(0.15)
+            c.set_state_all(eq[0], eq[1])
+            c.init_forces()
+            rb0 = [c.replica_stats(i)["rebuilds"] for i in range(2)]
+            c.run(150, MODE_NVE, graph=graph)
+            builds = [c.inner_builds(i) for i in range(2)]
+            rebuilds = [c.replica_stats(i)["rebuilds"] - rb0[i] for i in range(2)]
+            st = c.get_state_all()
+            U = [c.replica_stats(i)["U_short"] for i in range(2)]
+        outs.append(st)
+        assert all(b >= 2 for b in builds), (builds, rebuilds)
+        assert all(b > rb for b, rb in zip(builds, rebuilds)), (builds, rebuilds)
+        with Context(reps, precision=FP32) as c:  # the Verlet lists themselves
+            c.set_tuning(pp_tpi=2, skin=skin)
+            c.set_state_all(st[0], st[1])
+            c.init_forces()
+            acc = c.get_state_all()[2]
+            U0 = [c.replica_stats(i)["U_short"] for i in range(2)]
+        assert rel_rms(st[2], acc) < 1e-6
+        for a, b in zip(U, U0):
+            assert a == pytest.approx(b, rel=1e-6)
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+
+
+def test_inner_list_settings_are_checked():
+    """prune_buf: FP32 only, non-negative, below every replica's skin; a
+    rejected setting leaves the context's shapes as they were."""
+    from p3m_b200 import FP32, FP64, Context, P3MError, Replica
+
+    N = 2000
+    L = (4 * np.pi * N / 3) ** (1 / 3)
+    r = Replica(N=N, L=L, kappa=1.0, alpha=0.8, rc=L / 4, M=32)
+    with Context(r, precision=FP64) as c:
+        with pytest.raises(P3MError):
+            c.set_tuning(prune_buf=0.2)
+    with Context(r, precision=FP32) as c:
+        c.set_tuning(skin=0.5)
+        before = c.tuning()
+        for bad in (-0.1, 0.5, 0.7, float("nan")):
+            with pytest.raises(P3MError):
+                c.set_tuning(prune_buf=bad)
+            assert c.tuning() == before
+        c.set_tuning(prune_buf=0.3)
+        c.set_tuning(prune_buf=0.0)
+        assert c.tuning()["prune_buf"] == 0.0
 
 
 def test_get_step_async_matches_sync_reads():
