@@ -88,11 +88,30 @@ __device__ __forceinline__ typename Coord<T>::I qdiff(typename Coord<T>::U a, ty
     return (typename Coord<T>::I)(a - b);
 }
 
-// Index of list entry k of sorted particle s: lists are interleaved by warps
-// of 32 consecutive particles so a warp's k-th entries are contiguous.
-__device__ __forceinline__ long long list_index(int s, int k, int maxnb)
+// List layout. A particle's entries come in blocks of PP_LIST_PAD = 16, and
+// block b of the 32 consecutive sorted particles s >> 5 is stored as one
+// group block of 512 entries (2 KB) at ((s >> 5) maxnb + 16 b) 32. Inside a
+// group block the order follows the FP32 pair kernel with TPI = 2^lt lanes
+// per particle: a pass takes STEP = UNR TPI entries of a particle (UNR =
+// min(16 / TPI, 8)), lane `sub` entries v TPI + sub (v < UNR) as UNR / C
+// chunks of C = min(UNR, 4) contiguous entries, and chunk i of all 32
+// particles' lanes lies together -- so one vector load of a warp reads 512
+// contiguous bytes (256 at TPI 8), and the 16 entries of a particle's block
+// lie within its group block (coalesced list writes). Lists are rebuilt
+// whenever TPI changes.
+__host__ __device__ constexpr int pp_unr(int tpi) { return 16 / tpi < 8 ? 16 / tpi : 8; }
+__host__ __device__ constexpr int pp_chunk(int tpi) { return pp_unr(tpi) < 4 ? pp_unr(tpi) : 4; }
+
+__device__ __forceinline__ long long list_index(int s, int e, int maxnb, int lt)
 {
-    return ((long long)(s >> 5) * maxnb + k) * 32 + (s & 31);
+    const int lu = lt == 0 ? 3 : 4 - lt;  // log2 UNR
+    const int ls = lu + lt;               // log2 STEP (3 or 4)
+    const int lc = lu < 2 ? lu : 2;       // log2 C
+    const int e16 = e & 15, pass = e16 >> ls, w = e16 & ((1 << ls) - 1);
+    const int sub = w & ((1 << lt) - 1), v = w >> lt;
+    const int chunk = (pass << (lu - lc)) + (v >> lc);
+    const int off = (((((chunk << 5) + (s & 31)) << lt) + sub) << lc) + (v & ((1 << lc) - 1));
+    return ((long long)(s >> 5) * maxnb + (e & ~15)) * 32 + off;
 }
 
 // ---------------------------------------------------------------------------
@@ -120,7 +139,7 @@ __global__ void __launch_bounds__(LB_THREADS)
 k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
               const typename Coord<T>::Q *__restrict__ xq, int *__restrict__ nnb,
               int *__restrict__ nlist, int maxnb, const int *__restrict__ rb_list, int nrep_all,
-              int *status)
+              int *status, int lt)
 {
     using Q = typename Coord<T>::Q;
     constexpr int SCAP = lb_scap<T>();
@@ -221,7 +240,7 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                                              ((1u << LB_TPI) - 1u);
                         if (in) {
                             const int pos = cnt + __popc(grp & below);
-                            if (pos < maxnb) nlist[list_index(s, pos, maxnb)] = j;
+                            if (pos < maxnb) nlist[list_index(s, pos, maxnb, lt)] = j;
                         }
                         cnt += __popc(grp);
                     }
@@ -241,7 +260,7 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                 // multiple of PP_LIST_PAD, so the pad stays in the list
                 const int pe = nn + sub;
                 if (pe < ((nn + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1)))
-                    nlist[list_index(s, pe, maxnb)] = s;
+                    nlist[list_index(s, pe, maxnb, lt)] = s;
             }
         }
     }
@@ -284,6 +303,7 @@ k_pp_f64(const RepDev *__restrict__ reps, int nrep, const ulonglong4 *__restrict
     using T = double;
     using Q = ulonglong4;
     constexpr int PPB = PPL_THREADS / TPI;  // particles per block
+    constexpr int LT = TPI == 1 ? 0 : TPI == 2 ? 1 : TPI == 4 ? 2 : 3;
     constexpr int CH = 32;                  // entries per Kahan flush
     __shared__ double red[32];
     const int b = blockIdx.x;
@@ -313,7 +333,7 @@ k_pp_f64(const RepDev *__restrict__ reps, int nrep, const ulonglong4 *__restrict
 #pragma unroll
                 for (int v = 0; v < UNR; ++v) {
                     const int kk = k + v * TPI;
-                    j[v] = kk < k1 ? __ldg(nlist + list_index(s, kk, maxnb)) : s;
+                    j[v] = kk < k1 ? __ldg(nlist + list_index(s, kk, maxnb, LT)) : s;
                 }
                 Q q[UNR];
 #pragma unroll
@@ -461,6 +481,27 @@ __device__ __forceinline__ void pair_table2(const uint4 &xi, const uint4 &qa, co
 // which reads the inner lists. The two touch disjoint replicas and blocks.
 enum PpMode { PP_OUTER = 0, PP_INNER = 1, PP_PRUNE = 2 };
 
+// One particle's block of 16 list entries, buf[e] = entry e, written by its
+// TPI lanes in the list layout: og = the lane's first chunk in the particle's
+// group block (see list_index).
+template <int TPI>
+__device__ __forceinline__ void store_block(int *og, const int *buf, int sub)
+{
+    constexpr int UNR = pp_unr(TPI), STEP = UNR * TPI, C = pp_chunk(TPI), NCH = UNR / C;
+    constexpr int CSTRIDE = 32 * TPI * C;
+#pragma unroll
+    for (int pass = 0; pass < PP_LIST_PAD / STEP; ++pass)
+#pragma unroll
+        for (int i = 0; i < NCH; ++i) {
+            const int *e = buf + pass * STEP + i * C * TPI + sub;  // entries (i C + c) TPI + sub
+            int *dst = og + (pass * NCH + i) * CSTRIDE;
+            if constexpr (C == 4)
+                *reinterpret_cast<int4 *>(dst) = make_int4(e[0], e[TPI], e[2 * TPI], e[3 * TPI]);
+            else
+                *reinterpret_cast<int2 *>(dst) = make_int2(e[0], e[TPI]);
+        }
+}
+
 struct PruneArgs {
     const int *rebuild = nullptr, *prune = nullptr;  // per-replica flags
     int *nnb_in = nullptr, *nlist_in = nullptr;      // inner lists (written by PP_PRUNE)
@@ -481,11 +522,16 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
     constexpr bool P = P3M_PP_PACK != 0;
     constexpr bool PRUNE = PM == PP_PRUNE;
     constexpr int PPB = PPL_THREADS / TPI;               // particles per block
-    constexpr int UNR = PP_LIST_PAD / TPI < 8 ? PP_LIST_PAD / TPI : 8;  // entries per lane per pass
-    constexpr int STEP = UNR * TPI;                       // entries of a particle per pass
+    constexpr int UNR = pp_unr(TPI);                     // entries per lane per pass
+    constexpr int STEP = UNR * TPI;                      // entries of a particle per pass
+    constexpr int C = pp_chunk(TPI), NCH = UNR / C;      // list chunks of a lane per pass
+    constexpr int CSTRIDE = 32 * TPI * C;                // between a lane's chunks (entries)
     static_assert(UNR % 2 == 0 && PP_LIST_PAD % STEP == 0, "whole pairs, whole pad blocks");
-    static_assert(STEP <= 32, "a pass's keep bits fit one word");
+    static_assert(PP_LIST_PAD == 16 && STEP <= 16, "the list layout's blocks");
     __shared__ double red[32];
+    // PP_PRUNE: each particle's inner entries wait here until a whole block
+    // of 16 can be written (up to 15 carried + 16 of a pass)
+    __shared__ __align__(16) int pstage[PRUNE ? PPB * 32 : 1];
     extern __shared__ __align__(16) float4 ppl_tab[];
     const int b = blockIdx.x;
     const int r = find_rep(b, nrep, [&](int k) { return reps[k].pp_blk_off; });
@@ -516,23 +562,38 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
     const float2 inv_h = f2(ih, ih);
     const float rin2 = PRUNE ? (float)((R.rc + R.pbuf) * (R.rc + R.pbuf)) : 0.f;
     const int gbase = (threadIdx.x & 31) & ~(TPI - 1);   // first lane of this particle's group
+    const int p32 = s & 31;
 
     float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     double u = 0.0;
     if (have) {
         const uint4 xi = xq[s];
         const int nr = (nnb[s] + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1);
-        const int *lp = nlist + list_index(s, sub, maxnb);
-        int cin = 0;  // PP_PRUNE: inner entries so far
-        for (int k0 = 0; k0 < nr; k0 += STEP, lp += STEP * 32) {
+        // this lane's first chunk in the particle's group blocks
+        const int *lg = nlist + (long long)(s >> 5) * maxnb * 32 + (p32 * TPI + sub) * C;
+        int *buf = pstage + (threadIdx.x / TPI) * 32;    // PP_PRUNE staging
+        int fill = 0, blk = 0;                           // PP_PRUNE: staged entries, blocks written
+        int *og = PRUNE ? pa.nlist_in + (long long)(s >> 5) * pa.maxnb_in * 32 + (p32 * TPI + sub) * C
+                        : nullptr;
+        const unsigned gm = ((1u << TPI) - 1u) << gbase;
+        for (int k0 = 0; k0 < nr; k0 += STEP) {
+            const int *lp = lg + (long long)(k0 & ~15) * 32 + ((k0 & 15) / STEP) * NCH * CSTRIDE;
             int j[UNR];
 #pragma unroll
-            for (int v = 0; v < UNR; ++v) j[v] = __ldg(lp + v * TPI * 32);
+            for (int i = 0; i < NCH; ++i) {
+                if constexpr (C == 4) {
+                    const int4 t = __ldg(reinterpret_cast<const int4 *>(lp + i * CSTRIDE));
+                    j[4 * i + 0] = t.x; j[4 * i + 1] = t.y; j[4 * i + 2] = t.z; j[4 * i + 3] = t.w;
+                } else {
+                    const int2 t = __ldg(reinterpret_cast<const int2 *>(lp + i * CSTRIDE));
+                    j[2 * i + 0] = t.x; j[2 * i + 1] = t.y;
+                }
+            }
             uint4 q[UNR];
 #pragma unroll
             for (int v = 0; v < UNR; ++v) q[v] = xq[j[v]];
             float2 px = f2(0.f, 0.f), py = px, pz = px, pu = px;
-            unsigned keep = 0;  // PP_PRUNE: bit v = entry v of this lane goes to the inner list
+            unsigned keep = 0;  // PP_PRUNE: bit v = this lane's entry v goes to the inner list
 #pragma unroll
             for (int v = 0; v < UNR; v += 2) {
                 unsigned k2 = 0;
@@ -549,13 +610,12 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
 #pragma unroll
                 for (int v = 0; v < UNR; ++v)
                     if (j[v] == s) keep &= ~(1u << v);  // list padding
-                // entry v of lane `sub` is entry v * TPI + sub of the pass:
-                // the group's keep bits in entry order give each its place
+                // this lane's entry v is entry v TPI + sub of the pass: the
+                // group's keep bits in entry order give each kept one its place
                 unsigned mask = 0;
                 if constexpr (TPI == 1) {
                     mask = keep;
                 } else {
-                    const unsigned gm = ((1u << TPI) - 1u) << gbase;
 #pragma unroll
                     for (int v = 0; v < UNR; ++v) {
                         const unsigned bal = __ballot_sync(gm, (keep >> v) & 1u);
@@ -564,27 +624,36 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
                 }
 #pragma unroll
                 for (int v = 0; v < UNR; ++v)
-                    if ((keep >> v) & 1u) {
-                        const int e = v * TPI + sub;
-                        const int pos = cin + __popc(mask & ((1u << e) - 1u));
-                        if (pos < pa.maxnb_in) pa.nlist_in[list_index(s, pos, pa.maxnb_in)] = j[v];
-                    }
-                cin += __popc(mask);
+                    if ((keep >> v) & 1u) buf[fill + __popc(mask & ((1u << (v * TPI + sub)) - 1u))] = j[v];
+                fill += __popc(mask);
+                __syncwarp(gm);
+                if (fill >= PP_LIST_PAD) {  // a whole block: out, in the list layout
+                    if ((blk + 1) * PP_LIST_PAD <= pa.maxnb_in)
+                        store_block<TPI>(og + (long long)blk * PP_LIST_PAD * 32, buf, sub);
+                    ++blk;
+                    __syncwarp(gm);
+                    for (int e = sub; e < fill - PP_LIST_PAD; e += TPI) buf[e] = buf[PP_LIST_PAD + e];
+                    fill -= PP_LIST_PAD;
+                    __syncwarp(gm);
+                }
             }
         }
         if constexpr (PRUNE) {
-            const int nn = min(cin, pa.maxnb_in);
+            const int cin = blk * PP_LIST_PAD + fill;
+            if (fill > 0) {  // the last block, padded with the particle itself
+                for (int e = fill + sub; e < PP_LIST_PAD; e += TPI) buf[e] = s;
+                __syncwarp(gm);
+                if ((blk + 1) * PP_LIST_PAD <= pa.maxnb_in)
+                    store_block<TPI>(og + (long long)blk * PP_LIST_PAD * 32, buf, sub);
+            }
             if (sub == 0) {
                 if (cin > pa.maxnb_in) raise_status(pa.status, ST_NBOVF);
-                pa.nnb_in[s] = nn;
+                pa.nnb_in[s] = min(cin, pa.maxnb_in);
                 const int o = pa.cell_perm[s];
                 pa.pos_pref[3 * o + 0] = pa.pos[3 * o + 0];
                 pa.pos_pref[3 * o + 1] = pa.pos[3 * o + 1];
                 pa.pos_pref[3 * o + 2] = pa.pos[3 * o + 2];
             }
-            // pad like the outer lists (maxnb_in is a multiple of PP_LIST_PAD)
-            const int pend = (nn + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1);
-            for (int e = nn + sub; e < pend; e += TPI) pa.nlist_in[list_index(s, e, pa.maxnb_in)] = s;
         }
     }
 #pragma unroll
@@ -654,7 +723,7 @@ template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st
     auto kern = s.cell_div == 1 ? k_build_lists<T, 1> : k_build_lists<T, 2>;
     kern<<<grid, LB_THREADS, lb_scap<T>() * sizeof(Q), st>>>(
         s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.rb_list, s.nrep,
-        s.status);
+        s.status, __builtin_ctz((unsigned)s.pp_tpi));
 }
 
 template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cudaStream_t st)
