@@ -134,13 +134,14 @@ static_assert(LB_TPI >= PP_LIST_PAD, "one pad entry per lane at most");
 // and a warp ballot gives each candidate in range its place: the list holds
 // the in-range candidates in stencil order, as a scan by one thread would,
 // then the particle's own index up to a whole block of PP_LIST_PAD entries.
-template <typename T, int D>
+template <typename T, int D, int LT>
 __global__ void __launch_bounds__(LB_THREADS)
 k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_start,
               const typename Coord<T>::Q *__restrict__ xq, int *__restrict__ nnb,
               int *__restrict__ nlist, int maxnb, const int *__restrict__ rb_list, int nrep_all,
-              int *status, int lt)
+              int *status)
 {
+    constexpr int lt = LT;  // the list layout of the pair kernel's TPI = 2^LT
     using Q = typename Coord<T>::Q;
     constexpr int SCAP = lb_scap<T>();
     constexpr int CELL_SPAN = 2 * D + 1;
@@ -566,28 +567,37 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
 
     float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     double u = 0.0;
-    if (have) {
-        const uint4 xi = xq[s];
-        const int nr = (nnb[s] + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1);
+    // PP_PRUNE keeps the warp converged for its ballots and shared staging:
+    // every lane runs the warp's longest list, lanes past their own (or
+    // without a particle) evaluating their own slot, which adds nothing
+    if (have || PRUNE) {
+        const int sv = have ? s : R.p_off;
+        const uint4 xi = xq[sv];
+        const int nr = have ? (nnb[s] + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1) : 0;
+        const int nloop = PRUNE ? __reduce_max_sync(0xffffffffu, nr) : nr;
         // this lane's first chunk in the particle's group blocks
-        const int *lg = nlist + (long long)(s >> 5) * maxnb * 32 + (p32 * TPI + sub) * C;
+        const int *lg = nlist + (long long)(sv >> 5) * maxnb * 32 + (p32 * TPI + sub) * C;
         int *buf = pstage + (threadIdx.x / TPI) * 32;    // PP_PRUNE staging
         int fill = 0, blk = 0;                           // PP_PRUNE: staged entries, blocks written
-        int *og = PRUNE ? pa.nlist_in + (long long)(s >> 5) * pa.maxnb_in * 32 + (p32 * TPI + sub) * C
+        int *og = PRUNE ? pa.nlist_in + (long long)(sv >> 5) * pa.maxnb_in * 32 + (p32 * TPI + sub) * C
                         : nullptr;
-        const unsigned gm = ((1u << TPI) - 1u) << gbase;
-        for (int k0 = 0; k0 < nr; k0 += STEP) {
+        for (int k0 = 0; k0 < nloop; k0 += STEP) {
             const int *lp = lg + (long long)(k0 & ~15) * 32 + ((k0 & 15) / STEP) * NCH * CSTRIDE;
             int j[UNR];
+            if (!PRUNE || k0 < nr) {
 #pragma unroll
-            for (int i = 0; i < NCH; ++i) {
-                if constexpr (C == 4) {
-                    const int4 t = __ldg(reinterpret_cast<const int4 *>(lp + i * CSTRIDE));
-                    j[4 * i + 0] = t.x; j[4 * i + 1] = t.y; j[4 * i + 2] = t.z; j[4 * i + 3] = t.w;
-                } else {
-                    const int2 t = __ldg(reinterpret_cast<const int2 *>(lp + i * CSTRIDE));
-                    j[2 * i + 0] = t.x; j[2 * i + 1] = t.y;
+                for (int i = 0; i < NCH; ++i) {
+                    if constexpr (C == 4) {
+                        const int4 t = __ldg(reinterpret_cast<const int4 *>(lp + i * CSTRIDE));
+                        j[4 * i + 0] = t.x; j[4 * i + 1] = t.y; j[4 * i + 2] = t.z; j[4 * i + 3] = t.w;
+                    } else {
+                        const int2 t = __ldg(reinterpret_cast<const int2 *>(lp + i * CSTRIDE));
+                        j[2 * i + 0] = t.x; j[2 * i + 1] = t.y;
+                    }
                 }
+            } else {
+#pragma unroll
+                for (int v = 0; v < UNR; ++v) j[v] = sv;
             }
             uint4 q[UNR];
 #pragma unroll
@@ -609,7 +619,7 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
             if constexpr (PRUNE) {
 #pragma unroll
                 for (int v = 0; v < UNR; ++v)
-                    if (j[v] == s) keep &= ~(1u << v);  // list padding
+                    if (j[v] == sv) keep &= ~(1u << v);  // list padding, idle lanes
                 // this lane's entry v is entry v TPI + sub of the pass: the
                 // group's keep bits in entry order give each kept one its place
                 unsigned mask = 0;
@@ -618,7 +628,7 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
                 } else {
 #pragma unroll
                     for (int v = 0; v < UNR; ++v) {
-                        const unsigned bal = __ballot_sync(gm, (keep >> v) & 1u);
+                        const unsigned bal = __ballot_sync(0xffffffffu, (keep >> v) & 1u);
                         mask |= ((bal >> gbase) & ((1u << TPI) - 1u)) << (v * TPI);
                     }
                 }
@@ -626,27 +636,31 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
                 for (int v = 0; v < UNR; ++v)
                     if ((keep >> v) & 1u) buf[fill + __popc(mask & ((1u << (v * TPI + sub)) - 1u))] = j[v];
                 fill += __popc(mask);
-                __syncwarp(gm);
-                if (fill >= PP_LIST_PAD) {  // a whole block: out, in the list layout
-                    if ((blk + 1) * PP_LIST_PAD <= pa.maxnb_in)
-                        store_block<TPI>(og + (long long)blk * PP_LIST_PAD * 32, buf, sub);
-                    ++blk;
-                    __syncwarp(gm);
+                __syncwarp();
+                // a whole block: out, in the list layout (group-uniform tests,
+                // no synchronisation inside them)
+                const bool full = fill >= PP_LIST_PAD;
+                if (full && (blk + 1) * PP_LIST_PAD <= pa.maxnb_in)
+                    store_block<TPI>(og + (long long)blk * PP_LIST_PAD * 32, buf, sub);
+                __syncwarp();
+                if (full)
                     for (int e = sub; e < fill - PP_LIST_PAD; e += TPI) buf[e] = buf[PP_LIST_PAD + e];
+                __syncwarp();
+                if (full) {
                     fill -= PP_LIST_PAD;
-                    __syncwarp(gm);
+                    ++blk;
                 }
             }
         }
         if constexpr (PRUNE) {
             const int cin = blk * PP_LIST_PAD + fill;
-            if (fill > 0) {  // the last block, padded with the particle itself
-                for (int e = fill + sub; e < PP_LIST_PAD; e += TPI) buf[e] = s;
-                __syncwarp(gm);
-                if ((blk + 1) * PP_LIST_PAD <= pa.maxnb_in)
-                    store_block<TPI>(og + (long long)blk * PP_LIST_PAD * 32, buf, sub);
-            }
-            if (sub == 0) {
+            // the last block, padded with the particle itself
+            if (fill > 0)
+                for (int e = fill + sub; e < PP_LIST_PAD; e += TPI) buf[e] = sv;
+            __syncwarp();
+            if (have && fill > 0 && (blk + 1) * PP_LIST_PAD <= pa.maxnb_in)
+                store_block<TPI>(og + (long long)blk * PP_LIST_PAD * 32, buf, sub);
+            if (have && sub == 0) {
                 if (cin > pa.maxnb_in) raise_status(pa.status, ST_NBOVF);
                 pa.nnb_in[s] = min(cin, pa.maxnb_in);
                 const int o = pa.cell_perm[s];
@@ -694,10 +708,12 @@ int pp_particles_per_block(int tpi) { return PPL_THREADS / tpi; }
 template <typename T> void configure_pp_kernels()
 {
     using Q = typename Coord<T>::Q;
-    cudaFuncSetAttribute(k_build_lists<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(lb_scap<T>() * sizeof(Q)));
-    cudaFuncSetAttribute(k_build_lists<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(lb_scap<T>() * sizeof(Q)));
+    const int lbs = (int)(lb_scap<T>() * sizeof(Q));
+    auto setl = [&](auto k) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lbs); };
+    setl(k_build_lists<T, 1, 0>); setl(k_build_lists<T, 1, 1>);
+    setl(k_build_lists<T, 1, 2>); setl(k_build_lists<T, 1, 3>);
+    setl(k_build_lists<T, 2, 0>); setl(k_build_lists<T, 2, 1>);
+    setl(k_build_lists<T, 2, 2>); setl(k_build_lists<T, 2, 3>);
     if constexpr (sizeof(T) == 4) {
         const int tab = (int)(PP_TABLE_N * PP_TABLE_COPIES * sizeof(float4));
         auto set = [&](auto k) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tab); };
@@ -720,10 +736,15 @@ template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st
 {
     using Q = typename Coord<T>::Q;
     const int grid = s.ncell < 148 * 16 ? s.ncell : 148 * 16;
-    auto kern = s.cell_div == 1 ? k_build_lists<T, 1> : k_build_lists<T, 2>;
+    using K = void (*)(const RepDev *, int, const int *, const Q *, int *, int *, int, const int *,
+                       int, int *);
+    static const K kerns[2][4] = {
+        {k_build_lists<T, 1, 0>, k_build_lists<T, 1, 1>, k_build_lists<T, 1, 2>, k_build_lists<T, 1, 3>},
+        {k_build_lists<T, 2, 0>, k_build_lists<T, 2, 1>, k_build_lists<T, 2, 2>, k_build_lists<T, 2, 3>}};
+    const K kern = kerns[s.cell_div == 1 ? 0 : 1][__builtin_ctz((unsigned)s.pp_tpi) & 3];
     kern<<<grid, LB_THREADS, lb_scap<T>() * sizeof(Q), st>>>(
         s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.rb_list, s.nrep,
-        s.status, __builtin_ctz((unsigned)s.pp_tpi));
+        s.status);
 }
 
 template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cudaStream_t st)
