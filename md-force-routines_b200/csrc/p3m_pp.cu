@@ -304,7 +304,6 @@ k_pp_f64(const RepDev *__restrict__ reps, int nrep, const ulonglong4 *__restrict
     using T = double;
     using Q = ulonglong4;
     constexpr int PPB = PPL_THREADS / TPI;  // particles per block
-    constexpr int LT = TPI == 1 ? 0 : TPI == 2 ? 1 : TPI == 4 ? 2 : 3;
     constexpr int CH = 32;                  // entries per Kahan flush
     __shared__ double red[32];
     const int b = blockIdx.x;
@@ -322,19 +321,29 @@ k_pp_f64(const RepDev *__restrict__ reps, int nrep, const ulonglong4 *__restrict
     double u = 0.0;
     if (have) {
         const Q xi = xq[s];
-        const int n = nnb[s];
-        constexpr int UNR = 8;  // list entries in flight per thread
-        for (int k0 = 0; k0 < n; k0 += CH) {
-            const int k1 = min(k0 + CH, n);
+        // the padded list in passes of the layout (see list_index): lane sub
+        // takes entries v TPI + sub of each pass, as chunks of C
+        constexpr int UNR = pp_unr(TPI), STEP = UNR * TPI, C = pp_chunk(TPI), NCH = UNR / C;
+        constexpr int CSTRIDE = 32 * TPI * C;
+        const int nr = (nnb[s] + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1);
+        const int *lg = nlist + (long long)(s >> 5) * maxnb * 32 + ((s & 31) * TPI + sub) * C;
+        for (int c0 = 0; c0 < nr; c0 += CH) {
+            const int c1 = min(c0 + CH, nr);
             T px = 0, py = 0, pz = 0, pu = 0;
-            for (int k = k0 + sub; k < k1; k += UNR * TPI) {
-                // independent loads first (missing entries point at the
-                // particle itself: r2 = 0 is skipped below)
+            for (int k0 = c0; k0 < c1; k0 += STEP) {
+                // independent loads first (padding points at the particle
+                // itself: r2 = 0 is skipped below)
+                const int *lp = lg + (long long)(k0 & ~15) * 32 + ((k0 & 15) / STEP) * NCH * CSTRIDE;
                 int j[UNR];
 #pragma unroll
-                for (int v = 0; v < UNR; ++v) {
-                    const int kk = k + v * TPI;
-                    j[v] = kk < k1 ? __ldg(nlist + list_index(s, kk, maxnb, LT)) : s;
+                for (int i = 0; i < NCH; ++i) {
+                    if constexpr (C == 4) {
+                        const int4 t = __ldg(reinterpret_cast<const int4 *>(lp + i * CSTRIDE));
+                        j[4 * i + 0] = t.x; j[4 * i + 1] = t.y; j[4 * i + 2] = t.z; j[4 * i + 3] = t.w;
+                    } else {
+                        const int2 t = __ldg(reinterpret_cast<const int2 *>(lp + i * CSTRIDE));
+                        j[2 * i + 0] = t.x; j[2 * i + 1] = t.y;
+                    }
                 }
                 Q q[UNR];
 #pragma unroll
