@@ -508,8 +508,15 @@ __device__ __forceinline__ void x_r2c_item(const RepDev &R, int w, const T *__re
     const T *t = tiles + R.tile_off;
     T *dst = reinterpret_cast<T *>(&buf[brev(x, LOGM) * LSX]);
     __syncthreads();
-    for (int j = threadIdx.x >> LOGM; j < NROW; j += FFT_THREADS >> LOGM)
-        dst[j] = rho_sum<T>(t, ax, axis_y(y0 + j, R.nb), az);  // line j/2, part j%2
+    // FP32: several rows' tile loads in flight per thread (the pass waits on them)
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll 4
+        for (int j = threadIdx.x >> LOGM; j < NROW; j += FFT_THREADS >> LOGM)
+            dst[j] = rho_sum<T>(t, ax, axis_y(y0 + j, R.nb), az);  // line j/2, part j%2
+    } else {
+        for (int j = threadIdx.x >> LOGM; j < NROW; j += FFT_THREADS >> LOGM)
+            dst[j] = rho_sum<T>(t, ax, axis_y(y0 + j, R.nb), az);
+    }
     __syncthreads();
     fft_lines_t<T, LOGM>(buf, 1, LSX, LNL, tw, false);
     // split the two real rows: Xa = (Z[k] + conj Z[M-k])/2, Xb = (Z[k] - conj Z[M-k])/2i
@@ -806,6 +813,21 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
 // 2l and 2l+1 share complex line l: Z[k] = Xa[k] + i Xb[k] over the
 // Hermitian extension, with the imaginary parts at k = 0 and M/2 dropped.
 // Instantiated per mesh side like pass A.
+// Two adjacent spectrum rows a, b of line l, wavenumber k, packed into the
+// complex line of an inverse transform whose real and imaginary parts come
+// out as the two real rows (k and M - k from Hermitian symmetry).
+template <typename T, int LOGM>
+__device__ __forceinline__ void c2r_split(cplx<T> *buf, int k, int l, cplx<T> a, cplx<T> b)
+{
+    constexpr int M = 1 << LOGM;
+    if (k == 0 || k == (M >> 1)) {
+        buf[brev(k, LOGM) * LSX + l] = make_c<T>(a.x, b.x);
+    } else {
+        buf[brev(k, LOGM) * LSX + l] = make_c<T>(a.x - b.y, a.y + b.x);
+        buf[brev(M - k, LOGM) * LSX + l] = make_c<T>(a.x + b.y, b.x - a.y);
+    }
+}
+
 template <typename T, int LOGM>
 __device__ __forceinline__ void x_c2r_item(const RepDev &R, int comp, int w,
                                            const cplx<T> *__restrict__ ek, long long nspec,
@@ -818,23 +840,23 @@ __device__ __forceinline__ void x_c2r_item(const RepDev &R, int comp, int w,
     const int z = w / NYT, y0 = (w % NYT) * NROW;
     const cplx<T> *src = ek + comp * nspec + R.spec_off + (long long)z * M + y0;
     __syncthreads();
-    for (int e = threadIdx.x; e < (NK << LNL); e += FFT_THREADS) {
-        const int l = e & ((1 << LNL) - 1), k = e >> LNL;
-        const long long o = (long long)k * M * M + 2 * l;
-        cplx<T> a, b;  // o is even: one 16-byte load in FP32
-        if constexpr (sizeof(T) == 4) {
+    // FP32: all of a thread's spectrum loads in flight at once (the pass
+    // waits on them)
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int e = threadIdx.x; e < (NK << LNL); e += FFT_THREADS) {
+            const int l = e & ((1 << LNL) - 1), k = e >> LNL;
+            const long long o = (long long)k * M * M + 2 * l;
+            // o is even: one 16-byte load
             const float4 ab = __ldg(reinterpret_cast<const float4 *>(src + o));
-            a = make_c<T>(ab.x, ab.y);
-            b = make_c<T>(ab.z, ab.w);
-        } else {
-            a = src[o];
-            b = src[o + 1];
+            const cplx<T> a = make_c<T>(ab.x, ab.y), b = make_c<T>(ab.z, ab.w);
+            c2r_split<T, LOGM>(buf, k, l, a, b);
         }
-        if (k == 0 || k == (M >> 1)) {
-            buf[brev(k, LOGM) * LSX + l] = make_c<T>(a.x, b.x);
-        } else {
-            buf[brev(k, LOGM) * LSX + l] = make_c<T>(a.x - b.y, a.y + b.x);
-            buf[brev(M - k, LOGM) * LSX + l] = make_c<T>(a.x + b.y, b.x - a.y);
+    } else {
+        for (int e = threadIdx.x; e < (NK << LNL); e += FFT_THREADS) {
+            const int l = e & ((1 << LNL) - 1), k = e >> LNL;
+            const long long o = (long long)k * M * M + 2 * l;
+            c2r_split<T, LOGM>(buf, k, l, src[o], src[o + 1]);
         }
     }
     __syncthreads();
@@ -848,7 +870,7 @@ __device__ __forceinline__ void x_c2r_item(const RepDev &R, int comp, int w,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(FFT_THREADS)
+__global__ void __launch_bounds__(FFT_THREADS, sizeof(T) == 4 ? 4 : 3)
 k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict__ ek,
             long long nspec, T *__restrict__ efield, long long nmesh,
             const cplx<T> *__restrict__ twg, int nitems_per_comp)
