@@ -482,39 +482,17 @@ __device__ __forceinline__ void pair_table2(const uint4 &xi, const uint4 &qa, co
 #define P3M_PP_MINB 3
 #endif
 
-// List modes of the FP32 pair kernel. Without inner lists (prune buffer 0)
-// it reads the outer lists (PP_OUTER). With them a step launches it twice:
-// PP_PRUNE for the replicas whose flag (outer rebuild or inner prune) is set
-// -- the outer lists, writing each particle's inner list on the way: the
-// entries closer than rc + pbuf, in outer-list order, padded like the outer
-// ones, and the positions they were taken at -- and PP_INNER for the others,
-// which reads the inner lists. The two touch disjoint replicas and blocks.
-enum PpMode { PP_OUTER = 0, PP_INNER = 1, PP_PRUNE = 2 };
-
-// One particle's block of 16 list entries, buf[e] = entry e, written by its
-// TPI lanes in the list layout: og = the lane's first chunk in the particle's
-// group block (see list_index).
-template <int TPI>
-__device__ __forceinline__ void store_block(int *og, const int *buf, int sub)
-{
-    constexpr int UNR = pp_unr(TPI), STEP = UNR * TPI, C = pp_chunk(TPI), NCH = UNR / C;
-    constexpr int CSTRIDE = 32 * TPI * C;
-#pragma unroll
-    for (int pass = 0; pass < PP_LIST_PAD / STEP; ++pass)
-#pragma unroll
-        for (int i = 0; i < NCH; ++i) {
-            const int *e = buf + pass * STEP + i * C * TPI + sub;  // entries (i C + c) TPI + sub
-            int *dst = og + (pass * NCH + i) * CSTRIDE;
-            if constexpr (C == 4)
-                *reinterpret_cast<int4 *>(dst) = make_int4(e[0], e[TPI], e[2 * TPI], e[3 * TPI]);
-            else
-                *reinterpret_cast<int2 *>(dst) = make_int2(e[0], e[TPI]);
-        }
-}
+// List modes of the FP32 pair kernel. PP_OUTER (no inner lists, prune
+// buffer 0) reads the Verlet lists. PP_DYN decides per block: a replica whose
+// flag is set (Verlet rebuild or inner prune) has its outer lists read and
+// each particle's inner list written on the way -- the entries closer than
+// rc + pbuf, in outer-list order, padded like the outer ones -- with the
+// positions they were taken at; the other replicas read their inner lists.
+enum PpMode { PP_OUTER = 0, PP_DYN = 1 };
 
 struct PruneArgs {
     const int *rebuild = nullptr, *prune = nullptr;  // per-replica flags
-    int *nnb_in = nullptr, *nlist_in = nullptr;      // inner lists (written by PP_PRUNE)
+    int *nnb_in = nullptr, *nlist_in = nullptr;      // inner lists (written by pruning blocks)
     int maxnb_in = 0;
     const int *cell_perm = nullptr;                  // sorted -> original particle
     const double *pos = nullptr;
@@ -522,46 +500,60 @@ struct PruneArgs {
     int *status = nullptr;
 };
 
-template <int TPI, int PM>
-__global__ void __launch_bounds__(PPL_THREADS, P3M_PP_MINB)
-k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq,
-         const int *__restrict__ nnb, const int *__restrict__ nlist, int maxnb,
-         const float4 *__restrict__ tables, float4 *__restrict__ acc_out,
-         double *__restrict__ u_part, PruneArgs pa)
+// Staging of the inner entries of a warp's particles while a block of 16
+// fills: position q of the warp's particle w at stage[q * PPW + w] (PPW =
+// 32 / TPI particles per warp), so the TPI lanes of a particle, which touch
+// consecutive positions, and the warp's particles, one bank apart, never
+// share a bank. 32 positions: up to 15 carried and 16 of a pass.
+template <int TPI> struct Stage {
+    static constexpr int PPW = 32 / TPI;
+    int *w;  // this warp's area (32 PPW ints)
+    int p;   // this particle's index in the warp
+    __device__ __forceinline__ int &operator[](int q) const { return w[q * PPW + p]; }
+};
+
+// One particle's block of 16 staged entries, written by its TPI lanes in
+// the list layout: og = the lane's first chunk in the particle's group
+// block (see list_index).
+template <int TPI>
+__device__ __forceinline__ void store_block(int *og, const Stage<TPI> &buf, int sub)
+{
+    constexpr int UNR = pp_unr(TPI), STEP = UNR * TPI, C = pp_chunk(TPI), NCH = UNR / C;
+    constexpr int CSTRIDE = 32 * TPI * C;
+#pragma unroll
+    for (int pass = 0; pass < PP_LIST_PAD / STEP; ++pass)
+#pragma unroll
+        for (int i = 0; i < NCH; ++i) {
+            const int e = pass * STEP + i * C * TPI + sub;  // entries (i C + c) TPI + sub
+            int *dst = og + (pass * NCH + i) * CSTRIDE;
+            if constexpr (C == 4)
+                *reinterpret_cast<int4 *>(dst) =
+                    make_int4(buf[e], buf[e + TPI], buf[e + 2 * TPI], buf[e + 3 * TPI]);
+            else
+                *reinterpret_cast<int2 *>(dst) = make_int2(buf[e], buf[e + TPI]);
+        }
+}
+
+// The pair loop of one particle slot s (have: s holds a particle of
+// replica R) over the list (nnb, nlist, maxnb); PRUNE: also its inner list.
+// Returns the energy partial; the force goes to acc_out.
+template <int TPI, bool PRUNE>
+__device__ __forceinline__ double pp_body(const RepDev &R, int s, bool have,
+                                          const uint4 *__restrict__ xq,
+                                          const int *__restrict__ nnb,
+                                          const int *__restrict__ nlist, int maxnb,
+                                          const float4 *__restrict__ tab,
+                                          float4 *__restrict__ acc_out, const PruneArgs &pa,
+                                          int *stage_warp)
 {
     constexpr bool P = P3M_PP_PACK != 0;
-    constexpr bool PRUNE = PM == PP_PRUNE;
-    constexpr int PPB = PPL_THREADS / TPI;               // particles per block
     constexpr int UNR = pp_unr(TPI);                     // entries per lane per pass
     constexpr int STEP = UNR * TPI;                      // entries of a particle per pass
     constexpr int C = pp_chunk(TPI), NCH = UNR / C;      // list chunks of a lane per pass
     constexpr int CSTRIDE = 32 * TPI * C;                // between a lane's chunks (entries)
     static_assert(UNR % 2 == 0 && PP_LIST_PAD % STEP == 0, "whole pairs, whole pad blocks");
     static_assert(PP_LIST_PAD == 16 && STEP <= 16, "the list layout's blocks");
-    __shared__ double red[32];
-    // PP_PRUNE: each particle's inner entries wait here until a whole block
-    // of 16 can be written (up to 15 carried + 16 of a pass)
-    __shared__ __align__(16) int pstage[PRUNE ? PPB * 32 : 1];
-    extern __shared__ __align__(16) float4 ppl_tab[];
-    const int b = blockIdx.x;
-    const int r = find_rep(b, nrep, [&](int k) { return reps[k].pp_blk_off; });
-    if constexpr (PM != PP_OUTER) {
-        // block-uniform: this block's replica belongs to the other launch
-        const bool flagged = (pa.rebuild[r] | pa.prune[r]) != 0;
-        if (flagged != PRUNE) return;
-    }
-    const RepDev &R = reps[r];
-    {
-        const float4 *src = tables + (long long)r * PP_TABLE_N;
-        for (int k = threadIdx.x; k < PP_TABLE_N * PP_TABLE_COPIES; k += PPL_THREADS)
-            cp_async16(ppl_tab + k, src + k / PP_TABLE_COPIES);
-        cp_async_wait_all();
-        __syncthreads();
-    }
-    const float4 *tab = ppl_tab + (threadIdx.x & (PP_TABLE_COPIES - 1));  // this lane's copy
     const int sub = threadIdx.x % TPI;
-    const int s = R.p_off + (b - R.pp_blk_off) * PPB + threadIdx.x / TPI;
-    const bool have = s < R.p_off + R.n;
     // L / 2^32 as a hi + lo pair (a plain FP32 scale would bias every dx of
     // the replica by the same relative rounding)
     const double scd = R.L / 4294967296.0;
@@ -576,7 +568,7 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
 
     float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     double u = 0.0;
-    // PP_PRUNE keeps the warp converged for its ballots and shared staging:
+    // pruning keeps the warp converged for its ballots and shared staging:
     // every lane runs the warp's longest list, lanes past their own (or
     // without a particle) evaluating their own slot, which adds nothing
     if (have || PRUNE) {
@@ -586,8 +578,8 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
         const int nloop = PRUNE ? __reduce_max_sync(0xffffffffu, nr) : nr;
         // this lane's first chunk in the particle's group blocks
         const int *lg = nlist + (long long)(sv >> 5) * maxnb * 32 + (p32 * TPI + sub) * C;
-        int *buf = pstage + (threadIdx.x / TPI) * 32;    // PP_PRUNE staging
-        int fill = 0, blk = 0;                           // PP_PRUNE: staged entries, blocks written
+        const Stage<TPI> buf{stage_warp, (threadIdx.x & 31) / TPI};
+        int fill = 0, blk = 0;  // pruning: staged entries, blocks written
         int *og = PRUNE ? pa.nlist_in + (long long)(sv >> 5) * pa.maxnb_in * 32 + (p32 * TPI + sub) * C
                         : nullptr;
         for (int k0 = 0; k0 < nloop; k0 += STEP) {
@@ -612,7 +604,7 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
 #pragma unroll
             for (int v = 0; v < UNR; ++v) q[v] = xq[j[v]];
             float2 px = f2(0.f, 0.f), py = px, pz = px, pu = px;
-            unsigned keep = 0;  // PP_PRUNE: bit v = this lane's entry v goes to the inner list
+            unsigned keep = 0;  // pruning: bit v = this lane's entry v goes to the inner list
 #pragma unroll
             for (int v = 0; v < UNR; v += 2) {
                 unsigned k2 = 0;
@@ -686,6 +678,43 @@ k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq
         fz += __shfl_xor_sync(0xffffffffu, fz, o);
     }
     if (have && sub == 0) acc_out[s] = make_float4(fx, fy, fz, 0.f);
+    return u;
+}
+
+template <int TPI, int PM>
+__global__ void __launch_bounds__(PPL_THREADS, P3M_PP_MINB)
+k_pp_f32(const RepDev *__restrict__ reps, int nrep, const uint4 *__restrict__ xq,
+         const int *__restrict__ nnb, const int *__restrict__ nlist, int maxnb,
+         const float4 *__restrict__ tables, float4 *__restrict__ acc_out,
+         double *__restrict__ u_part, PruneArgs pa)
+{
+    constexpr int PPB = PPL_THREADS / TPI;  // particles per block
+    __shared__ double red[32];
+    __shared__ __align__(16) int pstage[PM == PP_DYN ? PPB * 32 : 1];  // 32 positions per particle
+    extern __shared__ __align__(16) float4 ppl_tab[];
+    const int b = blockIdx.x;
+    const int r = find_rep(b, nrep, [&](int k) { return reps[k].pp_blk_off; });
+    const RepDev &R = reps[r];
+    {
+        const float4 *src = tables + (long long)r * PP_TABLE_N;
+        for (int k = threadIdx.x; k < PP_TABLE_N * PP_TABLE_COPIES; k += PPL_THREADS)
+            cp_async16(ppl_tab + k, src + k / PP_TABLE_COPIES);
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    const float4 *tab = ppl_tab + (threadIdx.x & (PP_TABLE_COPIES - 1));  // this lane's copy
+    const int s = R.p_off + (b - R.pp_blk_off) * PPB + threadIdx.x / TPI;
+    const bool have = s < R.p_off + R.n;
+    int *stage_warp = pstage + (PM == PP_DYN ? (threadIdx.x >> 5) * 32 * (32 / TPI) : 0);
+    double u;
+    if constexpr (PM == PP_OUTER) {
+        u = pp_body<TPI, false>(R, s, have, xq, nnb, nlist, maxnb, tab, acc_out, pa, stage_warp);
+    } else if ((pa.rebuild[r] | pa.prune[r]) != 0) {  // block-uniform
+        u = pp_body<TPI, true>(R, s, have, xq, nnb, nlist, maxnb, tab, acc_out, pa, stage_warp);
+    } else {
+        u = pp_body<TPI, false>(R, s, have, xq, pa.nnb_in, pa.nlist_in, pa.maxnb_in, tab,
+                                acc_out, pa, stage_warp);
+    }
     const double ut = block_sum(u, red);
     if (threadIdx.x == 0) u_part[b] = ut;
 }
@@ -728,10 +757,8 @@ template <typename T> void configure_pp_kernels()
         auto set = [&](auto k) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tab); };
         set(k_pp_f32<1, PP_OUTER>); set(k_pp_f32<2, PP_OUTER>);
         set(k_pp_f32<4, PP_OUTER>); set(k_pp_f32<8, PP_OUTER>);
-        set(k_pp_f32<1, PP_INNER>); set(k_pp_f32<2, PP_INNER>);
-        set(k_pp_f32<4, PP_INNER>); set(k_pp_f32<8, PP_INNER>);
-        set(k_pp_f32<1, PP_PRUNE>); set(k_pp_f32<2, PP_PRUNE>);
-        set(k_pp_f32<4, PP_PRUNE>); set(k_pp_f32<8, PP_PRUNE>);
+        set(k_pp_f32<1, PP_DYN>); set(k_pp_f32<2, PP_DYN>);
+        set(k_pp_f32<4, PP_DYN>); set(k_pp_f32<8, PP_DYN>);
     }
 }
 
@@ -777,11 +804,8 @@ template <typename T, int TPI> static void launch_pp_tpi(const DevState &s, cuda
         pa.pos = s.pos;
         pa.pos_pref = s.pos_pref;
         pa.status = s.status;
-        k_pp_f32<TPI, PP_PRUNE><<<s.pp_nblk, PPL_THREADS, tab, st>>>(
+        k_pp_f32<TPI, PP_DYN><<<s.pp_nblk, PPL_THREADS, tab, st>>>(
             s.reps, s.nrep, (const uint4 *)s.xq, s.nnb, s.nlist, s.maxnb, s.pp_tables,
-            (float4 *)s.acc_pp, s.u_pp_part, pa);
-        k_pp_f32<TPI, PP_INNER><<<s.pp_nblk, PPL_THREADS, tab, st>>>(
-            s.reps, s.nrep, (const uint4 *)s.xq, s.nnb_in, s.nlist_in, s.maxnb_in, s.pp_tables,
             (float4 *)s.acc_pp, s.u_pp_part, pa);
     } else {
         k_pp_f64<TPI><<<s.pp_nblk, PPL_THREADS, 0, st>>>(s.reps, s.nrep, (const Q *)s.xq, s.nnb,
@@ -800,7 +824,7 @@ template <typename T> void launch_pp(const DevState &s, cudaStream_t st)
     }
 }
 
-int pp_kernel_count(const DevState &s) { return s.prune_buf > 0.0 ? 2 : 1; }
+int pp_kernel_count(const DevState &) { return 1; }
 
 void launch_reduce_pp(const DevState &s, cudaStream_t st)
 {
