@@ -508,15 +508,8 @@ __device__ __forceinline__ void x_r2c_item(const RepDev &R, int w, const T *__re
     const T *t = tiles + R.tile_off;
     T *dst = reinterpret_cast<T *>(&buf[brev(x, LOGM) * LSX]);
     __syncthreads();
-    // FP32: several rows' tile loads in flight per thread (the pass waits on them)
-    if constexpr (sizeof(T) == 4) {
-#pragma unroll 4
-        for (int j = threadIdx.x >> LOGM; j < NROW; j += FFT_THREADS >> LOGM)
-            dst[j] = rho_sum<T>(t, ax, axis_y(y0 + j, R.nb), az);  // line j/2, part j%2
-    } else {
-        for (int j = threadIdx.x >> LOGM; j < NROW; j += FFT_THREADS >> LOGM)
-            dst[j] = rho_sum<T>(t, ax, axis_y(y0 + j, R.nb), az);
-    }
+    for (int j = threadIdx.x >> LOGM; j < NROW; j += FFT_THREADS >> LOGM)
+        dst[j] = rho_sum<T>(t, ax, axis_y(y0 + j, R.nb), az);  // line j/2, part j%2
     __syncthreads();
     fft_lines_t<T, LOGM>(buf, 1, LSX, LNL, tw, false);
     // split the two real rows: Xa = (Z[k] + conj Z[M-k])/2, Xb = (Z[k] - conj Z[M-k])/2i
@@ -840,10 +833,7 @@ __device__ __forceinline__ void x_c2r_item(const RepDev &R, int comp, int w,
     const int z = w / NYT, y0 = (w % NYT) * NROW;
     const cplx<T> *src = ek + comp * nspec + R.spec_off + (long long)z * M + y0;
     __syncthreads();
-    // FP32: all of a thread's spectrum loads in flight at once (the pass
-    // waits on them)
     if constexpr (sizeof(T) == 4) {
-#pragma unroll
         for (int e = threadIdx.x; e < (NK << LNL); e += FFT_THREADS) {
             const int l = e & ((1 << LNL) - 1), k = e >> LNL;
             const long long o = (long long)k * M * M + 2 * l;
@@ -870,7 +860,7 @@ __device__ __forceinline__ void x_c2r_item(const RepDev &R, int comp, int w,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(FFT_THREADS, sizeof(T) == 4 ? 4 : 3)
+__global__ void __launch_bounds__(FFT_THREADS)
 k_fft_x_c2r(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict__ ek,
             long long nspec, T *__restrict__ efield, long long nmesh,
             const cplx<T> *__restrict__ twg, int nitems_per_comp)
