@@ -310,9 +310,6 @@ k_assign(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ bric
 // value is (hi + lo / 2^fb) / S, resolved to 2^-fb / S. fb = 16, or fewer for
 // bricks of more than 2^14 particles, so that the n fractions of a node (each
 // at most 2^fb) cannot overflow: n 2^fb <= 2^30.
-#ifndef P3M_ASSIGN_ATOM64
-#define P3M_ASSIGN_ATOM64 0
-#endif
 constexpr int A32_THREADS = 256;
 constexpr float kRound = 12582912.0f;  // 1.5 * 2^23
 constexpr int kRoundBits = 0x4B400000;
@@ -418,13 +415,8 @@ k_assign_i32(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ 
                         const int hi = __float_as_int(hb) - kRoundBits;
                         const float frac = t - (hb - kRound);         // in [0, 1], exact
                         const int lo = __float_as_int(frac * F + kRound) - kRoundBits;
-#if P3M_ASSIGN_ATOM64
-                        atomicAdd(reinterpret_cast<unsigned long long *>(a32_smem) + row + c,
-                                  (unsigned long long)((long long)hi * (1LL << fb) + lo));
-#else
                         atomicAdd(thi + row + c, hi);
                         atomicAdd(tlo + row + c, lo);
-#endif
                     }
                 }
             }
@@ -433,14 +425,8 @@ k_assign_i32(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ 
         float *dst = tiles + R.tile_off + (long long)local * TILE3;
         const double inv = 1.0 / (double)S;
         const double invF = 1.0 / (double)F;  // exact: F is a power of two
-#if P3M_ASSIGN_ATOM64
-        for (int k = threadIdx.x; k < TILE3; k += A32_THREADS)
-            dst[k] = (float)((double)(long long)reinterpret_cast<unsigned long long *>(a32_smem)[k] *
-                             invF * inv);
-#else
         for (int k = threadIdx.x; k < TILE3; k += A32_THREADS)
             dst[k] = (float)(((double)thi[k] + (double)tlo[k] * invF) * inv);
-#endif
     }
 }
 
