@@ -801,11 +801,6 @@ k_fft_plane(const RepDev *__restrict__ reps, int nrep, const cplx<T> *__restrict
     }
 }
 
-// Pass E: C2R along x of the three field spectra, written as real meshes
-// efield[c][z][y][x]. Item = (replica, component, z, tile of 2 x_lines rows); rows
-// 2l and 2l+1 share complex line l: Z[k] = Xa[k] + i Xb[k] over the
-// Hermitian extension, with the imaginary parts at k = 0 and M/2 dropped.
-// Instantiated per mesh side like pass A.
 // Two adjacent spectrum rows a, b of line l, wavenumber k, packed into the
 // complex line of an inverse transform whose real and imaginary parts come
 // out as the two real rows (k and M - k from Hermitian symmetry).
@@ -821,6 +816,11 @@ __device__ __forceinline__ void c2r_split(cplx<T> *buf, int k, int l, cplx<T> a,
     }
 }
 
+// Pass E: C2R along x of the three field spectra, written as real meshes
+// efield[c][z][y][x]. Item = (replica, component, z, tile of 2 x_lines rows); rows
+// 2l and 2l+1 share complex line l: Z[k] = Xa[k] + i Xb[k] over the
+// Hermitian extension, with the imaginary parts at k = 0 and M/2 dropped.
+// Instantiated per mesh side like pass A.
 template <typename T, int LOGM>
 __device__ __forceinline__ void x_c2r_item(const RepDev &R, int comp, int w,
                                            const cplx<T> *__restrict__ ek, long long nspec,
