@@ -13,6 +13,8 @@ CPU restatement of the reference's algorithm). For a workload of
   over ``drift_steps`` NVE steps relative to |E(0)| and to the kinetic
   energy (E(0) nears zero in weakly coupled replicas), and the drift proper,
   the least-squares slope of E(t) times the run length over |E(0)|;
+* the FP32 path runs with the kernel shapes the autotuner installs on the
+  equilibrated ensemble (inner lists included), as the benchmark does;
 * for the ensemble with n(q,t) (cfg3): S(q, w) of the FP32 and the FP64
   ensembles, both from their own trajectories (which part after a few hundred
   steps: the comparison is statistical), the frequency and height of the peak
@@ -102,7 +104,7 @@ def _bootstrap_peaks(S_rep, dw, n_boot=400, seed=0):
 
 
 def validate(workload="cfg1", equil=1000, traj_steps=1000, drift_steps=10000, sqw_steps=4096,
-             quench=200, device=0, fp64_drift=True):
+             quench=200, device=0, fp64_drift=True, tune=True):
     reps = WORKLOADS[workload]()
     offs = np.cumsum([0] + [r.N for r in reps])
     res = {"workload": workload, "replicas": len(reps), "particles": int(offs[-1]),
@@ -115,6 +117,13 @@ def validate(workload="cfg1", equil=1000, traj_steps=1000, drift_steps=10000, sq
         c64.init_forces()
         c64.equilibrate(equil, quench_steps=quench)
         pos_eq, vel_eq, _ = c64.get_state_all()
+        if tune:  # the FP32 kernel shapes the benchmark would install
+            from .autotune import tune as _tune
+
+            c32.set_state_all(pos_eq, vel_eq)
+            c32.init_forces()
+            _tune(c32, use_cache=False)
+        res["fp32_tuning"] = c32.tuning()
         # force error along the FP64 trajectory
         samples = []
         for k in range(0, traj_steps + 1, 100):
@@ -185,9 +194,11 @@ def main(argv=None):
     ap.add_argument("--sqw-steps", type=int, default=4096)
     ap.add_argument("--quench", type=int, default=200)
     ap.add_argument("--no-fp64-drift", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the FP32 context's default kernel shapes instead of autotuning")
     a = ap.parse_args(argv)
     print(json.dumps(validate(a.workload, a.equil, a.traj_steps, a.drift_steps, a.sqw_steps,
-                              a.quench, fp64_drift=not a.no_fp64_drift)))
+                              a.quench, fp64_drift=not a.no_fp64_drift, tune=not a.no_tune)))
 
 
 if __name__ == "__main__":
