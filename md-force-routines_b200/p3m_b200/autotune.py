@@ -34,7 +34,7 @@ from ._lib import FP32, MODE_NVE, P3MError
 
 CANDIDATES = [(tpi, skin) for tpi in (1, 2, 4) for skin in (0.5, 0.8, 1.1, 1.4)]
 #: FP32 inner-list buffers, each tried with the best skin so far and larger ones
-PRUNE_BUFS = (0.15, 0.25)
+PRUNE_BUFS = (0.2, 0.3)
 PRUNE_SKINS = (1.1, 1.4)
 CACHE = os.environ.get("P3M_B200_TUNE_CACHE",
                        os.path.join(os.path.expanduser("~"), ".cache", "p3m_b200", "autotune.json"))

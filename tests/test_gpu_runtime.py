@@ -386,7 +386,7 @@ def test_autotune_installs_a_finalist():
         assert res["prune_trials"] >= 2
         assert len(res["ms_per_step"]) == 3 + 1 + 1 + 2 + res["prune_trials"]
         assert len(res["final_ms_per_step"]) == 2
-        assert any(k.endswith("prune0.15") for k in res["ms_per_step"])
+        assert any(k.endswith("prune0.2") for k in res["ms_per_step"])
         best = min(res["final_ms_per_step"], key=res["final_ms_per_step"].get)
         assert best in res["ms_per_step"]
         assert c.tuning() == res["choice"]
