@@ -629,20 +629,19 @@ template <typename T> static int seq_force(p3m_ctx *ctx, bool keys)
 }
 
 // One integrator step of every replica (mode 0 NVE, 1 thermostat). After the
-// drift and the key scan the step forks: the mesh branch (brick sort,
-// assignment, FFTs, gather) runs on a second stream and the n(q,t) sums of the
-// new positions on a third, while the particle branch (cell sort, lists, PP)
-// runs on the first -- they share no arrays -- and they join before the
-// forces are combined, so the latency-bound mesh kernels fill the SMs the PP
-// kernel leaves idle (one graph holds all branches).
+// drift (which keys the particles' bricks) the step forks: the mesh branch
+// (brick scan and sort, assignment, FFTs, gather) runs on a second stream and
+// the n(q,t) sums of the new positions on a third, while the particle branch
+// (cell keys and scan, cell sort, lists, PP) runs on the first -- they share
+// no arrays -- and they join before the forces are combined, so the
+// latency-bound kernels of each branch fill the SMs the others leave idle
+// (one graph holds all branches).
 template <typename T> static int seq_step(p3m_ctx *ctx, int mode, int record_nqt)
 {
     DevState &s = ctx->s;
     cudaStream_t st = ctx->st, st2 = ctx->st2;
     launch_kick_drift(s, st);
-    launch_cell_keys(s, st);
-    launch_scan(s, st);
-    ctx->launches += 3;
+    ctx->launches++;
     const int rec = (record_nqt && ctx->nq > 0) ? 1 : 0;
     const bool fork = s.has_mesh || rec;
     cudaError_t e = cudaSuccess;
@@ -651,8 +650,9 @@ template <typename T> static int seq_step(p3m_ctx *ctx, int mode, int record_nqt
         if (e == cudaSuccess && s.has_mesh) {
             e = cudaStreamWaitEvent(st2, ctx->ev_fork, 0);
             if (e == cudaSuccess) {
+                launch_scan(s, st2, 1);
                 launch_sort_bricks(s, st2);
-                ctx->launches += 3;
+                ctx->launches += 4;
                 seq_pm<T>(ctx, false, st2);
                 e = cudaEventRecord(ctx->ev_join, st2);
             }
@@ -668,11 +668,13 @@ template <typename T> static int seq_step(p3m_ctx *ctx, int mode, int record_nqt
             }
         }
     }
+    launch_cell_keys(s, st);
+    launch_scan(s, st, s.has_mesh ? 0 : -1);  // without a mesh branch: the bricks here too
     launch_scatter(s, st);
     launch_fix_cells<T>(s, st);
     launch_quantize<T>(s, st);     // sorted coordinates of this step
     launch_build_lists<T>(s, st);  // from those coordinates (rebuild steps)
-    ctx->launches += 4;
+    ctx->launches += 6;
     seq_pp<T>(ctx, false, st);
     if (e == cudaSuccess && s.has_mesh) e = cudaStreamWaitEvent(st, ctx->ev_join, 0);
     if (e == cudaSuccess && rec) e = cudaStreamWaitEvent(st, ctx->ev_join3, 0);

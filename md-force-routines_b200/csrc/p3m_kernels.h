@@ -84,7 +84,7 @@ template <typename T> void configure_pp_kernels();
 template <typename T> void configure_mesh_kernels();
 template <typename T> void launch_keys(const DevState &s, cudaStream_t st);
 void launch_cell_keys(const DevState &s, cudaStream_t st);
-void launch_scan(const DevState &s, cudaStream_t st);
+void launch_scan(const DevState &s, cudaStream_t st, int part = -1);  // -1 both, 0 cells, 1 bricks
 void launch_scatter(const DevState &s, cudaStream_t st);
 template <typename T> void launch_fix_cells(const DevState &s, cudaStream_t st);
 void launch_sort_bricks(const DevState &s, cudaStream_t st);  // 3 kernels

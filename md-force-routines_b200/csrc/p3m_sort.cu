@@ -110,10 +110,10 @@ __device__ void block_scan_array(int *count, int *start, int *cursor, int n, int
 __global__ void k_scan(const RepDev *__restrict__ reps, int nrep, int *cell_count,
                        int *cell_start, int *cell_cursor, int *brick_count, int *brick_start,
                        int *brick_cursor, int nbrick, const int *__restrict__ rebuild,
-                       int *__restrict__ rb_list)
+                       int *__restrict__ rb_list, int first_part)
 {
     __shared__ int sm[64];
-    if (blockIdx.x == 0) {
+    if (blockIdx.x + first_part == 0) {
         int k = 0, cells = 0;
         for (int r = 0; r < nrep; ++r) {
             if (!rebuild[r]) continue;
@@ -303,11 +303,14 @@ void launch_cell_keys(const DevState &s, cudaStream_t st)
                                                        s.status);
 }
 
-void launch_scan(const DevState &s, cudaStream_t st)
+// Both scans (block 0: the cells of the rebuilding replicas, block 1: the
+// bricks), or one of them: part 0 / 1.
+void launch_scan(const DevState &s, cudaStream_t st, int part)
 {
-    k_scan<<<2, 1024, 0, st>>>(s.reps, s.nrep, s.cell_count, s.cell_start, s.cell_cursor,
-                               s.brick_count, s.brick_start, s.brick_cursor,
-                               s.has_mesh ? s.nbrick : 0, s.rebuild, s.rb_list);
+    const int first = part == 1 ? 1 : 0, nblocks = part < 0 ? 2 : 1;
+    k_scan<<<nblocks, 1024, 0, st>>>(s.reps, s.nrep, s.cell_count, s.cell_start, s.cell_cursor,
+                                     s.brick_count, s.brick_start, s.brick_cursor,
+                                     s.has_mesh ? s.nbrick : 0, s.rebuild, s.rb_list, first);
 }
 
 void launch_scatter(const DevState &s, cudaStream_t st)
