@@ -20,7 +20,7 @@ What it searches (p3m_tuning of the C ABI):
 The list cells, FFT tiles and gather are searched one at a time from the
 best PP setting (coordinate descent), then inner-list buffers with a few
 skins from the best of those; then the fastest few settings are timed again over
-twice the steps (list rebuilds come every few tens of steps, so short runs
+four times the steps (list rebuilds come every few tens of steps, so short runs
 rank close candidates by chance) and the fastest is installed. The state
 should already be equilibrated: each timing advances the system. Results are
 cached per workload signature in a JSON file.
@@ -142,7 +142,7 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
             n_prune += 1
     final = {}
     for k in sorted(times, key=times.get)[:max(1, finalists)]:
-        final[k] = timed(settings[k], 2 * steps)
+        final[k] = timed(settings[k], 4 * steps)
     win = min(final, key=final.get)
     choice = settings[win]
     ctx.set_tuning(**choice)
