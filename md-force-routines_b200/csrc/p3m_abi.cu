@@ -253,7 +253,7 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
                     s.cell_start, s.cell_cursor, s.cell_tmp, s.cell_perm, s.cell_slot, s.xq, s.nnb,
                     s.cell_sub,
                     s.nlist, s.rebuild, s.rb_list, s.pos_ref, s.pp_tables,
-                    s.nnb_in, s.nlist_in, s.prune, s.pos_pref, s.prune_count, s.kf_done,
+                    s.nnb_in, s.nlist_in, s.prune, s.pos_pref, s.prune_count,
                     s.acc_pp, s.brick_key, s.brick_count, s.brick_start, s.brick_cursor,
                     s.brick_perm, s.brick_slot, s.brick_hist, s.tiles, s.spec, s.ek, s.green, s.efield,
                     s.acc_pm, s.twiddle, s.u_pp_part, s.u_pm_part, s.kin_part, s.rep_out,
@@ -496,7 +496,6 @@ extern "C" int p3m_create(const p3m_replica_desc *reps, int n_reps, int precisio
     CKC(dalloc(&s.nnb_in, (size_t)p));
     CKC(dalloc(&s.pos_pref, (size_t)3 * p));
     CKC(dalloc(&s.prune_count, (size_t)n_reps));
-    CKC(dalloc(&s.kf_done, 1));
     CKC(dalloc(&s.cell_tmp, (size_t)p));
     CKC(dalloc(&s.cell_perm, (size_t)p));
     CKC(dalloc(&s.cell_slot, (size_t)p));
@@ -679,15 +678,16 @@ template <typename T> static int seq_step(p3m_ctx *ctx, int mode, int record_nqt
     seq_pp<T>(ctx, false, st);
     if (e == cudaSuccess && s.has_mesh) e = cudaStreamWaitEvent(st, ctx->ev_join, 0);
     if (e == cudaSuccess && rec) e = cudaStreamWaitEvent(st, ctx->ev_join3, 0);
+    launch_kick_finish<T>(s, 1, nullptr, st);
+    ctx->launches++;
     StepSums sums;  // the energy sums, in the reduction (the n(q,t) row is summed on its branch)
     sums.u_pp_part = s.u_pp_part;
     sums.pp_nblk = s.pp_nblk;
     sums.u_pm_part = s.u_pm_part;
     sums.wc_total = s.wc;
     sums.wp_total = s.wp;
-    // the second half kick, with the step's reduction in its last block
-    launch_kick_finish_reduce<T>(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, st, rec,
-                                 ctx->snap_interval, ctx->snap_cap, sums);
+    launch_step_reduce(s, mode, ctx->counters, ctx->ring, ctx->ring_cap, st, rec,
+                       ctx->snap_interval, ctx->snap_cap, sums);
     ctx->launches++;
     if (mode == P3M_MODE_THERMOSTAT) {
         launch_scale_vel(s, st);

@@ -83,21 +83,17 @@ __device__ __forceinline__ int block_replica(const RepDev *reps, int nrep, int b
     return find_rep(b, nrep, [&](int k) { return reps[k].blk_off; });
 }
 
-__device__ void step_reduce_body(const StepReduceArgs &a);
-
 // acc = af (a_pp + Z E) for every particle; with do_kick the second half kick
-// and the per-block FP64 sum of v^2; with `done`, the step's reduction too.
+// and the per-block FP64 sum of v^2.
 template <typename T>
 __global__ void __launch_bounds__(PBLK)
 k_kick_finish(const RepDev *__restrict__ reps, int nrep, const int *__restrict__ cell_slot,
               const int *__restrict__ brick_slot, const typename V4<T>::t *__restrict__ acc_pp,
               const typename V4<T>::t *__restrict__ acc_pm, int has_mesh,
               double *__restrict__ acc, double *__restrict__ vel, double *__restrict__ kin_part,
-              int do_kick, double *__restrict__ ep_out, int *status,
-              unsigned *__restrict__ done, StepReduceArgs sr)
+              int do_kick, double *__restrict__ ep_out, int *status)
 {
     __shared__ double red[32];
-    __shared__ bool last;
     const int b = blockIdx.x;
     const int r = block_replica(reps, nrep, b);
     const RepDev &R = reps[r];
@@ -134,36 +130,18 @@ k_kick_finish(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
     }
     const double t = block_sum(kin, red);
     if (threadIdx.x == 0) kin_part[b] = t;
-    if (!done) return;
-    // with the step's reduction: the block that finishes last runs it (its
-    // partials and every other block's are out: fence, then count)
-    if (threadIdx.x == 0) {
-        __threadfence();
-        last = atomicAdd(done, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    step_reduce_body(sr);
-    if (threadIdx.x == 0) *done = 0;  // for the next launch
 }
 
 // Per replica: energies, temperature and the thermostat factor; one row of
 // the energy ring; step counter advance. mode: 0 NVE, 1 thermostat, 2 force
-// only (no kinetic terms). One block: k_step_reduce, or the last block of
-// k_kick_finish to finish (the partials read past L1: other blocks wrote them).
-__device__ void step_reduce_body(const StepReduceArgs &a)
+// only (no kinetic terms). Single block.
+__global__ void k_step_reduce(const RepDev *__restrict__ reps, int nrep, int nblk,
+                              const double *__restrict__ kin_part, double *__restrict__ rep_out,
+                              int mode, int *__restrict__ counters, double *__restrict__ ring,
+                              int ring_cap, int recorded, int snap_interval, int snap_cap,
+                              int *rebuild, int *status, StepSums sums, int *prune,
+                              double *prune_count)
 {
-    const RepDev *__restrict__ reps = a.reps;
-    const int nrep = a.nrep, nblk = a.nblk, mode = a.mode, ring_cap = a.ring_cap;
-    const double *__restrict__ kin_part = a.kin_part;
-    double *__restrict__ rep_out = a.rep_out;
-    int *__restrict__ counters = a.counters;
-    double *__restrict__ ring = a.ring;
-    const int recorded = a.recorded, snap_interval = a.snap_interval, snap_cap = a.snap_cap;
-    int *rebuild = a.rebuild, *status = a.status, *prune = a.prune;
-    double *prune_count = a.prune_count;
-    const StepSums &sums = a.sums;
     // counters: [0] steps since the run started, [1] energy-ring position,
     // [2] step index of the run's first step (thermostat_p3m_ord6.py:15 tests
     // it <= 1999), [3] n(q,t) rows recorded, [4] snapshots taken, [5] the
@@ -195,7 +173,7 @@ __device__ void step_reduce_body(const StepReduceArgs &a)
         }
         const int b0 = R.blk_off, b1 = (r + 1 < nrep) ? reps[r + 1].blk_off : nblk;
         double s = 0.0;
-        for (int k = b0 + lane; k < b1; k += 32) s += __ldcg(kin_part + k);
+        for (int k = b0 + lane; k < b1; k += 32) s += kin_part[k];
         s = warp_sum(s);
         if (lane == 0) {
             double *o = rep_out + 8 * r;
@@ -250,8 +228,6 @@ __device__ void step_reduce_body(const StepReduceArgs &a)
         rebuild[r] = 0;
     }
 }
-
-__global__ void k_step_reduce(StepReduceArgs a) { step_reduce_body(a); }
 
 // The state after this step, [slot][particle][pos, vel, acc] (the rows of
 // yukawa_MD_p3m_ord6.py:223), into the slot k_step_reduce chose; steps[slot]
@@ -602,53 +578,17 @@ void launch_kick_finish(const DevState &s, int do_kick, double *ep_out, cudaStre
     k_kick_finish<T><<<s.nblk, PBLK, 0, st>>>(s.reps, s.nrep, s.cell_slot, s.brick_slot,
                                               (const T4 *)s.acc_pp, (const T4 *)s.acc_pm,
                                               s.has_mesh, s.acc, s.vel, s.kin_part, do_kick,
-                                              ep_out, s.status, nullptr, StepReduceArgs());
-}
-
-static StepReduceArgs step_reduce_args(const DevState &s, int mode, int *counters, double *ring,
-                                       int ring_cap, int recorded, int snap_interval,
-                                       int snap_cap, const StepSums &sums)
-{
-    StepReduceArgs a;
-    a.reps = s.reps;
-    a.nrep = s.nrep;
-    a.nblk = s.nblk;
-    a.kin_part = s.kin_part;
-    a.rep_out = s.rep_out;
-    a.mode = mode;
-    a.counters = counters;
-    a.ring = ring;
-    a.ring_cap = ring_cap;
-    a.recorded = recorded;
-    a.snap_interval = snap_interval;
-    a.snap_cap = snap_cap;
-    a.rebuild = s.rebuild;
-    a.status = s.status;
-    a.sums = sums;
-    a.prune = s.prune_buf > 0.0 ? s.prune : nullptr;
-    a.prune_count = s.prune_count;
-    return a;
-}
-
-template <typename T>
-void launch_kick_finish_reduce(const DevState &s, int mode, int *counters, double *ring,
-                               int ring_cap, cudaStream_t st, int recorded, int snap_interval,
-                               int snap_cap, const StepSums &sums)
-{
-    using T4 = typename V4<T>::t;
-    k_kick_finish<T><<<s.nblk, PBLK, 0, st>>>(
-        s.reps, s.nrep, s.cell_slot, s.brick_slot, (const T4 *)s.acc_pp, (const T4 *)s.acc_pm,
-        s.has_mesh, s.acc, s.vel, s.kin_part, 1, nullptr, s.status, s.kf_done,
-        step_reduce_args(s, mode, counters, ring, ring_cap, recorded, snap_interval, snap_cap,
-                         sums));
+                                              ep_out, s.status);
 }
 
 void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring, int ring_cap,
                         cudaStream_t st, int recorded, int snap_interval, int snap_cap,
                         const StepSums &sums)
 {
-    k_step_reduce<<<1, 1024, 0, st>>>(step_reduce_args(s, mode, counters, ring, ring_cap,
-                                                       recorded, snap_interval, snap_cap, sums));
+    k_step_reduce<<<1, 1024, 0, st>>>(s.reps, s.nrep, s.nblk, s.kin_part, s.rep_out, mode,
+                                      counters, ring, ring_cap, recorded, snap_interval, snap_cap,
+                                      s.rebuild, s.status, sums,
+                                      s.prune_buf > 0.0 ? s.prune : nullptr, s.prune_count);
 }
 
 void launch_snapshot(const DevState &s, const int *counters, double *snap, int *steps,
@@ -713,8 +653,6 @@ int gf_opt_blocks(int M) { return (int)(((long long)M * M * M + 255) / 256); }
 
 #define P3M_INST(T)                                                                             \
     template void launch_kick_finish<T>(const DevState &, int, double *, cudaStream_t);          \
-    template void launch_kick_finish_reduce<T>(const DevState &, int, int *, double *, int,      \
-                                               cudaStream_t, int, int, int, const StepSums &);   \
     template void launch_nqt<T>(const DevState &, const double *, const double *, int, int,      \
                                 double *, double *, const int *, int, cudaStream_t);            \
     template void configure_integrate_kernels<T>(int);                                          \

@@ -53,7 +53,6 @@ struct DevState {
     int *prune = nullptr;        // per-replica flags: rebuild the inner lists this step
     double *pos_pref = nullptr;  // positions at the last inner-list build (ntot,3)
     double *prune_count = nullptr;  // per replica: inner-list builds between outer rebuilds
-    unsigned *kf_done = nullptr;    // blocks of the fused kick-finish + reduction done (reset to 0)
     float4 *pp_tables = nullptr; // FP32 pair tables: cubic of psi = phi r, [nrep][PP_TABLE_N]
     void *acc_pp = nullptr;      // V4<T> PP acceleration, cell-sorted order
     // brick sort
@@ -126,25 +125,6 @@ struct StepSums {
     const double *u_pm_part = nullptr;
     int wc_total = 0, wp_total = 0;
 };
-// Everything the step reduction reads and writes (see launch_step_reduce).
-struct StepReduceArgs {
-    const RepDev *reps = nullptr;
-    int nrep = 0, nblk = 0;
-    const double *kin_part = nullptr;
-    double *rep_out = nullptr;
-    int mode = 0;
-    int *counters = nullptr;
-    double *ring = nullptr;
-    int ring_cap = 0, recorded = 0, snap_interval = 0, snap_cap = 0;
-    int *rebuild = nullptr, *status = nullptr, *prune = nullptr;
-    double *prune_count = nullptr;
-    StepSums sums;
-};
-// k_kick_finish with the step's reduction run by its last block (one launch)
-template <typename T>
-void launch_kick_finish_reduce(const DevState &s, int mode, int *counters, double *ring,
-                               int ring_cap, cudaStream_t st, int recorded, int snap_interval,
-                               int snap_cap, const StepSums &sums);
 void launch_step_reduce(const DevState &s, int mode, int *counters, double *ring, int ring_cap,
                         cudaStream_t st, int recorded = 0, int snap_interval = 0,
                         int snap_cap = 0, const StepSums &sums = StepSums());
