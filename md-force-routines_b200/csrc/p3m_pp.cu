@@ -578,7 +578,7 @@ __device__ __forceinline__ double pp_body(const RepDev &R, int s, bool have,
         const int nloop = PRUNE ? __reduce_max_sync(0xffffffffu, nr) : nr;
         // this lane's first chunk in the particle's group blocks
         const int *lg = nlist + (long long)(sv >> 5) * maxnb * 32 + (p32 * TPI + sub) * C;
-        const Stage<TPI> buf{stage_warp, (threadIdx.x & 31) / TPI};
+        const Stage<TPI> buf{stage_warp, (int)(threadIdx.x & 31) / TPI};
         int fill = 0, blk = 0;  // pruning: staged entries, blocks written
         int *og = PRUNE ? pa.nlist_in + (long long)(sv >> 5) * pa.maxnb_in * 32 + (p32 * TPI + sub) * C
                         : nullptr;
