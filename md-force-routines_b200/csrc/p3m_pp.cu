@@ -398,6 +398,7 @@ k_pp_f64(const RepDev *__restrict__ reps, int nrep, const ulonglong4 *__restrict
 #ifndef P3M_PP_PACK
 #define P3M_PP_PACK 0
 #endif
+
 // Copies of the pair table in shared memory. A warp's 128-bit table reads go
 // through the banks eight lanes at a time; with random intervals two of
 // those lanes often hit the same bank group (8.4 wavefronts per read measured
@@ -465,7 +466,19 @@ __device__ __forceinline__ void pair_table2(const uint4 &xi, const uint4 &qa, co
     const int ib = min(__float_as_int(tb.y) - 0x4B400000, PP_TABLE_N - 1);
     const float2 fl = v_add<P>(tb, f2(-kMagic, -kMagic));       // the interval index, exact
     const float2 u = v_fma<P>(fl, f2(-1.f, -1.f), t);            // t - fl, exact
-    const float4 ca = tab[ia * PP_TABLE_COPIES], cb = tab[ib * PP_TABLE_COPIES];
+    // reading the inner lists, entries beyond rc and list padding (masked
+    // below) skip their table read: fewer shared-memory wavefronts in the
+    // L1-bound loop (0.146 against 0.150 ms at cfg3). Over the Verlet lists
+    // of a list-building pass the predication cost more than it saved.
+    float4 ca, cb;
+    if constexpr (KEEP) {
+        ca = tab[ia * PP_TABLE_COPIES];
+        cb = tab[ib * PP_TABLE_COPIES];
+    } else {
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        ca = m.x != 0.f ? tab[ia * PP_TABLE_COPIES] : z4;
+        cb = m.y != 0.f ? tab[ib * PP_TABLE_COPIES] : z4;
+    }
     const float2 c0 = f2(ca.x, cb.x), c1 = f2(ca.y, cb.y), c2 = f2(ca.z, cb.z), c3 = f2(ca.w, cb.w);
     const float2 ps = v_fma<P>(v_fma<P>(v_fma<P>(c3, u, c2), u, c1), u, c0);
     const float2 dps = v_fma<P>(v_fma<P>(v_mul<P>(c3, f2(3.f, 3.f)), u, v_add<P>(c2, c2)), u, c1);
