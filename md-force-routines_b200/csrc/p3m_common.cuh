@@ -21,14 +21,19 @@ constexpr int PENCIL = 16;
 constexpr int LOG_PENCIL = 4;
 static_assert(PENCIL == 1 << LOG_PENCIL, "PENCIL is 2^LOG_PENCIL");
 // Complex lines per item of the x passes (two real rows each): 32, or M/2 for
-// M = 32, so each radix pass has a group for every one of 256 threads.
+// M = 32, so each radix pass has a group for every one of 256 threads; 16 at
+// M = 256, where the shorter items balance the last wave (FFT 0.576 against
+// 0.587 ms at 256^3; at 64^3 16 lines measured 0.144 against 0.130).
 constexpr int XL_MAX = 32;
 // PP cells are at least (rc + skin) / D wide (D, the cell divisor of a
 // context: 1 or 2), so the neighbours of a particle lie in the (2 D + 1)^3
 // cells around its own.
 constexpr int CELL_DIV_MAX = 2;
 __host__ __device__ constexpr int cell_stencil(int d) { return (2 * d + 1) * (2 * d + 1) * (2 * d + 1); }
-__host__ __device__ constexpr int x_lines_log(int logM) { return logM - 1 < 5 ? logM - 1 : 5; }
+__host__ __device__ constexpr int x_lines_log(int logM)
+{
+    return logM >= 8 ? 4 : (logM - 1 < 5 ? logM - 1 : 5);
+}
 constexpr int MAX_LOGM = 8;  // M <= 256
 constexpr int PBLK = 256;      // particles per block in replica-aligned particle kernels
 
