@@ -146,3 +146,36 @@ def test_uneven_batch_each_replica_against_its_oracle():
                 else:
                     assert rel_rms(a, ao) <= 1e-5, (r.M, rel_rms(a, ao))
                     assert abs(st["U"] - Uo) < 1e-6 * abs(parts_o[0])
+
+
+def test_ensemble_inner_lists_at_config_size():
+    """The 20 x 1e4 ensemble (64^3) with the tuned shapes (skin 1.4, inner
+    lists at r_c + 0.3): after 200 NVE steps with inner-list builds between
+    the Verlet rebuilds, the last step's accelerations and short-range
+    energies equal a fresh evaluation over the Verlet lists at the same
+    positions, to FP32 rounding (1e-6 of the RMS acceleration)."""
+    from p3m_b200 import FP32, MODE_NVE, Context
+    from p3m_b200.configs import cfg3
+
+    reps = cfg3()
+    P, V = zip(*(_state(r.N, r.L, r.T_desired, r.seed) for r in reps))
+    pos, vel = np.concatenate(P), np.concatenate(V)
+    with Context(reps, precision=FP32) as c:
+        c.set_state_all(pos, vel)
+        c.init_forces()
+        c.equilibrate(100, quench_steps=100)
+        c.set_tuning(pp_tpi=2, skin=1.4, prune_buf=0.3)
+        c.run(200, MODE_NVE)
+        builds = sum(c.inner_builds(i) for i in range(len(reps)))
+        st = c.get_state_all()
+        U = [c.replica_stats(i)["U_short"] for i in range(len(reps))]
+    assert builds >= len(reps)
+    with Context(reps, precision=FP32) as c:
+        c.set_tuning(pp_tpi=2, skin=1.4)
+        c.set_state_all(st[0], st[1])
+        c.init_forces()
+        acc = c.get_state_all()[2]
+        U0 = [c.replica_stats(i)["U_short"] for i in range(len(reps))]
+    assert rel_rms(st[2], acc) < 1e-6
+    for a, b in zip(U, U0):
+        assert a == pytest.approx(b, rel=1e-6)
