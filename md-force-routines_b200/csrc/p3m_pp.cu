@@ -639,6 +639,17 @@ __device__ __forceinline__ double pp_body(const RepDev &R, int s, bool have,
                 unsigned mask = 0;
                 if constexpr (TPI == 1) {
                     mask = keep;
+                } else if constexpr (TPI == 2) {
+                    // the partner's 8 bits by one shuffle, both spread to
+                    // alternate bits (entry 2 v + sub)
+                    const unsigned other = __shfl_xor_sync(0xffffffffu, keep, 1);
+                    auto spread = [](unsigned x) {
+                        x = (x | (x << 4)) & 0x0F0Fu;
+                        x = (x | (x << 2)) & 0x3333u;
+                        return (x | (x << 1)) & 0x5555u;
+                    };
+                    const unsigned k0 = sub ? other : keep, k1 = sub ? keep : other;
+                    mask = spread(k0) | (spread(k1) << 1);
                 } else {
 #pragma unroll
                     for (int v = 0; v < UNR; ++v) {
