@@ -121,7 +121,7 @@ constexpr int LB_THREADS = 256;
 constexpr int LB_TPI = 16;                    // lanes per particle
 constexpr int LB_PPB = LB_THREADS / LB_TPI;   // particles per pass
 constexpr int LB_HC = 256;                    // home particles per chunk
-template <typename T> __host__ __device__ constexpr int lb_scap() { return sizeof(T) == 4 ? 1024 : 512; }
+constexpr int LB_SCAP = 1024;                 // candidates staged per window (16 KB)
 static_assert(cell_stencil(CELL_DIV_MAX) <= LB_THREADS, "one thread per stencil cell");
 static_assert(LB_TPI >= PP_LIST_PAD, "one pad entry per lane at most");
 
@@ -129,8 +129,15 @@ static_assert(LB_TPI >= PP_LIST_PAD, "one pad entry per lane at most");
 // wrote); cells are (rc + skin)/D wide (about 10 particles at D = 2 and unit
 // density 3/(4 pi), 80 at D = 1). The (2D+1)^3 neighbour cells'
 // coordinates are staged in shared memory in the fixed stencil order (x
-// fastest, offsets -D .. D), a window of SCAP candidates at a time; the
-// LB_TPI lanes of a particle test LB_TPI consecutive candidates per round,
+// fastest, offsets -D .. D), a window of LB_SCAP candidates at a time, as
+// FP32 offsets from the home cell's centre: the wrap-around integer
+// difference, exact, then one rounding. A home particle lies within half a
+// cell of the centre and a candidate in range within rc + skin <= D cells of
+// it, so both offsets are minimum images (at most (D + 1/2) L / nc <= L/2,
+// nc >= 3 D) and their difference is the pair's separation; a test is three
+// subtractions and the squared length, against a cutoff with a 1e-5
+// relative margin over the rounding, so the list holds every pair within
+// rc + skin. The LB_TPI lanes of a particle test LB_TPI consecutive candidates per round,
 // and a warp ballot gives each candidate in range its place: the list holds
 // the in-range candidates in stencil order, as a scan by one thread would,
 // then the particle's own index up to a whole block of PP_LIST_PAD entries.
@@ -143,11 +150,12 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
 {
     constexpr int lt = LT;  // the list layout of the pair kernel's TPI = 2^LT
     using Q = typename Coord<T>::Q;
-    constexpr int SCAP = lb_scap<T>();
+    using U = typename Coord<T>::U;
+    constexpr int SCAP = LB_SCAP;
     constexpr int CELL_SPAN = 2 * D + 1;
     constexpr int CELL_STENCIL = cell_stencil(D);
     extern __shared__ __align__(16) unsigned char lb_smem[];
-    Q *stage = reinterpret_cast<Q *>(lb_smem);
+    float4 *stage = reinterpret_cast<float4 *>(lb_smem);  // offsets from the centre, .w = index bits
     __shared__ int pre[CELL_STENCIL + 1];  // candidates before stencil cell k
     __shared__ int nstart[CELL_STENCIL];   // first sorted index of stencil cell k
     __shared__ int wsum[LB_THREADS / 32];
@@ -168,7 +176,10 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
         const int nc = R.nc, local = hc - R.cell_off;
         const int cx = local % nc, cy = (local / nc) % nc, cz = local / (nc * nc);
         const float sc = (float)(R.L / Coord<T>::scale);
-        const float rl2 = (float)(R.rcl * R.rcl);
+        const float rl2 = (float)(R.rcl * R.rcl * (1.0 + 1e-5));
+        // the home cell's centre in the integer coordinates
+        const U ox = Coord<T>::q(((double)cx + 0.5) / nc), oy = Coord<T>::q(((double)cy + 0.5) / nc),
+                oz = Coord<T>::q(((double)cz + 0.5) / nc);
         __syncthreads();  // the previous cell is done with pre, nstart and stage
         // stencil cell tid: its start and count; pre = exclusive prefix sum
         int cntc = 0;
@@ -213,28 +224,32 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                         if (pre[mid] <= gg) lo = mid; else hi = mid - 1;
                     }
                     const int j = nstart[lo] + gg - pre[lo];
-                    Q q = xq[j];
-                    q.w = j;  // the staged copy carries the sorted index
-                    stage[g] = q;
+                    const Q q = xq[j];
+                    // the staged copy carries the sorted index
+                    stage[g] = make_float4((float)qdiff<T>(q.x, ox) * sc, (float)qdiff<T>(q.y, oy) * sc,
+                                           (float)qdiff<T>(q.z, oz) * sc, __int_as_float(j));
                 }
                 __syncthreads();
                 for (int i0 = 0; i0 < nch; i0 += LB_PPB) {
                     const int i = i0 + tid / LB_TPI;
                     const bool have = i < nch;
                     const int s = hstart + c0 + i;
-                    Q xi;
-                    if (have) xi = xq[s];
+                    float xr = 0.f, yr = 0.f, zr = 0.f;  // this particle's offset from the centre
+                    if (have) {
+                        const Q xi = xq[s];
+                        xr = (float)qdiff<T>(xi.x, ox) * sc;
+                        yr = (float)qdiff<T>(xi.y, oy) * sc;
+                        zr = (float)qdiff<T>(xi.z, oz) * sc;
+                    }
                     int cnt = have ? cnt_sm[i] : 0;
                     for (int kb = 0; kb < wlen; kb += LB_TPI) {  // uniform over the block
                         const int k = kb + sub;
                         bool in = false;
                         int j = 0;
                         if (have && k < wlen) {
-                            const Q q = stage[k];
-                            const float dx = (float)qdiff<T>(xi.x, q.x) * sc;
-                            const float dy = (float)qdiff<T>(xi.y, q.y) * sc;
-                            const float dz = (float)qdiff<T>(xi.z, q.z) * sc;
-                            j = (int)q.w;
+                            const float4 q = stage[k];
+                            const float dx = xr - q.x, dy = yr - q.y, dz = zr - q.z;
+                            j = __float_as_int(q.w);
                             in = (dx * dx + dy * dy + dz * dz < rl2) && j != s;
                         }
                         const unsigned grp = (__ballot_sync(0xffffffffu, in) >> gshift) &
@@ -770,7 +785,7 @@ int pp_particles_per_block(int tpi) { return PPL_THREADS / tpi; }
 template <typename T> void configure_pp_kernels()
 {
     using Q = typename Coord<T>::Q;
-    const int lbs = (int)(lb_scap<T>() * sizeof(Q));
+    const int lbs = (int)(LB_SCAP * sizeof(float4));
     auto setl = [&](auto k) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lbs); };
     setl(k_build_lists<T, 1, 0>); setl(k_build_lists<T, 1, 1>);
     setl(k_build_lists<T, 1, 2>); setl(k_build_lists<T, 1, 3>);
@@ -802,7 +817,7 @@ template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st
         {k_build_lists<T, 1, 0>, k_build_lists<T, 1, 1>, k_build_lists<T, 1, 2>, k_build_lists<T, 1, 3>},
         {k_build_lists<T, 2, 0>, k_build_lists<T, 2, 1>, k_build_lists<T, 2, 2>, k_build_lists<T, 2, 3>}};
     const K kern = kerns[s.cell_div == 1 ? 0 : 1][__builtin_ctz((unsigned)s.pp_tpi) & 3];
-    kern<<<grid, LB_THREADS, lb_scap<T>() * sizeof(Q), st>>>(
+    kern<<<grid, LB_THREADS, LB_SCAP * sizeof(float4), st>>>(
         s.reps, s.nrep, s.cell_start, (const Q *)s.xq, s.nnb, s.nlist, s.maxnb, s.rb_list, s.nrep,
         s.status);
 }
