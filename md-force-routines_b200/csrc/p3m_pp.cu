@@ -102,16 +102,26 @@ __device__ __forceinline__ typename Coord<T>::I qdiff(typename Coord<T>::U a, ty
 __host__ __device__ constexpr int pp_unr(int tpi) { return 16 / tpi < 8 ? 16 / tpi : 8; }
 __host__ __device__ constexpr int pp_chunk(int tpi) { return pp_unr(tpi) < 4 ? pp_unr(tpi) : 4; }
 
-__device__ __forceinline__ long long list_index(int s, int e, int maxnb, int lt)
+// list_index(s, e) = list_row(s) + list_col(e): the particle's part and the
+// entry's part of the index.
+__device__ __forceinline__ int list_lc(int lt) { return (lt == 0 ? 3 : 4 - lt) < 2 ? 1 : 2; }  // log2 C
+__device__ __forceinline__ long long list_row(int s, int maxnb, int lt)
+{
+    return (long long)(s >> 5) * maxnb * 32 + ((s & 31) << (lt + list_lc(lt)));
+}
+__device__ __forceinline__ int list_col(int e, int lt)
 {
     const int lu = lt == 0 ? 3 : 4 - lt;  // log2 UNR
     const int ls = lu + lt;               // log2 STEP (3 or 4)
-    const int lc = lu < 2 ? lu : 2;       // log2 C
+    const int lc = list_lc(lt);           // log2 C
     const int e16 = e & 15, pass = e16 >> ls, w = e16 & ((1 << ls) - 1);
     const int sub = w & ((1 << lt) - 1), v = w >> lt;
     const int chunk = (pass << (lu - lc)) + (v >> lc);
-    const int off = (((((chunk << 5) + (s & 31)) << lt) + sub) << lc) + (v & ((1 << lc) - 1));
-    return ((long long)(s >> 5) * maxnb + (e & ~15)) * 32 + off;
+    return ((e & ~15) << 5) + (chunk << (5 + lt + lc)) + (sub << lc) + (v & ((1 << lc) - 1));
+}
+__device__ __forceinline__ long long list_index(int s, int e, int maxnb, int lt)
+{
+    return list_row(s, maxnb, lt) + list_col(e, lt);
 }
 
 // ---------------------------------------------------------------------------
@@ -229,6 +239,10 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                     stage[g] = make_float4((float)qdiff<T>(q.x, ox) * sc, (float)qdiff<T>(q.y, oy) * sc,
                                            (float)qdiff<T>(q.z, oz) * sc, __int_as_float(j));
                 }
+                // the window's last round filled with candidates out of range
+                const int wpad = (wlen + LB_TPI - 1) & ~(LB_TPI - 1);
+                for (int g = wlen + tid; g < wpad; g += LB_THREADS)
+                    stage[g] = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(-1));
                 __syncthreads();
                 for (int i0 = 0; i0 < nch; i0 += LB_PPB) {
                     const int i = i0 + tid / LB_TPI;
@@ -242,21 +256,17 @@ k_build_lists(const RepDev *__restrict__ reps, int nrep, const int *__restrict__
                         zr = (float)qdiff<T>(xi.z, oz) * sc;
                     }
                     int cnt = have ? cnt_sm[i] : 0;
-                    for (int kb = 0; kb < wlen; kb += LB_TPI) {  // uniform over the block
-                        const int k = kb + sub;
-                        bool in = false;
-                        int j = 0;
-                        if (have && k < wlen) {
-                            const float4 q = stage[k];
-                            const float dx = xr - q.x, dy = yr - q.y, dz = zr - q.z;
-                            j = __float_as_int(q.w);
-                            in = (dx * dx + dy * dy + dz * dz < rl2) && j != s;
-                        }
+                    int *lrow = nlist + list_row(have ? s : hstart, maxnb, lt);
+                    for (int kb = 0; kb < wpad; kb += LB_TPI) {  // uniform over the block
+                        const float4 q = stage[kb + sub];
+                        const float dx = xr - q.x, dy = yr - q.y, dz = zr - q.z;
+                        const int j = __float_as_int(q.w);
+                        const bool in = have && (dx * dx + dy * dy + dz * dz < rl2) && j != s;
                         const unsigned grp = (__ballot_sync(0xffffffffu, in) >> gshift) &
                                              ((1u << LB_TPI) - 1u);
                         if (in) {
                             const int pos = cnt + __popc(grp & below);
-                            if (pos < maxnb) nlist[list_index(s, pos, maxnb, lt)] = j;
+                            if (pos < maxnb) lrow[list_col(pos, lt)] = j;
                         }
                         cnt += __popc(grp);
                     }
