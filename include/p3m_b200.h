@@ -312,7 +312,7 @@ int p3m_get_pp_config(p3m_ctx *ctx, int *tpi, double *skin, int *maxnb);
 /* Kernel shapes of a context (no counterpart in the reference, whose PP and
  * PM stages have no GPU path): what the autotuner of the Python package
  * searches. p3m_create picks pp_tpi from the particle count, cell_div 2,
- * plane_max 64, gather_mode 1, prune_buf 0 and skin_temp 0. Setting waits
+ * plane_max 64, gather_mode 1 and prune_buf 0. Setting waits
  * for the context's work, drops its captured step graphs and forces a list
  * rebuild. Every setting computes the same sums; they differ only in the
  * order of additions (pair order in the lists, lanes per particle, FFT
@@ -333,9 +333,6 @@ typedef struct {
                              the Verlet-list entries closer than rc + prune_buf, which
                              it rebuilds itself whenever a particle of the replica has
                              moved prune_buf/2 since their last build (dynamic pruning)  */
-    int32_t skin_temp;    /* 1: with skin >= 0, each replica's skin is skin x
-                             sqrt(T_desired / mean T_desired), within [skin/4, rc/2]
-                             (hot replicas cross their skin sooner); 0: one skin      */
 } p3m_tuning;
 int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t);
 int p3m_get_tuning(p3m_ctx *ctx, p3m_tuning *t);

@@ -1,6 +1,5 @@
 // C ABI of libp3m_b200: contexts, device buffers, the compat entry points that
 // mirror the reference's Python functions, and the device-resident stepper.
-#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -198,19 +197,10 @@ static void plan_lists(p3m_ctx *ctx, double skin_override, int tpi)
     int cell = 0, blk = 0;
     double maxmean = 0.0, maxmean_in = 0.0;
     const int ppb = pp_particles_per_block(tpi);
-    // skin_temp: the set skin scaled per replica by sqrt(T_desired / mean
-    // T_desired) -- the thermal speed, which sets how soon a replica's
-    // particles cross it -- within [skin/4, rc/2]
-    double tmean = 0.0;
-    for (int r = 0; r < ctx->nrep; ++r) tmean += ctx->desc[r].t_desired / ctx->nrep;
     for (int r = 0; r < ctx->nrep; ++r) {
         const p3m_replica_desc &d = ctx->desc[r];
         RepDev &R = ctx->rh[r];
         double skin = skin_override >= 0.0 ? skin_override : (d.skin >= 0.0 ? d.skin : kDefaultSkin);
-        if (s.skin_temp && skin_override >= 0.0 && tmean > 0.0) {
-            skin = std::min(std::max(skin_override * std::sqrt(d.t_desired / tmean), 0.25 * skin_override),
-                            0.5 * d.rc);
-        }
         // rc + skin <= L/3 keeps >= 3 cell_div cells per side, more than
         // the stencil spans (no cell is visited twice)
         const double smax = d.box / 3.0 * (1.0 - 1e-12) - d.rc;
@@ -1499,8 +1489,6 @@ extern "C" int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t)
     for (int r = 0; r < ctx->nrep; ++r)
         if (t->skin > 0.5 * ctx->desc[r].rc)
             return fail(ctx, P3M_EARG, "p3m_set_tuning", "skin must be <= rc/2 (negative: default)");
-    if (t->skin_temp != 0 && t->skin_temp != 1)
-        return fail(ctx, P3M_EARG, "p3m_set_tuning", "skin_temp must be 0 or 1");
     if (!(t->prune_buf >= 0.0 && t->prune_buf <= 1e3))
         return fail(ctx, P3M_EARG, "p3m_set_tuning", "prune_buf must be >= 0");
     if (t->prune_buf > 0.0 && ctx->prec != P3M_FP32)
@@ -1518,7 +1506,6 @@ extern "C" int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t)
     s.plane_max = t->plane_max;
     s.gather_mode = (ctx->prec == P3M_FP64 && t->gather_mode == 2) ? 1 : t->gather_mode;
     s.prune_buf = t->prune_buf;
-    s.skin_temp = t->skin_temp ? 1 : 0;
     plan_lists(ctx, t->skin, tpi);
     plan_mesh_passes(ctx);
     for (int r = 0; r < ctx->nrep; ++r)
@@ -1566,7 +1553,6 @@ extern "C" int p3m_get_tuning(p3m_ctx *ctx, p3m_tuning *t)
     t->gather_mode = ctx->s.gather_mode;
     t->skin = ctx->skin_override;
     t->prune_buf = ctx->s.prune_buf;
-    t->skin_temp = ctx->s.skin_temp;
     return P3M_OK;
 }
 

@@ -25,7 +25,6 @@ struct DevState {
     int pp_nblk = 0;             // blocks of the PP force kernel (replica-aligned)
     int maxnb = 0;               // list capacity per particle
     double prune_buf = 0.0;      // inner-list buffer beyond rc (FP32; 0: no inner lists)
-    int skin_temp = 0;           // 1: the set skin scaled per replica by sqrt(T_desired / mean)
     int maxnb_in = 0;            // inner-list capacity per particle
     int has_mesh = 0;
     int max_mesh = 0;            // largest M over replicas

@@ -47,7 +47,6 @@ class Tuning(ctypes.Structure):
         ("gather_mode", ctypes.c_int32),
         ("skin", ctypes.c_double),
         ("prune_buf", ctypes.c_double),
-        ("skin_temp", ctypes.c_int32),
     ]
 
     def as_dict(self):

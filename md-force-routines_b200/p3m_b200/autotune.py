@@ -15,9 +15,7 @@ What it searches (p3m_tuning of the C ABI):
   component (three times the work items);
 * on the FP32 path, inner lists (dynamic pruning): the pair kernel reads the
   Verlet entries closer than rc + prune_buf and rebuilds those lists itself
-  every few steps, which makes larger skins (rarer Verlet rebuilds) cheap;
-* for replicas of unequal temperatures, skins scaled per replica by the
-  thermal speed (skin_temp), tried last from the best setting so far.
+  every few steps, which makes larger skins (rarer Verlet rebuilds) cheap.
 
 The list cells, FFT tiles and gather are searched one at a time from the
 best PP setting (coordinate descent), then inner-list buffers with a few
@@ -65,19 +63,7 @@ def _save(d):
 
 def _key(t):
     return (f"tpi{t['pp_tpi']},skin{t['skin']:g},div{t['cell_div']},plane{t['plane_max']},"
-            f"gather{t['gather_mode']},prune{t.get('prune_buf', 0.0):g}"
-            + (",skinT" if t.get("skin_temp") else ""))
-
-
-#: skins tried scaled per replica by sqrt(T_desired / mean) (replicas of unequal temperatures)
-TEMP_SKINS = (0.5, 0.8, 1.1)
-
-
-def temp_options(ctx):
-    """Skins worth trying per-replica scaled: only for replicas whose
-    temperatures differ by more than 1.5x."""
-    ts = [r.T_desired for r in ctx.replicas]
-    return list(TEMP_SKINS) if min(ts) > 0 and max(ts) / min(ts) > 1.5 else []
+            f"gather{t['gather_mode']},prune{t.get('prune_buf', 0.0):g}")
 
 
 def shape_options(ctx):
@@ -140,7 +126,6 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
         return times[k]
 
     base["prune_buf"] = 0.0
-    base["skin_temp"] = 0
     for tpi, skin in (candidates or CANDIDATES):
         if skin <= max_skin:
             trial(dict(base, pp_tpi=tpi, skin=skin))
@@ -155,9 +140,6 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
         for skin, pb in prune_options(ctx, best["skin"], max_skin):
             trial(dict(best, skin=skin, prune_buf=pb))
             n_prune += 1
-        best = dict(settings[min(times, key=times.get)])
-    for skin in temp_options(ctx):
-        trial(dict(best, skin=skin, skin_temp=1))
     final = {}
     for k in sorted(times, key=times.get)[:max(1, finalists)]:
         final[k] = timed(settings[k], 4 * steps)

@@ -578,36 +578,3 @@ def test_set_priority_keeps_results():
             out.append(c.get_state(0) + (c.energies(max_steps=5),))
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
-
-
-def test_temperature_scaled_skins():
-    """skin_temp: each replica's skin is the set skin times sqrt(T_desired /
-    mean T_desired); over a trajectory with rebuilds at each replica's own
-    pace the last step's forces equal a fresh evaluation at the same
-    positions, and the setting round-trips."""
-    from p3m_b200 import FP32, MODE_NVE, Context, Replica
-
-    reps = []
-    for N, T in ((3000, 0.005), (3000, 0.05)):
-        L = (4 * np.pi * N / 3) ** (1 / 3)
-        reps.append(Replica(N=N, L=L, kappa=1.5, alpha=0.7, rc=min(4.0, L / 3.6), M=32, dt=0.1,
-                            T_desired=T))
-    states = [_init_state(r, 61 + i) for i, r in enumerate(reps)]
-    with Context(reps, precision=FP32) as c:
-        for i, (p, v) in enumerate(states):
-            c.set_state(i, p, v)
-        c.init_forces()
-        c.equilibrate(100, quench_steps=100)
-        c.set_tuning(pp_tpi=2, skin=0.4, skin_temp=1)
-        assert c.tuning()["skin_temp"] == 1
-        rb0 = [c.replica_stats(i)["rebuilds"] for i in range(2)]
-        c.run(150, MODE_NVE)
-        rebuilds = [c.replica_stats(i)["rebuilds"] - rb0[i] for i in range(2)]
-        st = c.get_state_all()
-    assert rebuilds[1] >= 1
-    with Context(reps, precision=FP32) as c:
-        c.set_tuning(pp_tpi=2, skin=0.4)
-        c.set_state_all(st[0], st[1])
-        c.init_forces()
-        acc = c.get_state_all()[2]
-    assert rel_rms(st[2], acc) < 1e-6
