@@ -40,7 +40,7 @@ struct DevState {
     void *xq = nullptr;          // integer coordinates in sorted order (uint4 / ulonglong4)
     int *nnb = nullptr;          // list length per sorted particle
     int *cell_sub = nullptr;     // [particle] sub-cell Morton code (rebuild steps)
-    int *nlist = nullptr;        // neighbour lists (sorted indices), warp-interleaved
+    int *nlist = nullptr;        // neighbour lists (sorted indices), in 16-entry group blocks (list_index)
     int *rebuild = nullptr;      // per-replica flags: rebuild cells and lists this step
     // the replicas rebuilding this step (written by k_scan): [0] = count k,
     // [1 .. k] replica indices, [nrep + 1 + j] = cells of the first j of them
