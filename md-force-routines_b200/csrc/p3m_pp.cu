@@ -21,6 +21,13 @@
 // A list holds every pair closer than rc + skin at rebuild time, so it holds
 // every pair closer than rc until the next rebuild.
 //
+// Inner lists (FP32, prune buffer b > 0): the entries of a particle's Verlet
+// list closer than rc + b, built inside the pair kernel whenever some
+// particle of the replica has moved more than b/2 since their last build (or
+// the Verlet lists were rebuilt). A pair missing from an inner list was
+// either farther than rc + b at its build or missing from the Verlet list, so
+// it cannot come within rc before one of the two checks fires.
+//
 // Pair terms: the FP64 path evaluates the reference's formula directly,
 // written with the shared Gaussian factor
 //   e^{+-kr} erfc(u+-) = erfcx(u+-) exp(-(a^2 r^2 + k^2/4a^2)),  u+- = ar +- k/2a,
