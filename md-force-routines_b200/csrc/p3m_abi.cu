@@ -53,7 +53,9 @@ struct p3m_ctx {
     long long step_launches = 0;  // launches when the copies were queued
     bool state_set = false;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    long long graph_kernels[2][2] = {{0, 0}, {0, 0}};  // kernels each graph launches
+    // kGraphSteps steps per graph (launched for whole groups of steps)
+    cudaGraphExec_t graphK[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    long long graph_kernels[2][2] = {{0, 0}, {0, 0}};  // kernels per step of the captured graphs
     int ncell_cap = 0;            // cells allocated (grid with skin 0)
     long long nlist_cap = 0;      // list entries allocated
     long long nlist_in_cap = 0;   // inner-list entries allocated
@@ -63,6 +65,20 @@ struct p3m_ctx {
 };
 
 static thread_local std::string g_err;
+
+// Steps captured in one multi-step graph: fewer graph launches, and no gap
+// between them, for small systems whose steps last tens of microseconds.
+static const int kGraphSteps = 8;
+
+// Drop the captured step graphs (all, or only those recording n(q,t)).
+static void drop_graphs(p3m_ctx *ctx, bool rec_only = false)
+{
+    for (int a = 0; a < 2; ++a)
+        for (int b = rec_only ? 1 : 0; b < 2; ++b) {
+            if (ctx->graph[a][b]) { cudaGraphExecDestroy(ctx->graph[a][b]); ctx->graph[a][b] = nullptr; }
+            if (ctx->graphK[a][b]) { cudaGraphExecDestroy(ctx->graphK[a][b]); ctx->graphK[a][b] = nullptr; }
+        }
+}
 
 #define P3M_VERSION 200
 
@@ -245,9 +261,7 @@ extern "C" int p3m_destroy(p3m_ctx *ctx)
     if (!ctx) return P3M_OK;
     cudaSetDevice(ctx->device);
     if (ctx->st) cudaStreamSynchronize(ctx->st);
-    for (auto &row : ctx->graph)
-        for (auto &g : row)
-            if (g) cudaGraphExecDestroy(g);
+    drop_graphs(ctx);
     DevState &s = ctx->s;
     void *ptrs[] = {s.reps, s.pos, s.vel, s.acc, s.charge, s.prep, s.cell_key, s.cell_count,
                     s.cell_start, s.cell_cursor, s.cell_tmp, s.cell_perm, s.cell_slot, s.xq, s.nnb,
@@ -1208,8 +1222,7 @@ extern "C" int p3m_set_nqt(p3m_ctx *ctx, const double *qmult, int nq, int capaci
     if (ctx->nqt_part) cudaFree(ctx->nqt_part);
     if (ctx->nqt_ring) cudaFree(ctx->nqt_ring);
     ctx->qmult = ctx->nqt_part = ctx->nqt_ring = nullptr;
-    for (auto &row : ctx->graph)
-        if (row[1]) { cudaGraphExecDestroy(row[1]); row[1] = nullptr; }
+    drop_graphs(ctx, true);
     ctx->nq = nq;
     ctx->nqt_cap = capacity;
     ctx->nqt_rows = 0;
@@ -1235,24 +1248,34 @@ template <typename T> static int do_run(p3m_ctx *ctx, int n_steps, int mode, int
     launch_set_counters(ctx->counters, 0, -1, it0, ctx->st);
     ctx->launches++;
     const int gi = (mode == P3M_MODE_THERMOSTAT) ? 1 : 0, gr = rec ? 1 : 0;
-    if (use_graph && !ctx->graph[gi][gr]) {
+    // capture `steps` steps into `*out` (the kernels of one step are counted)
+    auto capture = [&](int steps, cudaGraphExec_t *out) -> int {
         cudaGraph_t g;
         const long long before = ctx->launches;
         CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
-        const int step_rc = seq_step<T>(ctx, mode, rec);
+        int step_rc = P3M_OK;
+        for (int k = 0; k < steps && step_rc == P3M_OK; ++k) step_rc = seq_step<T>(ctx, mode, rec);
         cudaError_t e = cudaStreamEndCapture(ctx->st, &g);
-        ctx->graph_kernels[gi][gr] = ctx->launches - before;  // kernels per replay
+        ctx->graph_kernels[gi][gr] = (ctx->launches - before) / steps;  // kernels per step
         ctx->launches = before;
         if (step_rc != P3M_OK) {
             if (e == cudaSuccess) cudaGraphDestroy(g);
             return step_rc;
         }
         if (e != cudaSuccess) return fail(ctx, P3M_ECUDA, "cudaStreamEndCapture", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&ctx->graph[gi][gr], g, 0);
+        e = cudaGraphInstantiate(out, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(ctx, P3M_ECUDA, "cudaGraphInstantiate", cudaGetErrorString(e));
+        return P3M_OK;
+    };
+    const int groups = use_graph ? n_steps / kGraphSteps : 0;
+    if (use_graph && !ctx->graph[gi][gr]) RET(capture(1, &ctx->graph[gi][gr]));
+    if (groups > 0 && !ctx->graphK[gi][gr]) RET(capture(kGraphSteps, &ctx->graphK[gi][gr]));
+    for (int k = 0; k < groups; ++k) {
+        CK(cudaGraphLaunch(ctx->graphK[gi][gr], ctx->st));
+        ctx->launches += (long long)kGraphSteps * ctx->graph_kernels[gi][gr];
     }
-    for (int k = 0; k < n_steps; ++k) {
+    for (int k = groups * kGraphSteps; k < n_steps; ++k) {
         if (use_graph) {
             CK(cudaGraphLaunch(ctx->graph[gi][gr], ctx->st));
             ctx->launches += ctx->graph_kernels[gi][gr];  // counted while capturing
@@ -1337,12 +1360,7 @@ extern "C" int p3m_set_snapshots(p3m_ctx *ctx, int interval, int capacity)
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->st));
     // the step sequence changes: drop the captured graphs
-    for (auto &row : ctx->graph)
-        for (auto &g : row)
-            if (g) {
-                cudaGraphExecDestroy(g);
-                g = nullptr;
-            }
+    drop_graphs(ctx);
     if (capacity != ctx->snap_cap || interval == 0) {
         cudaFree(ctx->snap);
         cudaFree(ctx->snap_steps);
@@ -1464,9 +1482,7 @@ extern "C" int p3m_set_priority(p3m_ctx *ctx, int level)
             return fail(ctx, P3M_ECUDA, "cudaStreamSynchronize", cudaGetErrorString(e));
         }
     }
-    for (auto &row : ctx->graph)
-        for (auto &g : row)
-            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    drop_graphs(ctx);
     for (int k = 0; k < 3; ++k) {
         cudaStreamDestroy(*streams[k]);
         *streams[k] = fresh[k];
@@ -1495,9 +1511,7 @@ extern "C" int p3m_set_tuning(p3m_ctx *ctx, const p3m_tuning *t)
         return fail(ctx, P3M_EARG, "p3m_set_tuning", "inner lists (prune_buf > 0) are an FP32-path option");
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->st));
-    for (auto &row : ctx->graph)
-        for (auto &g : row)
-            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    drop_graphs(ctx);
     DevState &s = ctx->s;
     // the new plan replaces the old one only once its list storage exists
     const DevState saved = s;
