@@ -1268,9 +1268,11 @@ template <typename T> static int do_run(p3m_ctx *ctx, int n_steps, int mode, int
         if (e != cudaSuccess) return fail(ctx, P3M_ECUDA, "cudaGraphInstantiate", cudaGetErrorString(e));
         return P3M_OK;
     };
+    // both graphs on first use, so that a warm-up of any length has captured
+    // them before the runs it prepares
     const int groups = use_graph ? n_steps / kGraphSteps : 0;
     if (use_graph && !ctx->graph[gi][gr]) RET(capture(1, &ctx->graph[gi][gr]));
-    if (groups > 0 && !ctx->graphK[gi][gr]) RET(capture(kGraphSteps, &ctx->graphK[gi][gr]));
+    if (use_graph && !ctx->graphK[gi][gr]) RET(capture(kGraphSteps, &ctx->graphK[gi][gr]));
     for (int k = 0; k < groups; ++k) {
         CK(cudaGraphLaunch(ctx->graphK[gi][gr], ctx->st));
         ctx->launches += (long long)kGraphSteps * ctx->graph_kernels[gi][gr];
