@@ -240,9 +240,9 @@ int p3m_set_nqt(p3m_ctx *ctx, const double *qmult, int nq, int capacity);
 /* Advance all replicas n_steps. mode: P3M_MODE_NVE or P3M_MODE_THERMOSTAT
  * (it0 = step index of the first step, for the thermostat's it<=1999 switch).
  * record_nqt: accumulate n(q,t) rows each step. use_graph: capture the step
- * (and a group of 8 steps) in CUDA graphs on first use and replay them --
- * whole groups of 8 as one graph, the rest one step at a time. sync: wait
- * for completion. */
+ * (and, on the FP32 path, a group of 8 steps) in CUDA graphs on first use
+ * and replay them -- whole groups of 8 as one graph, the rest one step at a
+ * time. sync: wait for completion. */
 int p3m_run(p3m_ctx *ctx, int n_steps, int mode, int it0, int record_nqt, int use_graph,
             int sync);
 
