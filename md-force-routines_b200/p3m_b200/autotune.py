@@ -19,8 +19,8 @@ What it searches (p3m_tuning of the C ABI):
 
 The list cells, FFT tiles and gather are searched one at a time from the
 best PP setting (coordinate descent), then inner-list buffers with a few
-skins from the best of those (and, if one wins, the list-cell divisor again
-for its skin); then the fastest few settings are timed again over
+skins from the best of those, each with both list-cell divisors; then the
+fastest few settings are timed again over
 four times the steps (list rebuilds come every few tens of steps, so short runs
 rank close candidates by chance) and the fastest is installed. The state
 should already be equilibrated: each timing advances the system. Results are
@@ -138,13 +138,12 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
             best = dict(settings[min(times, key=times.get)])
     n_before = len(times)
     if prune:
+        # the cell size follows the skin: each inner-list setting with every
+        # list-cell divisor
+        divs = shape_options(ctx)["cell_div"] if shapes else (best["cell_div"],)
         for skin, pb in prune_options(ctx, best["skin"], max_skin):
-            trial(dict(best, skin=skin, prune_buf=pb))
-        best = dict(settings[min(times, key=times.get)])
-        if shapes and best.get("prune_buf", 0.0) > 0.0:
-            # the cell size follows the skin: the list cells again for the new one
-            for v in shape_options(ctx)["cell_div"]:
-                trial(dict(best, cell_div=v))
+            for d in divs:
+                trial(dict(best, skin=skin, prune_buf=pb, cell_div=d))
     n_prune = len(times) - n_before
     final = {}
     for k in sorted(times, key=times.get)[:max(1, finalists)]:
