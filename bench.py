@@ -74,6 +74,8 @@ def parse():
                     help="set threads per particle and Verlet skin instead of autotuning")
     ap.add_argument("--prune-buf", type=float, default=0.0,
                     help="with --pp-config: FP32 inner-list buffer beyond rc (0: none)")
+    ap.add_argument("--e2e-parts", type=int, default=5,
+                    help="contexts the ensemble is split into for the end-to-end number")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the FP64, e2e, roofline and CPU-baseline legs")
     return ap.parse_args()
@@ -567,7 +569,7 @@ def extras(args, line, ctx, reps, states, device):
     # own streams with asynchronous copies, so one part's copies overlap the
     # others' steps (the copy engines and the SMs work at the same time).
     ntot = sum(r.N for r in reps)
-    nparts = min(5, len(reps))
+    nparts = min(args.e2e_parts, len(reps))
     cuts = [round(k * len(reps) / nparts) for k in range(nparts + 1)]
     halves = [reps[cuts[k]:cuts[k + 1]] for k in range(nparts)]
     offs = np.cumsum([0] + [sum(r.N for r in h) for h in halves])
@@ -583,9 +585,12 @@ def extras(args, line, ctx, reps, states, device):
     ctxs = [Context(h, precision=FP32, device=device) for h in halves]
     try:
         # descending stream priorities: the first part finishes its step first
-        # and its copies back overlap the later parts' steps
+        # and its copies back overlap the later parts' steps; every part runs
+        # the kernel shapes installed on the timed ensemble
+        shapes = ctx.tuning()
         for k, c in enumerate(ctxs):
             c.set_priority(k)
+            c.set_tuning(**shapes)
         for c, hb in zip(ctxs, host):
             c.set_state_all(hb[0], hb[1])
             c.init_forces()
