@@ -79,3 +79,47 @@ def test_reference_driver_calls_bind_to_package_modules():
     assert seen == {("yukawa_gf_opt", "gf_opt"), ("yukawa_p3m_ord6", "force_pot"),
                     ("thermostat_p3m_ord6", "vscale"), ("velocity_verlet_p3m_ord6", "update"),
                     ("read", "initL"), ("initialize_pos_vel", "initial")}
+
+
+def test_tuning_struct_layout():
+    """p3m_tuning of the C header: four int32 shapes, then the skin and the
+    inner-list buffer as doubles."""
+    import ctypes
+
+    from p3m_b200._lib import Tuning
+
+    assert ctypes.sizeof(Tuning) == 4 * 4 + 2 * 8
+    assert [f for f, _ in Tuning._fields_] == ["pp_tpi", "cell_div", "plane_max", "gather_mode",
+                                             "skin", "prune_buf"]
+
+
+class _FakeCtx:
+    def __init__(self, precision, Ms):
+        from p3m_b200 import Replica
+
+        self.precision = precision
+        self.replicas = [Replica(N=1000, L=10.0, kappa=1.0, alpha=0.7, rc=3.0, M=M) for M in Ms]
+
+
+def test_autotune_search_space():
+    """The autotuner's options: inner-list buffers only on FP32 and below the
+    skin, larger skins only up to the cap, plane/pencil only for meshes up
+    to 64^3, the two-buffer gather only on FP32, and keys that tell every
+    setting apart."""
+    from p3m_b200 import FP32, FP64
+    from p3m_b200.autotune import PRUNE_BUFS, _key, prune_options, shape_options
+
+    c32, c64 = _FakeCtx(FP32, [32, 128]), _FakeCtx(FP64, [128])
+    assert prune_options(c64, 0.8, 1.5) == []
+    opts = prune_options(c32, 0.8, 1.5)
+    assert all(pb < sk <= 1.5 for sk, pb in opts)
+    assert {pb for _, pb in opts} == set(PRUNE_BUFS)
+    assert {sk for sk, _ in opts} == {0.8, 1.1, 1.4}
+    assert {sk for sk, _ in prune_options(c32, 0.5, 1.2)} == {0.5, 1.1}
+    assert shape_options(c32) == {"cell_div": (2, 1), "plane_max": (64, 0), "gather_mode": (1, 0, 2)}
+    assert shape_options(c64) == {"cell_div": (2, 1), "gather_mode": (1, 0)}
+    base = {"pp_tpi": 2, "cell_div": 2, "plane_max": 64, "gather_mode": 1, "skin": 0.8,
+            "prune_buf": 0.0}
+    keys = {_key(dict(base, **kw)) for kw in ({}, {"prune_buf": 0.3}, {"cell_div": 1},
+                                              {"skin": 1.1}, {"gather_mode": 2})}
+    assert len(keys) == 5
