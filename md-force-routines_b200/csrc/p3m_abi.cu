@@ -592,7 +592,7 @@ template <typename T> static void seq_pp(p3m_ctx *ctx, bool reduce = true, cudaS
 {
     if (!st) st = ctx->st;
     launch_pp<T>(ctx->s, st);
-    ctx->launches += pp_kernel_count(ctx->s);
+    ctx->launches++;
     if (reduce) {
         launch_reduce_pp(ctx->s, st);
         ctx->launches++;

@@ -92,7 +92,6 @@ template <typename T> void launch_quantize(const DevState &s, cudaStream_t st);
 template <typename T> void launch_build_lists(const DevState &s, cudaStream_t st);
 template <typename T> void launch_pp(const DevState &s, cudaStream_t st);
 int pp_particles_per_block(int tpi);
-int pp_kernel_count(const DevState &s);  // pair-kernel launches per force evaluation
 void launch_reduce_pp(const DevState &s, cudaStream_t st);
 
 template <typename T> void launch_assign(const DevState &s, cudaStream_t st);

@@ -880,7 +880,6 @@ template <typename T> void launch_pp(const DevState &s, cudaStream_t st)
     }
 }
 
-int pp_kernel_count(const DevState &) { return 1; }
 
 void launch_reduce_pp(const DevState &s, cudaStream_t st)
 {
