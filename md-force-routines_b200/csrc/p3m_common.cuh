@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "p3m_b200.h"
+#include "p3m_list_layout.h"  // PP_LIST_PAD and the neighbour-list layout
 
 namespace p3m {
 
@@ -49,10 +50,6 @@ enum : int {
 #define P3M_PP_TABLE_N 512
 #endif
 constexpr int PP_TABLE_N = P3M_PP_TABLE_N;  // FP32 pair table: cubic intervals on [0, rc]
-// Neighbour lists are padded with the particle's own index to a multiple of
-// this many entries (a padded entry has r = 0 and adds nothing), so the FP32
-// pair loop reads whole blocks of entries without a bounds test.
-constexpr int PP_LIST_PAD = 16;
 
 // Per-replica constants. Offsets index the concatenated device arrays.
 struct RepDev {

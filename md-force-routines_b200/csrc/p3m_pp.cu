@@ -95,41 +95,8 @@ __device__ __forceinline__ typename Coord<T>::I qdiff(typename Coord<T>::U a, ty
     return (typename Coord<T>::I)(a - b);
 }
 
-// List layout. A particle's entries come in blocks of PP_LIST_PAD = 16, and
-// block b of the 32 consecutive sorted particles s >> 5 is stored as one
-// group block of 512 entries (2 KB) at ((s >> 5) maxnb + 16 b) 32. Inside a
-// group block the order follows the FP32 pair kernel with TPI = 2^lt lanes
-// per particle: a pass takes STEP = UNR TPI entries of a particle (UNR =
-// min(16 / TPI, 8)), lane `sub` entries v TPI + sub (v < UNR) as UNR / C
-// chunks of C = min(UNR, 4) contiguous entries, and chunk i of all 32
-// particles' lanes lies together -- so one vector load of a warp reads 512
-// contiguous bytes (256 at TPI 8), and the 16 entries of a particle's block
-// lie within its group block (coalesced list writes). Lists are rebuilt
-// whenever TPI changes.
-__host__ __device__ constexpr int pp_unr(int tpi) { return 16 / tpi < 8 ? 16 / tpi : 8; }
-__host__ __device__ constexpr int pp_chunk(int tpi) { return pp_unr(tpi) < 4 ? pp_unr(tpi) : 4; }
-
-// list_index(s, e) = list_row(s) + list_col(e): the particle's part and the
-// entry's part of the index.
-__device__ __forceinline__ int list_lc(int lt) { return (lt == 0 ? 3 : 4 - lt) < 2 ? 1 : 2; }  // log2 C
-__device__ __forceinline__ long long list_row(int s, int maxnb, int lt)
-{
-    return (long long)(s >> 5) * maxnb * 32 + ((s & 31) << (lt + list_lc(lt)));
-}
-__device__ __forceinline__ int list_col(int e, int lt)
-{
-    const int lu = lt == 0 ? 3 : 4 - lt;  // log2 UNR
-    const int ls = lu + lt;               // log2 STEP (3 or 4)
-    const int lc = list_lc(lt);           // log2 C
-    const int e16 = e & 15, pass = e16 >> ls, w = e16 & ((1 << ls) - 1);
-    const int sub = w & ((1 << lt) - 1), v = w >> lt;
-    const int chunk = (pass << (lu - lc)) + (v >> lc);
-    return ((e & ~15) << 5) + (chunk << (5 + lt + lc)) + (sub << lc) + (v & ((1 << lc) - 1));
-}
-__device__ __forceinline__ long long list_index(int s, int e, int maxnb, int lt)
-{
-    return list_row(s, maxnb, lt) + list_col(e, lt);
-}
+// The list layout (list_index for the writer; list_lane_at, list_pass_at,
+// list_block and list_chunk for the readers) is in p3m_list_layout.h.
 
 // ---------------------------------------------------------------------------
 // list build (rebuild steps only)
@@ -356,16 +323,16 @@ k_pp_f64(const RepDev *__restrict__ reps, int nrep, const ulonglong4 *__restrict
         // the padded list in passes of the layout (see list_index): lane sub
         // takes entries v TPI + sub of each pass, as chunks of C
         constexpr int UNR = pp_unr(TPI), STEP = UNR * TPI, C = pp_chunk(TPI), NCH = UNR / C;
-        constexpr int CSTRIDE = 32 * TPI * C;
+        constexpr int CSTRIDE = list_cstride(TPI);
         const int nr = (nnb[s] + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1);
-        const int *lg = nlist + (long long)(s >> 5) * maxnb * 32 + ((s & 31) * TPI + sub) * C;
+        const int *lg = list_lane_at<TPI>(nlist, s >> 5, s & 31, sub, maxnb);
         for (int c0 = 0; c0 < nr; c0 += CH) {
             const int c1 = min(c0 + CH, nr);
             T px = 0, py = 0, pz = 0, pu = 0;
             for (int k0 = c0; k0 < c1; k0 += STEP) {
                 // independent loads first (padding points at the particle
                 // itself: r2 = 0 is skipped below)
-                const int *lp = lg + (long long)(k0 & ~15) * 32 + ((k0 & 15) / STEP) * NCH * CSTRIDE;
+                const int *lp = list_pass_at<TPI>(lg, k0);
                 int j[UNR];
 #pragma unroll
                 for (int i = 0; i < NCH; ++i) {
@@ -558,19 +525,19 @@ template <int TPI> struct Stage {
 };
 
 // One particle's block of 16 staged entries, written by its TPI lanes in
-// the list layout: og = the lane's first chunk in the particle's group
-// block (see list_index).
+// the list layout: og = the lane's first chunk of the block (list_lane_at
+// plus list_block).
 template <int TPI>
 __device__ __forceinline__ void store_block(int *og, const Stage<TPI> &buf, int sub)
 {
     constexpr int UNR = pp_unr(TPI), STEP = UNR * TPI, C = pp_chunk(TPI), NCH = UNR / C;
-    constexpr int CSTRIDE = 32 * TPI * C;
+    constexpr int CSTRIDE = list_cstride(TPI);
 #pragma unroll
     for (int pass = 0; pass < PP_LIST_PAD / STEP; ++pass)
 #pragma unroll
         for (int i = 0; i < NCH; ++i) {
             const int e = pass * STEP + i * C * TPI + sub;  // entries (i C + c) TPI + sub
-            int *dst = og + (pass * NCH + i) * CSTRIDE;
+            int *dst = og + list_chunk<TPI>(pass, i);
             if constexpr (C == 4)
                 *reinterpret_cast<int4 *>(dst) =
                     make_int4(buf[e], buf[e + TPI], buf[e + 2 * TPI], buf[e + 3 * TPI]);
@@ -595,7 +562,7 @@ __device__ __forceinline__ double pp_body(const RepDev &R, int s, bool have,
     constexpr int UNR = pp_unr(TPI);                     // entries per lane per pass
     constexpr int STEP = UNR * TPI;                      // entries of a particle per pass
     constexpr int C = pp_chunk(TPI), NCH = UNR / C;      // list chunks of a lane per pass
-    constexpr int CSTRIDE = 32 * TPI * C;                // between a lane's chunks (entries)
+    constexpr int CSTRIDE = list_cstride(TPI);                // between a lane's chunks (entries)
     static_assert(UNR % 2 == 0 && PP_LIST_PAD % STEP == 0, "whole pairs, whole pad blocks");
     static_assert(PP_LIST_PAD == 16 && STEP <= 16, "the list layout's blocks");
     const int sub = threadIdx.x % TPI;
@@ -622,13 +589,12 @@ __device__ __forceinline__ double pp_body(const RepDev &R, int s, bool have,
         const int nr = have ? (nnb[s] + PP_LIST_PAD - 1) & ~(PP_LIST_PAD - 1) : 0;
         const int nloop = PRUNE ? __reduce_max_sync(0xffffffffu, nr) : nr;
         // this lane's first chunk in the particle's group blocks
-        const int *lg = nlist + (long long)(sv >> 5) * maxnb * 32 + (p32 * TPI + sub) * C;
+        const int *lg = list_lane_at<TPI>(nlist, sv >> 5, p32, sub, maxnb);
         const Stage<TPI> buf{stage_warp, (int)(threadIdx.x & 31) / TPI};
         int fill = 0, blk = 0;  // pruning: staged entries, blocks written
-        int *og = PRUNE ? pa.nlist_in + (long long)(sv >> 5) * pa.maxnb_in * 32 + (p32 * TPI + sub) * C
-                        : nullptr;
+        int *og = PRUNE ? list_lane_at<TPI>(pa.nlist_in, sv >> 5, p32, sub, pa.maxnb_in) : nullptr;
         for (int k0 = 0; k0 < nloop; k0 += STEP) {
-            const int *lp = lg + (long long)(k0 & ~15) * 32 + ((k0 & 15) / STEP) * NCH * CSTRIDE;
+            const int *lp = list_pass_at<TPI>(lg, k0);
             int j[UNR];
             if (!PRUNE || k0 < nr) {
 #pragma unroll
@@ -698,7 +664,7 @@ __device__ __forceinline__ double pp_body(const RepDev &R, int s, bool have,
                 // no synchronisation inside them)
                 const bool full = fill >= PP_LIST_PAD;
                 if (full && (blk + 1) * PP_LIST_PAD <= pa.maxnb_in)
-                    store_block<TPI>(og + (long long)blk * PP_LIST_PAD * 32, buf, sub);
+                    store_block<TPI>(og + list_block(blk), buf, sub);
                 __syncwarp();
                 if (full)
                     for (int e = sub; e < fill - PP_LIST_PAD; e += TPI) buf[e] = buf[PP_LIST_PAD + e];
@@ -716,7 +682,7 @@ __device__ __forceinline__ double pp_body(const RepDev &R, int s, bool have,
                 for (int e = fill + sub; e < PP_LIST_PAD; e += TPI) buf[e] = sv;
             __syncwarp();
             if (have && fill > 0 && (blk + 1) * PP_LIST_PAD <= pa.maxnb_in)
-                store_block<TPI>(og + (long long)blk * PP_LIST_PAD * 32, buf, sub);
+                store_block<TPI>(og + list_block(blk), buf, sub);
             if (have && sub == 0) {
                 if (cin > pa.maxnb_in) raise_status(pa.status, ST_NBOVF);
                 pa.nnb_in[s] = min(cin, pa.maxnb_in);
