@@ -77,12 +77,27 @@ def shape_options(ctx):
     return opts
 
 
-def prune_options(ctx, skin, max_skin):
+def max_skin(ctx):
+    """The largest skin every replica allows (half its cutoff)."""
+    return min(0.5 * r.rc for r in ctx.replicas)
+
+
+def pp_candidates(ctx, candidates=None):
+    """(threads per particle, skin) pairs of the PP grid that every replica
+    allows; with cutoffs too short for any of the grid's skins, each thread
+    count at the largest skin allowed."""
+    grid = list(candidates or CANDIDATES)
+    cap = max_skin(ctx)
+    fit = [(tpi, skin) for tpi, skin in grid if skin <= cap]
+    return fit or sorted({(tpi, cap) for tpi, _ in grid})
+
+
+def prune_options(ctx, skin, cap):
     """(skin, prune_buf) pairs worth trying from a best skin so far: FP32
-    only, each buffer below the skin."""
+    only, skins up to cap, each buffer below the skin."""
     if ctx.precision != FP32:
         return []
-    skins = sorted({skin, *(x for x in PRUNE_SKINS if x <= max_skin)})
+    skins = sorted({skin, *(x for x in PRUNE_SKINS if x <= cap)})
     return [(sk, pb) for pb in PRUNE_BUFS for sk in skins if pb < sk]
 
 
@@ -95,10 +110,10 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
 
     sig = signature(ctx)
     cache = _load() if use_cache else {}
-    max_skin = min(0.5 * r.rc for r in ctx.replicas)
+    cap = max_skin(ctx)
     if use_cache and sig in cache and isinstance(cache[sig].get("choice"), dict):
         choice = dict(cache[sig]["choice"])
-        choice["skin"] = min(choice["skin"], max_skin)
+        choice["skin"] = min(choice["skin"], cap)
         ctx.set_tuning(**choice)
         return cache[sig]
     stream = torch.cuda.ExternalStream(ctx.stream())
@@ -127,9 +142,8 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
         return times[k]
 
     base["prune_buf"] = 0.0
-    for tpi, skin in (candidates or CANDIDATES):
-        if skin <= max_skin:
-            trial(dict(base, pp_tpi=tpi, skin=skin))
+    for tpi, skin in pp_candidates(ctx, candidates):
+        trial(dict(base, pp_tpi=tpi, skin=skin))
     best = dict(settings[min(times, key=times.get)])
     if shapes:
         for name, values in shape_options(ctx).items():
@@ -141,7 +155,7 @@ def tune(ctx, steps=150, warm=5, use_cache=True, candidates=None, finalists=3, s
         # the cell size follows the skin: each inner-list setting with every
         # list-cell divisor
         divs = shape_options(ctx)["cell_div"] if shapes else (best["cell_div"],)
-        for skin, pb in prune_options(ctx, best["skin"], max_skin):
+        for skin, pb in prune_options(ctx, best["skin"], cap):
             for d in divs:
                 trial(dict(best, skin=skin, prune_buf=pb, cell_div=d))
     n_prune = len(times) - n_before

@@ -94,11 +94,12 @@ def test_tuning_struct_layout():
 
 
 class _FakeCtx:
-    def __init__(self, precision, Ms):
+    def __init__(self, precision, Ms, rc=3.0):
         from p3m_b200 import Replica
 
         self.precision = precision
-        self.replicas = [Replica(N=1000, L=10.0, kappa=1.0, alpha=0.7, rc=3.0, M=M) for M in Ms]
+        self.replicas = [Replica(N=1000, L=10.0, kappa=1.0, alpha=0.7, rc=rc, M=M)
+                         for M in Ms]
 
 
 def test_autotune_search_space():
@@ -123,3 +124,19 @@ def test_autotune_search_space():
     keys = {_key(dict(base, **kw)) for kw in ({}, {"prune_buf": 0.3}, {"cell_div": 1},
                                               {"skin": 1.1}, {"gather_mode": 2})}
     assert len(keys) == 5
+
+
+def test_autotune_pp_grid_fits_the_cutoffs():
+    """The PP grid keeps the skins every replica allows (at most rc/2); with
+    cutoffs too short for all of them, each thread count is tried at the
+    largest skin allowed instead of nothing."""
+    from p3m_b200 import FP32
+    from p3m_b200.autotune import CANDIDATES, max_skin, pp_candidates
+
+    wide = _FakeCtx(FP32, [64], rc=3.0)
+    assert max_skin(wide) == 1.5 and pp_candidates(wide) == CANDIDATES
+    mid = _FakeCtx(FP32, [64], rc=2.0)
+    assert {sk for _, sk in pp_candidates(mid)} == {0.5, 0.8}
+    short = _FakeCtx(FP32, [64], rc=0.8)
+    assert pp_candidates(short) == [(1, 0.4), (2, 0.4), (4, 0.4)]
+    assert pp_candidates(short, [(2, 0.8)]) == [(2, 0.4)]
