@@ -112,24 +112,34 @@ class ClockSampler:
         time.sleep(0.15)
         self.proc.terminate()
         self.proc.wait()
-        rows = []
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
+        with open(self.path) as f:
+            lines = f.readlines()
         os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
-        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
-        return {"sm_mhz": float(np.median(loaded)) if loaded else None,
-                "sm_max_mhz": max(mx) if mx else None,
-                "power_w_max": max(pw) if pw else None,
-                "samples": len(rows), "reasons": reasons}
+        return summarise_clocks(lines)
+
+
+def summarise_clocks(lines):
+    """The clocks record of a timed region from nvidia-smi rows of
+    ClockSampler.FIELDS (csv, no header, no units): the median SM clock of the
+    samples under load (above half the highest), the highest max clock, the
+    highest power draw, and every throttle reason seen active."""
+    rows = []
+    for line in lines:
+        parts = [p.strip() for p in line.split(",")]
+        if len(parts) >= 9:
+            rows.append(parts)
+    if not rows:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+    sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+    mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+    pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+    loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+    return {"sm_mhz": float(np.median(loaded)) if loaded else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "power_w_max": max(pw) if pw else None,
+            "samples": len(rows), "reasons": reasons}
 
 
 # ---------------------------------------------------------------------------

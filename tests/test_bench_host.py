@@ -1,0 +1,46 @@
+"""bench.py's host-side bookkeeping without a device: the clocks record
+taken from nvidia-smi samples during the timed region (its median under load
+and the throttle reasons are what decide whether a number stands)."""
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "md-force-routines_b200")]
+
+import bench  # noqa: E402
+
+
+def _row(sm, mx=1965, pw="650.25", reasons=("Not Active",) * 4, active="0x0000000000000000"):
+    return ", ".join(["0", str(sm), str(mx), pw, active, *reasons]) + "\n"
+
+
+def test_clocks_median_under_load_ignores_idle_samples():
+    lines = [_row(345), _row(1965), _row(1965), _row(1950), _row(1965), _row(210)]
+    c = bench.summarise_clocks(lines)
+    assert c["sm_mhz"] == 1965.0          # the two idle samples (< half the peak) are left out
+    assert c["sm_max_mhz"] == 1965.0
+    assert c["power_w_max"] == 650.25
+    assert c["samples"] == 6
+    assert c["reasons"] == []
+
+
+def test_clocks_reasons_seen_active_are_reported():
+    power = ("Not Active", "Not Active", "Not Active", "Active")
+    hot = ("Not Active", "Active", "Not Active", "Not Active")
+    lines = [_row(1800, reasons=power), _row(1700, reasons=hot), _row(1965)]
+    assert bench.summarise_clocks(lines)["reasons"] == ["hw_thermal_slowdown", "sw_power_cap"]
+
+
+def test_clocks_tolerate_missing_fields_and_bad_lines():
+    lines = ["garbage\n", "\n", _row(1965, pw="[N/A]"), _row(1965, pw="[N/A]")]
+    c = bench.summarise_clocks(lines)
+    assert c["samples"] == 2 and c["sm_mhz"] == 1965.0 and c["power_w_max"] is None
+    assert bench.summarise_clocks([]) == {"sm_mhz": None, "sm_max_mhz": None,
+                                          "reasons": ["no samples"]}
+
+
+def test_clock_stuck_low_is_visible():
+    """A leftover clock lock shows as a median well below the max clock with
+    no reason active (the record keeps both so the run can be rejected)."""
+    c = bench.summarise_clocks([_row(990)] * 10)
+    assert c["sm_mhz"] == 990.0 and c["sm_max_mhz"] == 1965.0 and c["reasons"] == []
