@@ -307,6 +307,18 @@ def _ref_group(wid, items, warm, steps, barrier, queue):
             queue.put((wid, 0.0, 0.0, repr(e)))
 
 
+def balance(sizes, nproc):
+    """Replica indices per process: largest first, each onto the process
+    with the fewest particles so far (ties: the lowest process)."""
+    groups = [[] for _ in range(nproc)]
+    load = [0] * nproc
+    for i in sorted(range(len(sizes)), key=lambda i: -sizes[i]):
+        k = load.index(min(load))
+        groups[k].append(i)
+        load[k] += sizes[i]
+    return groups
+
+
 def run_reference(args):
     world, rank, _ = dist_setup("gloo")
     if rank != 0:
@@ -323,14 +335,12 @@ def run_reference(args):
     with ctx.Pool(cores) as pool:
         greens = _ref_greens(pool, reps)
     params = [(r.N, r.L, r.kappa, r.alpha, r.rc, r.M, r.dt, 1.0 / r.T_desired, r.seed) for r in reps]
-    # each process owns a fixed set of replicas (largest first onto the least
-    # loaded process), so nothing is set up inside the timed region
-    groups = [[] for _ in range(nproc)]
-    load = [0] * nproc
-    for i in sorted(range(len(reps)), key=lambda i: -reps[i].N):
-        k = load.index(min(load))
-        groups[k].append((params[i], greens[(reps[i].kappa, reps[i].alpha, reps[i].M, reps[i].L)]))
-        load[k] += reps[i].N
+    # each process owns a fixed set of replicas, so nothing is set up inside
+    # the timed region
+    owned = balance([r.N for r in reps], nproc)
+    groups = [[(params[i], greens[(reps[i].kappa, reps[i].alpha, reps[i].M, reps[i].L)])
+               for i in idx] for idx in owned]
+    load = [sum(reps[i].N for i in idx) for idx in owned]
     # bounded sample: the GPU arm's step and warm-up counts, capped so the arm
     # ends within a few minutes (about 0.15 s per 1e4-particle replica step)
     big = max(load) > 2 * 10 ** 5

@@ -44,3 +44,22 @@ def test_clock_stuck_low_is_visible():
     no reason active (the record keeps both so the run can be rejected)."""
     c = bench.summarise_clocks([_row(990)] * 10)
     assert c["sm_mhz"] == 990.0 and c["sm_max_mhz"] == 1965.0 and c["reasons"] == []
+
+
+def test_reference_arm_balance():
+    """The reference arm's replicas per host process: each replica once,
+    largest first onto the least loaded process."""
+    assert bench.balance([10, 10, 10], 3) == [[0], [1], [2]]
+    sizes = [1000, 5000, 3000, 3000, 2000, 1000]
+    groups = bench.balance(sizes, 2)
+    assert sorted(i for g in groups for i in g) == list(range(len(sizes)))
+    assert groups == [[1, 4, 5], [2, 3, 0]]
+    loads = [sum(sizes[i] for i in g) for g in groups]
+    assert loads == [8000, 7000]
+    # uneven ensemble (sizes as the 64-replica draws span): imbalance below the largest replica
+    import numpy as np
+
+    rng = np.random.default_rng(4)
+    sizes = [int(x) for x in rng.integers(5000, 40000, size=64)]
+    loads = [sum(sizes[i] for i in g) for g in bench.balance(sizes, 16)]
+    assert max(loads) - min(loads) <= max(sizes)
