@@ -63,3 +63,21 @@ def test_reference_arm_balance():
     sizes = [int(x) for x in rng.integers(5000, 40000, size=64)]
     loads = [sum(sizes[i] for i in g) for g in bench.balance(sizes, 16)]
     assert max(loads) - min(loads) <= max(sizes)
+
+
+def test_roofline_work_figures_of_the_ensemble():
+    """The algorithmic work the bench line divides by, for the 20 x 1e4
+    ensemble (r_c 6, 64^3): N rc^3/2 pairs x 48 FLOP = 1.037 GFLOP per pair
+    launch, and the step's roofline time at 72.4 TFLOP/s and 6650 GB/s."""
+    from p3m_b200.configs import cfg3
+
+    reps = cfg3(20)
+    assert bench.pp_flop(reps) == 20 * 10 ** 4 * 6.0 ** 3 / 2 * 48
+    flop = 20 * 10 ** 4 * (6.0 ** 3 / 2 * 48 + 3 * 32 * 8)
+    byts = 20 * (66.0 * 64 ** 3 + 120.0 * 10 ** 4)
+    t = bench.step_roofline_s(reps, 72.4, 6650.0)
+    assert t == flop / 72.4e12 + byts / 6650e9
+    assert 0.0715e-3 < t < 0.0725e-3
+    # whole-job value: all ranks' particles over the slowest rank's time
+    assert bench.job_value(2 * 10 ** 5, 2000, 1, 938.75) == 2 * 10 ** 5 * 2000 / 0.93875
+    assert bench.job_value(2 * 10 ** 5, 10, 4, 5.0) == 4 * bench.job_value(2 * 10 ** 5, 10, 1, 5.0)
