@@ -1,6 +1,8 @@
 """bench.py's host-side bookkeeping without a device: the clocks record
 taken from nvidia-smi samples during the timed region (its median under load
-and the throttle reasons are what decide whether a number stands)."""
+and the throttle reasons are what decide whether a number stands), the
+reference arm's replicas per host process, and the algorithmic work and
+whole-job value the bench line is computed from."""
 import os
 import sys
 
